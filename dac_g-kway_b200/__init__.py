@@ -1,0 +1,395 @@
+"""Python binding of libgkway.so (the B200 multilevel k-way partitioner).
+
+A thin ctypes layer over the C ABI in ``include/gkway.h``.  The library is the
+product; this module exists for scripts, tests and the benchmark.  It never
+falls back to a CPU implementation: if the shared library is missing or fails
+to load, every call raises.
+
+The package directory name contains a hyphen, so import it with
+``load_package()`` from the repository root (``__graft_entry__`` and the tests
+do) or add the repository to ``sys.path`` and use ``importlib``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgkway.so")
+CLI_PATH = os.path.join(HERE, "bin", "g-kway")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "gkway.h")
+
+MAX_LEVELS = 64
+GKW_OK = 0
+GKW_E_INVALID = 1
+GKW_E_CUDA = 2
+GKW_E_NOMEM = 3
+GKW_E_UNSUPPORTED = 4
+GKW_E_INIT = 5
+GKW_E_INTERNAL = 6
+INIT_DEVICE = 0
+INIT_CALLBACK = 1
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+INIT_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p, _i32p,
+                           ctypes.c_int32, _i32p)
+
+
+class GkwError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gkw status {status}: {msg}")
+        self.status = status
+
+
+class Csr(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("nnz", ctypes.c_int64),
+        ("xadj", ctypes.c_void_p),
+        ("adjncy", ctypes.c_void_p),
+        ("adjwgt", ctypes.c_void_p),
+        ("vwgt", ctypes.c_void_p),
+    ]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("eps", ctypes.c_double),
+        ("group_cap", ctypes.c_int32),
+        ("threshold_factor", ctypes.c_int32),
+        ("move_cap", ctypes.c_int32),
+        ("init_method", ctypes.c_int32),
+        ("init_fn", INIT_FN),
+        ("init_user", ctypes.c_void_p),
+        ("seed", ctypes.c_uint64),
+        ("init_trials", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n_levels", ctypes.c_int32),
+        ("level_n", ctypes.c_int64 * MAX_LEVELS),
+        ("level_m", ctypes.c_int64 * MAX_LEVELS),
+        ("uf_rounds", ctypes.c_int32 * MAX_LEVELS),
+        ("refine_rounds", ctypes.c_int32 * MAX_LEVELS),
+        ("refine_moves", ctypes.c_int64 * MAX_LEVELS),
+        ("init_cut", ctypes.c_int64),
+        ("cut", ctypes.c_int64),
+        ("max_part_weight", ctypes.c_int64),
+        ("maxw", ctypes.c_float),
+        ("ms_coarsen", ctypes.c_double),
+        ("ms_init", ctypes.c_double),
+        ("ms_refine", ctypes.c_double),
+        ("ms_total", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        nl = self.n_levels
+        return dict(
+            n_levels=nl,
+            level_n=list(self.level_n[:nl]),
+            level_m=list(self.level_m[:nl]),
+            uf_rounds=list(self.uf_rounds[: max(nl - 1, 0)]),
+            refine_rounds=list(self.refine_rounds[: max(nl - 1, 0)]),
+            refine_moves=list(self.refine_moves[: max(nl - 1, 0)]),
+            init_cut=int(self.init_cut), cut=int(self.cut), max_part_weight=int(self.max_part_weight),
+            maxw=float(self.maxw), ms_coarsen=self.ms_coarsen, ms_init=self.ms_init,
+            ms_refine=self.ms_refine, ms_total=self.ms_total,
+        )
+
+
+# (name, restype, argtypes) of every C-ABI entry point
+_VP = ctypes.c_void_p
+_SIGS = [
+    ("gkw_create", ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int32]),
+    ("gkw_destroy", ctypes.c_int, [_VP]),
+    ("gkw_set_stream", ctypes.c_int, [_VP, _VP]),
+    ("gkw_get_stream", _VP, [_VP]),
+    ("gkw_last_error", ctypes.c_char_p, []),
+    ("gkw_default_options", None, [ctypes.POINTER(Options)]),
+    ("gkw_version", ctypes.c_char_p, []),
+    ("gkw_kernel_launches", ctypes.c_uint64, []),
+    ("gkw_partition", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.POINTER(Options), _VP,
+                                     _i64p, ctypes.POINTER(Stats)]),
+    ("gkw_partition_device", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.POINTER(Options),
+                                            _VP, _i64p, ctypes.POINTER(Stats)]),
+    ("gkw_match", ctypes.c_int, [_VP, ctypes.POINTER(Csr), _VP]),
+    ("gkw_union_find", ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, _VP, _i32p]),
+    ("gkw_group_map", ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, ctypes.c_int32, _VP, _i32p]),
+    ("gkw_contract", ctypes.c_int, [_VP, ctypes.POINTER(Csr), _VP, ctypes.c_int32, _VP, _VP, _VP, _VP, _i64p]),
+    ("gkw_update_vertex_info", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, _VP, _VP, _VP, _VP, _VP]),
+    ("gkw_refine", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.c_float, ctypes.c_int32, _VP,
+                                  _VP, _VP, _VP, _VP, _VP, ctypes.c_int32, _i32p, _i64p]),
+    ("gkw_init_partition", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.c_double,
+                                          ctypes.c_uint64, ctypes.c_int32, _VP]),
+    ("gkw_cut", ctypes.c_int, [_VP, ctypes.POINTER(Csr), _VP, ctypes.c_int32, _i64p, _i64p]),
+    ("gkw_read_metis", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _i32p, _i64p, ctypes.POINTER(_i32p),
+                                      ctypes.POINTER(_i32p), ctypes.POINTER(_i32p), ctypes.POINTER(_i32p)]),
+    ("gkw_write_partition", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _i32p]),
+    ("gkw_free", None, [_VP]),
+    ("gkw_max_part_weight", ctypes.c_float, [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]),
+]
+
+_lib = None
+
+
+def build() -> None:
+    """Compile libgkway.so and the CLI in place (nvcc, sm_100a)."""
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}"], check=True)
+
+
+def lib():
+    """The loaded shared library; raises if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GkwError(GKW_E_INTERNAL, f"{LIB_PATH} is missing: run build() first")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _SIGS:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process so far."""
+    return int(lib().gkw_kernel_launches())
+
+
+def last_error() -> str:
+    s = lib().gkw_last_error()
+    return s.decode() if s else ""
+
+
+def check(status: int) -> None:
+    if status != GKW_OK:
+        raise GkwError(status, last_error())
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().gkw_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def max_part_weight(total_vwgt: int, k: int, eps: float = 0.03) -> float:
+    return float(lib().gkw_max_part_weight(int(total_vwgt), int(k), float(eps)))
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def read_metis(path: str, reference_quirks: bool = False):
+    """Parse a METIS .graph file with the library's parser -> (xadj, adjncy, adjwgt, vwgt) 0-based."""
+    n = ctypes.c_int32()
+    nnz = ctypes.c_int64()
+    ptrs = [_i32p() for _ in range(4)]
+    check(lib().gkw_read_metis(path.encode(), int(reference_quirks), ctypes.byref(n), ctypes.byref(nnz),
+                               *[ctypes.byref(p) for p in ptrs]))
+    try:
+        sizes = [n.value + 1, nnz.value, nnz.value, n.value]
+        out = [np.ctypeslib.as_array(p, (max(s, 1),))[:s].copy() for p, s in zip(ptrs, sizes)]
+    finally:
+        for p in ptrs:
+            lib().gkw_free(ctypes.cast(p, _VP))
+    return tuple(out)
+
+
+def write_partition(path: str, part) -> None:
+    part = _i32(part)
+    check(lib().gkw_write_partition(path.encode(), int(part.shape[0]), part.ctypes.data_as(_i32p)))
+
+
+def _csr_host(xadj, adjncy, adjwgt=None, vwgt=None):
+    keep = [_i32(xadj), _i32(adjncy)]
+    keep.append(None if adjwgt is None else _i32(adjwgt))
+    keep.append(None if vwgt is None else _i32(vwgt))
+    c = Csr()
+    c.n = keep[0].shape[0] - 1
+    c.nnz = keep[1].shape[0]
+    c.xadj = keep[0].ctypes.data
+    c.adjncy = keep[1].ctypes.data if keep[1].shape[0] else None
+    c.adjwgt = None if keep[2] is None or not keep[2].shape[0] else keep[2].ctypes.data
+    c.vwgt = None if keep[3] is None or not keep[3].shape[0] else keep[3].ctypes.data
+    return c, keep
+
+
+def _csr_dev(xadj, adjncy, adjwgt, vwgt):
+    """Csr over torch CUDA int32 tensors (no copy)."""
+    c = Csr()
+    c.n = int(xadj.shape[0]) - 1
+    c.nnz = int(adjncy.shape[0])
+    c.xadj = xadj.data_ptr()
+    c.adjncy = adjncy.data_ptr() if adjncy.numel() else None
+    c.adjwgt = adjwgt.data_ptr() if adjwgt is not None and adjwgt.numel() else None
+    c.vwgt = vwgt.data_ptr() if vwgt is not None and vwgt.numel() else None
+    return c
+
+
+class Handle:
+    """One library handle (CUDA stream + device memory pools) on one device."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        check(lib().gkw_create(ctypes.byref(self._h), int(device)))
+        self.device = device
+
+    def close(self):
+        if self._h:
+            lib().gkw_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(lib().gkw_get_stream(self._h) or 0)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        check(lib().gkw_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    # ---- whole partitioner ----
+    def partition(self, xadj, adjncy, adjwgt, vwgt, k: int, opts: Options | None = None,
+                  init=None, part_out: np.ndarray | None = None):
+        """Host arrays in, host part out. ``init``: optional callable for the coarsest
+        level, ``init(xadj, adjncy, adjwgt, vwgt, k) -> part`` (numpy)."""
+        c, keep = _csr_host(xadj, adjncy, adjwgt, vwgt)
+        o = opts if opts is not None else default_options()
+        cb_keep = None
+        if init is not None:
+            cb_keep = _make_init_cb(init)
+            o.init_method = INIT_CALLBACK
+            o.init_fn = cb_keep
+        part = part_out if part_out is not None else np.empty(c.n, np.int32)
+        cut = ctypes.c_int64()
+        st = Stats()
+        rc = lib().gkw_partition(self._h, ctypes.byref(c), int(k), ctypes.byref(o),
+                                 part.ctypes.data if c.n else None, ctypes.byref(cut), ctypes.byref(st))
+        del keep, cb_keep
+        check(rc)
+        return part, int(cut.value), st.as_dict()
+
+    def partition_device(self, xadj, adjncy, adjwgt, vwgt, k: int, part_out, opts: Options | None = None,
+                         stats: bool = True):
+        """torch CUDA int32 tensors in, part written into ``part_out`` (torch CUDA int32)."""
+        c = _csr_dev(xadj, adjncy, adjwgt, vwgt)
+        o = opts if opts is not None else default_options()
+        cut = ctypes.c_int64()
+        st = Stats()
+        check(lib().gkw_partition_device(self._h, ctypes.byref(c), int(k), ctypes.byref(o),
+                                         part_out.data_ptr() if c.n else None, ctypes.byref(cut),
+                                         ctypes.byref(st) if stats else None))
+        return int(cut.value), (st.as_dict() if stats else None)
+
+    # ---- per-phase entry points (torch CUDA tensors) ----
+    def match(self, g) -> "torch.Tensor":
+        import torch
+        cand = torch.empty(g[0].shape[0] - 1, dtype=torch.int32, device=g[0].device)
+        c = _csr_dev(*g)
+        check(lib().gkw_match(self._h, ctypes.byref(c), cand.data_ptr() if cand.numel() else None))
+        return cand
+
+    def union_find(self, cand):
+        import torch
+        n = int(cand.shape[0])
+        root = torch.empty(n, dtype=torch.int32, device=cand.device)
+        dist = torch.empty(n, dtype=torch.int32, device=cand.device)
+        r = ctypes.c_int32()
+        check(lib().gkw_union_find(self._h, n, cand.data_ptr() if n else None, root.data_ptr() if n else None,
+                                   dist.data_ptr() if n else None, ctypes.byref(r)))
+        return root, dist, int(r.value)
+
+    def group_map(self, root, dist, group_cap: int = 6):
+        import torch
+        n = int(root.shape[0])
+        cmap = torch.empty(n, dtype=torch.int32, device=root.device)
+        nc = ctypes.c_int32()
+        check(lib().gkw_group_map(self._h, n, root.data_ptr() if n else None, dist.data_ptr() if n else None,
+                                  int(group_cap), cmap.data_ptr() if n else None, ctypes.byref(nc)))
+        return cmap, int(nc.value)
+
+    def contract(self, g, cmap, nc: int):
+        import torch
+        dev = g[0].device
+        m = int(g[1].shape[0])
+        cx = torch.empty(nc + 1, dtype=torch.int32, device=dev)
+        ca = torch.empty(max(m, 1), dtype=torch.int32, device=dev)
+        cw = torch.empty(max(m, 1), dtype=torch.int32, device=dev)
+        cv = torch.empty(max(nc, 1), dtype=torch.int32, device=dev)
+        mc = ctypes.c_int64()
+        c = _csr_dev(*g)
+        check(lib().gkw_contract(self._h, ctypes.byref(c), cmap.data_ptr() if cmap.numel() else None, int(nc),
+                                 cx.data_ptr(), ca.data_ptr(), cw.data_ptr(), cv.data_ptr(), ctypes.byref(mc)))
+        return cx, ca[: mc.value], cw[: mc.value], cv[:nc]
+
+    def update_vertex_info(self, g, k, part, updated, boundary, gain, target):
+        c = _csr_dev(*g)
+        check(lib().gkw_update_vertex_info(self._h, ctypes.byref(c), int(k), part.data_ptr(), updated.data_ptr(),
+                                           boundary.data_ptr(), gain.data_ptr(), target.data_ptr()))
+
+    def refine(self, g, k, maxw, move_cap, part, boundary, gain, target, updated, pw, initial_update=True):
+        c = _csr_dev(*g)
+        r = ctypes.c_int32()
+        mv = ctypes.c_int64()
+        check(lib().gkw_refine(self._h, ctypes.byref(c), int(k), float(maxw), int(move_cap), part.data_ptr(),
+                               boundary.data_ptr(), gain.data_ptr(), target.data_ptr(),
+                               updated.data_ptr() if updated is not None else None, pw.data_ptr(),
+                               int(initial_update), ctypes.byref(r), ctypes.byref(mv)))
+        return int(r.value), int(mv.value)
+
+    def init_partition(self, g, k, eps=0.03, seed=1, trials=8):
+        import torch
+        part = torch.empty(max(int(g[0].shape[0]) - 1, 1), dtype=torch.int32, device=g[0].device)
+        c = _csr_dev(*g)
+        check(lib().gkw_init_partition(self._h, ctypes.byref(c), int(k), float(eps), int(seed), int(trials),
+                                       part.data_ptr()))
+        return part[: int(g[0].shape[0]) - 1]
+
+    def cut(self, g, part, k):
+        c = _csr_dev(*g)
+        cut = ctypes.c_int64()
+        pw = np.zeros(k, np.int64)
+        check(lib().gkw_cut(self._h, ctypes.byref(c), part.data_ptr(), int(k), ctypes.byref(cut),
+                            pw.ctypes.data_as(_i64p)))
+        return int(cut.value), pw
+
+
+def _make_init_cb(init):
+    def cb(user, n, xadj, adjncy, adjwgt, vwgt, k, part):
+        try:
+            x = np.ctypeslib.as_array(xadj, (n + 1,)).copy()
+            m = int(x[-1])
+            a = np.ctypeslib.as_array(adjncy, (max(m, 1),))[:m].copy()
+            w = np.ctypeslib.as_array(adjwgt, (max(m, 1),))[:m].copy()
+            vw = np.ctypeslib.as_array(vwgt, (max(n, 1),))[:n].copy()
+            p = np.asarray(init(x, a, w, vw, k), dtype=np.int32)
+            if n:
+                np.ctypeslib.as_array(part, (n,))[:] = p
+            return 0
+        except Exception:
+            return -1
+    return INIT_FN(cb)
+
+
+def exported_symbols() -> list[str]:
+    """Names of the C-ABI functions declared in include/gkway.h."""
+    import re
+    src = open(HEADER_PATH).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gkw_[a-z_0-9]+)\s*\(", src)) - {"gkw_init_fn"})

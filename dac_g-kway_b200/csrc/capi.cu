@@ -1,0 +1,377 @@
+// C ABI entry points (declared in include/gkway.h).  Every entry point
+// catches the library's errors and turns them into a status code plus a
+// per-thread message; no exception crosses the boundary.
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <new>
+
+#include "gkw_internal.cuh"
+
+struct gkw_handle {
+  gkw::Handle h;
+};
+
+using namespace gkw;
+
+namespace {
+
+template <class F>
+gkw_status guard(F&& f) {
+  try {
+    f();
+    return GKW_OK;
+  } catch (const Error& e) {
+    set_error(e.msg);
+    return e.st;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return GKW_E_NOMEM;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return GKW_E_INTERNAL;
+  }
+}
+
+Handle& H(gkw_handle* h) {
+  if (!h) throw Error{GKW_E_INVALID, "handle is NULL"};
+  GKW_CUDA(cudaSetDevice(h->h.device));
+  return h->h;
+}
+
+DevGraph dev_view(const gkw_csr* g) {
+  GKW_REQUIRE(g != nullptr, GKW_E_INVALID, "graph is NULL");
+  GKW_REQUIRE(g->n >= 0 && g->nnz >= 0, GKW_E_INVALID, "negative size");
+  GKW_REQUIRE(g->nnz < ((int64_t)1 << 31), GKW_E_UNSUPPORTED, "nnz must be < 2^31");
+  GKW_REQUIRE(g->xadj != nullptr, GKW_E_INVALID, "xadj is NULL");
+  GKW_REQUIRE(g->nnz == 0 || g->adjncy != nullptr, GKW_E_INVALID, "adjncy is NULL");
+  DevGraph d;
+  d.n = g->n;
+  d.m = g->nnz;
+  d.xadj = g->xadj;
+  d.adjncy = g->adjncy;
+  d.adjwgt = g->adjwgt;
+  d.vwgt = g->vwgt;
+  return d;
+}
+
+void need_weights(const DevGraph& d) {
+  GKW_REQUIRE(d.m == 0 || d.adjwgt != nullptr, GKW_E_INVALID, "adjwgt is NULL");
+  GKW_REQUIRE(d.n == 0 || d.vwgt != nullptr, GKW_E_INVALID, "vwgt is NULL");
+}
+
+__global__ void k_fill(i32* p, i64 n, i32 v) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+__global__ void k_unpack_keys(i32 n, const u64* __restrict__ keys, i32* __restrict__ root,
+                              i32* __restrict__ dist) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) {
+    root[v] = (i32)(u32)(keys[v] >> 32);
+    dist[v] = (i32)(u32)keys[v];
+  }
+}
+
+__global__ void k_pack_keys(i32 n, const i32* __restrict__ root, const i32* __restrict__ dist,
+                            u64* __restrict__ keys) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) keys[v] = ((u64)(u32)root[v] << 32) | (u32)dist[v];
+}
+
+void sync(Handle& h) { GKW_CUDA(cudaStreamSynchronize(h.stream)); }
+
+}  // namespace
+
+extern "C" {
+
+const char* gkw_version(void) { return "gkway-b200 0.1.0"; }
+
+const char* gkw_last_error(void) { return last_error_cstr(); }
+
+uint64_t gkw_kernel_launches(void) { return launch_total(); }
+
+void gkw_default_options(gkw_options* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->eps = 0.03;
+  o->group_cap = 6;
+  o->threshold_factor = 20;
+  o->move_cap = 1024;
+  o->init_method = GKW_INIT_DEVICE;
+  o->init_fn = nullptr;
+  o->init_user = nullptr;
+  o->seed = 1;
+  o->init_trials = 8;
+}
+
+float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps) {
+  return max_part_weight(total_vwgt, k, eps);
+}
+
+gkw_status gkw_create(gkw_handle** out, int32_t device) {
+  return guard([&] {
+    GKW_REQUIRE(out != nullptr, GKW_E_INVALID, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    GKW_CUDA(cudaGetDeviceCount(&ndev));
+    GKW_REQUIRE(device >= 0 && device < ndev, GKW_E_INVALID, "no such CUDA device");
+    GKW_CUDA(cudaSetDevice(device));
+    gkw_handle* h = new gkw_handle();
+    h->h.device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->h.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete h;
+      GKW_CUDA(e);
+    }
+    h->h.own_stream = true;
+    e = cudaMallocHost(&h->h.h_pinned, 64 * sizeof(int64_t));
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(h->h.stream);
+      delete h;
+      GKW_CUDA(e);
+    }
+    int sms = 0;
+    GKW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    h->h.sm_count = sms;
+    *out = h;
+  });
+}
+
+gkw_status gkw_destroy(gkw_handle* h) {
+  return guard([&] {
+    if (!h) return;
+    cudaSetDevice(h->h.device);
+    cudaStreamSynchronize(h->h.stream);
+    if (h->h.own_stream) cudaStreamDestroy(h->h.stream);
+    cudaFreeHost(h->h.h_pinned);
+    delete h;
+  });
+}
+
+gkw_status gkw_set_stream(gkw_handle* h, void* stream) {
+  return guard([&] {
+    Handle& hh = H(h);
+    sync(hh);
+    if (hh.own_stream) cudaStreamDestroy(hh.stream);
+    hh.stream = (cudaStream_t)stream;
+    hh.own_stream = false;
+  });
+}
+
+void* gkw_get_stream(gkw_handle* h) { return h ? (void*)h->h.stream : nullptr; }
+
+gkw_status gkw_partition_device(gkw_handle* h, const gkw_csr* d_graph, int32_t k, const gkw_options* opt,
+                                int32_t* d_part_out, int64_t* cut_out, gkw_stats* stats) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    GKW_REQUIRE(g.n == 0 || d_part_out != nullptr, GKW_E_INVALID, "part_out is NULL");
+    gkw_options o;
+    if (opt) o = *opt; else gkw_default_options(&o);
+    hh.hier.reset();
+    hh.scratch.reset();
+    partition_impl(hh, g, k, o, d_part_out, cut_out, stats);
+  });
+}
+
+gkw_status gkw_partition(gkw_handle* h, const gkw_csr* graph, int32_t k, const gkw_options* opt,
+                         int32_t* part_out, int64_t* cut_out, gkw_stats* stats) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph hg = dev_view(graph);
+    GKW_REQUIRE(hg.n == 0 || part_out != nullptr, GKW_E_INVALID, "part_out is NULL");
+    gkw_options o;
+    if (opt) o = *opt; else gkw_default_options(&o);
+    hh.hier.reset();
+    hh.scratch.reset();
+    const i64 n = hg.n, m = hg.m;
+    i32* x = hh.hier.alloc_n<i32>(n + 1);
+    i32* a = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
+    i32* w = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
+    i32* vw = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
+    i32* part = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
+    GKW_CUDA(cudaMemcpyAsync(x, hg.xadj, sizeof(i32) * (n + 1), cudaMemcpyHostToDevice, hh.stream));
+    if (m) GKW_CUDA(cudaMemcpyAsync(a, hg.adjncy, sizeof(i32) * m, cudaMemcpyHostToDevice, hh.stream));
+    if (m) {
+      if (hg.adjwgt) GKW_CUDA(cudaMemcpyAsync(w, hg.adjwgt, sizeof(i32) * m, cudaMemcpyHostToDevice, hh.stream));
+      else launch(k_fill, ceil_div(m, 256), 256, 0, hh.stream, w, m, 1);
+    }
+    if (n) {
+      if (hg.vwgt) GKW_CUDA(cudaMemcpyAsync(vw, hg.vwgt, sizeof(i32) * n, cudaMemcpyHostToDevice, hh.stream));
+      else launch(k_fill, ceil_div(n, 256), 256, 0, hh.stream, vw, n, 1);
+    }
+    GKW_CHECK_LAUNCH();
+    DevGraph g;
+    g.n = hg.n;
+    g.m = m;
+    g.xadj = x;
+    g.adjncy = a;
+    g.adjwgt = w;
+    g.vwgt = vw;
+    partition_impl(hh, g, k, o, part, cut_out, stats);
+    if (n) GKW_CUDA(cudaMemcpyAsync(part_out, part, sizeof(i32) * n, cudaMemcpyDeviceToHost, hh.stream));
+    sync(hh);
+  });
+}
+
+gkw_status gkw_match(gkw_handle* h, const gkw_csr* d_graph, int32_t* d_cand) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    GKW_REQUIRE(g.m == 0 || g.adjwgt, GKW_E_INVALID, "adjwgt is NULL");
+    hh.scratch.reset();
+    run_match(hh, g, d_cand);
+    sync(hh);
+  });
+}
+
+gkw_status gkw_union_find(gkw_handle* h, int32_t n, const int32_t* d_cand, int32_t* d_root, int32_t* d_dist,
+                          int32_t* rounds_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    GKW_REQUIRE(n >= 0, GKW_E_INVALID, "negative n");
+    hh.scratch.reset();
+    u64* keys = hh.scratch.alloc_n<u64>(std::max(n, 1));
+    const i32 r = run_union_find(hh, n, d_cand, keys);
+    if (n) {
+      launch(k_unpack_keys, ceil_div(n, 256), 256, 0, hh.stream, n, keys, d_root, d_dist);
+      GKW_CHECK_LAUNCH();
+    }
+    sync(hh);
+    if (rounds_out) *rounds_out = r;
+  });
+}
+
+gkw_status gkw_group_map(gkw_handle* h, int32_t n, const int32_t* d_root, const int32_t* d_dist,
+                         int32_t group_cap, int32_t* d_cmap, int32_t* nc_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    GKW_REQUIRE(n >= 0, GKW_E_INVALID, "negative n");
+    hh.scratch.reset();
+    u64* keys = hh.scratch.alloc_n<u64>(std::max(n, 1));
+    if (n) {
+      launch(k_pack_keys, ceil_div(n, 256), 256, 0, hh.stream, n, d_root, d_dist, keys);
+      GKW_CHECK_LAUNCH();
+    }
+    const i32 nc = run_group_map(hh, n, keys, group_cap, d_cmap);
+    sync(hh);
+    if (nc_out) *nc_out = nc;
+  });
+}
+
+gkw_status gkw_contract(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_cmap, int32_t nc, int32_t* d_cxadj,
+                        int32_t* d_cadjncy, int32_t* d_cadjwgt, int32_t* d_cvwgt, int64_t* mc_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    GKW_REQUIRE(nc >= 0 && nc <= std::max(g.n, 0), GKW_E_INVALID, "nc out of range");
+    GKW_REQUIRE(d_cadjncy && d_cadjwgt, GKW_E_INVALID, "output arrays are NULL");
+    hh.scratch.reset();
+    // group cap: the largest coarse vertex may hold any number of members here
+    // (the per-phase entry point accepts any cmap), so size the member table
+    // by the largest member count.
+    i32 cap = 1;
+    {
+      std::vector<i32> hc(g.n);
+      if (g.n) GKW_CUDA(cudaMemcpy(hc.data(), d_cmap, sizeof(i32) * g.n, cudaMemcpyDeviceToHost));
+      std::vector<i32> cnt(std::max(nc, 1), 0);
+      for (i32 v = 0; v < g.n; ++v) {
+        GKW_REQUIRE(hc[v] >= 0 && hc[v] < nc, GKW_E_INVALID, "cmap entry out of range");
+        cap = std::max(cap, ++cnt[hc[v]]);
+      }
+    }
+    i32* cadj = d_cadjncy;
+    i32* cwgt = d_cadjwgt;
+    i64 mc = 0;
+    run_contract(hh, g, d_cmap, nc, cap, d_cxadj, &cadj, &cwgt, d_cvwgt, &mc, hh.scratch);
+    sync(hh);
+    if (mc_out) *mc_out = mc;
+  });
+}
+
+gkw_status gkw_update_vertex_info(gkw_handle* h, const gkw_csr* d_graph, int32_t k, const int32_t* d_part,
+                                  const int32_t* d_updated, int32_t* d_boundary, int32_t* d_gain,
+                                  int32_t* d_target) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    GKW_REQUIRE(g.m == 0 || g.adjwgt, GKW_E_INVALID, "adjwgt is NULL");
+    hh.scratch.reset();
+    check_parts(hh, g.n, d_part, k);
+    RefineCtx* c = refine_create_ext(hh, g.n, k, 1024, const_cast<i32*>(d_part), d_boundary, d_gain, d_target);
+    struct G {
+      RefineCtx* c;
+      ~G() { refine_destroy(c); }
+    } gg{c};
+    refine_update_flagged(hh, c, g, d_updated);
+    sync(hh);
+  });
+}
+
+gkw_status gkw_refine(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float maxw, int32_t move_cap,
+                      int32_t* d_part, int32_t* d_boundary, int32_t* d_gain, int32_t* d_target,
+                      const int32_t* d_updated, int32_t* d_pw, int32_t initial_update, int32_t* rounds_out,
+                      int64_t* moves_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    hh.scratch.reset();
+    check_parts(hh, g.n, d_part, k);
+    check_parts(hh, g.n, d_target, k);
+    RefineCtx* c = refine_create_ext(hh, g.n, k, move_cap, d_part, d_boundary, d_gain, d_target);
+    struct G {
+      RefineCtx* c;
+      ~G() { refine_destroy(c); }
+    } gg{c};
+    GKW_CUDA(cudaMemcpyAsync(refine_pw(c), d_pw, sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
+    refine_update_flagged(hh, c, g, initial_update ? d_updated : nullptr);
+    RefineParams p;
+    p.k = k;
+    p.maxw = maxw;
+    p.move_cap = move_cap;
+    RefineLevelStats s = refine_level(hh, c, g, p);
+    GKW_CUDA(cudaMemcpyAsync(d_pw, refine_pw(c), sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
+    sync(hh);
+    if (rounds_out) *rounds_out = s.rounds;
+    if (moves_out) *moves_out = s.moves;
+  });
+}
+
+gkw_status gkw_init_partition(gkw_handle* h, const gkw_csr* d_graph, int32_t k, double eps, uint64_t seed,
+                              int32_t trials, int32_t* d_part) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    GKW_REQUIRE(k >= 1, GKW_E_INVALID, "k must be >= 1");
+    hh.scratch.reset();
+    device_init_partition(hh, g, k, eps, seed, trials, d_part);
+    sync(hh);
+  });
+}
+
+gkw_status gkw_cut(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_part, int32_t k, int64_t* cut_out,
+                   int64_t* pw_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    GKW_REQUIRE(k >= 1, GKW_E_INVALID, "k must be >= 1");
+    hh.scratch.reset();
+    i64* d = hh.scratch.alloc_n<i64>(k + 2);
+    compute_cut_pw(hh, g, d_part, k, d, d + 2);
+    std::vector<i64> hm(k + 2);
+    GKW_CUDA(cudaMemcpyAsync(hm.data(), d, sizeof(i64) * (k + 2), cudaMemcpyDeviceToHost, hh.stream));
+    sync(hh);
+    GKW_REQUIRE(hm[1] == 0, GKW_E_INVALID, "part id out of range [0, k)");
+    if (cut_out) *cut_out = hm[0];
+    if (pw_out) memcpy(pw_out, hm.data() + 2, sizeof(i64) * k);
+  });
+}
+
+}  // extern "C"

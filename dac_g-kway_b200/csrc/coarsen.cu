@@ -1,0 +1,721 @@
+// Coarsening: heavy-edge candidates, union-find grouping, coarse ids, and
+// contraction into the coarse CSR.  Semantics follow the reference's
+// gkway/coarsen.hpp; the kernels are organised for B200 (sub-warp rows,
+// shared-memory hashing, no host round trip per union-find iteration).
+#include <algorithm>
+#include <climits>
+
+#include "gkw_internal.cuh"
+
+namespace gkw {
+
+static constexpr u32 kFull = 0xffffffffu;
+
+// ===========================================================================
+// Heavy-edge candidate (coarsen.hpp:39-78).  G lanes per vertex; each lane
+// keeps the best entry of its stride of the row under the key
+// (weight desc, neighbour degree asc, position asc), zero weights excluded;
+// the G partial results are reduced by shuffles.  This is the serial rule of
+// the reference: the first position with minimum degree among the maximum
+// weight entries, or the vertex itself when no entry has positive weight.
+// ===========================================================================
+template <int G>
+__global__ void __launch_bounds__(256) k_match(i32 n, const i32* __restrict__ xadj,
+                                               const i32* __restrict__ adjncy,
+                                               const i32* __restrict__ adjwgt, i32* __restrict__ cand) {
+  const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const i32 v = (i32)(t / G);
+  const int sub = threadIdx.x & (G - 1);
+  u32 bw = 0, bd = kFull;
+  i32 bpos = INT_MAX, bu = -1;
+  if (v < n) {
+    const i32 beg = __ldg(xadj + v), end = __ldg(xadj + v + 1);
+    for (i32 e = beg + sub; e < end; e += G) {
+      const u32 w = (u32)__ldg(adjwgt + e);
+      if (w == 0 || w < bw) continue;
+      const i32 u = __ldg(adjncy + e);
+      const u32 d = (u32)(__ldg(xadj + u + 1) - __ldg(xadj + u));
+      if (w > bw || d < bd) { bw = w; bd = d; bpos = e; bu = u; }
+    }
+  }
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    const u32 ow = __shfl_xor_sync(kFull, bw, o, G);
+    const u32 od = __shfl_xor_sync(kFull, bd, o, G);
+    const i32 op = __shfl_xor_sync(kFull, bpos, o, G);
+    const i32 ou = __shfl_xor_sync(kFull, bu, o, G);
+    const bool better = ow > bw || (ow == bw && (od < bd || (od == bd && op < bpos)));
+    if (better) { bw = ow; bd = od; bpos = op; bu = ou; }
+  }
+  if (v < n && sub == 0) cand[v] = bw > 0 ? bu : v;
+}
+
+void run_match(Handle& h, const DevGraph& g, i32* cand) {
+  if (g.n == 0) return;
+  const double avg = g.n ? (double)g.m / g.n : 0.0;
+  const int threads = 256;
+  auto go = [&](auto kern, int G) {
+    const i64 tot = (i64)g.n * G;
+    launch(kern, (u32)((tot + threads - 1) / threads), threads, 0, h.stream, g.n, g.xadj, g.adjncy,
+           g.adjwgt, cand);
+  };
+  if (avg <= 6.5) go(k_match<4>, 4);
+  else if (avg <= 14) go(k_match<8>, 8);
+  else if (avg <= 28) go(k_match<16>, 16);
+  else go(k_match<32>, 32);
+  GKW_CHECK_LAUNCH();
+}
+
+// ===========================================================================
+// Union-find label propagation (coarsen.hpp:80-118, loop :461-469), Jacobi
+// schedule.  Keys are (label << 32 | round of last raise).  Round r reads
+// buffer (r-1)&1 and raises buffer r&1 with atomicMax; that buffer still holds
+// round r-2's keys, which never exceed round r-1's, so max(own key, pushes)
+// is exactly the synchronous update.  A round whose predecessor saw no change
+// returns at once, so rounds are launched in batches without a host round trip
+// per round; the host reads the per-round change flags once per batch.
+// ===========================================================================
+__global__ void k_uf_init(i32 n, u64* __restrict__ k0, u64* __restrict__ k1) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) {
+    const u64 key = (u64)(u32)v << 32;
+    k0[v] = key;
+    k1[v] = key;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_uf_round(i32 n, const i32* __restrict__ cand,
+                                                  const u64* __restrict__ src, u64* __restrict__ dst,
+                                                  u32 it, i32* __restrict__ changed, i32 ring) {
+  // round `it` records its change flag in slot (it-1) % ring; a round whose
+  // predecessor saw no change returns at once (the test is grid-uniform)
+  if (it >= 2 && changed[(it - 2) % ring] == 0) return;
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  bool diff = false;
+  if (v < n) {
+    const i32 c = cand[v];
+    const u64 kv = src[v];
+    const u64 kc = src[c];
+    const u32 a = (u32)(kv >> 32), b = (u32)(kc >> 32);
+    atomicMax((unsigned long long*)&dst[v], (unsigned long long)kv);
+    if (a > b) {
+      atomicMax((unsigned long long*)&dst[c], (unsigned long long)(((u64)a << 32) | it));
+      diff = true;
+    } else if (a < b) {
+      atomicMax((unsigned long long*)&dst[v], (unsigned long long)(((u64)b << 32) | it));
+      diff = true;
+    }
+  }
+  const u32 any = __ballot_sync(kFull, diff);
+  if (any && (threadIdx.x & 31) == 0) atomicOr(&changed[(it - 1) % ring], 1);
+}
+
+i32 run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out) {
+  if (n == 0) return 1;
+  constexpr i32 kBatch = 16, kRing = 2 * kBatch;
+  Pool::Mark mk = h.scratch.mark();
+  u64* kb = h.scratch.alloc_n<u64>(n);
+  i32* changed = h.scratch.alloc_n<i32>(kRing);
+  const u32 nb = ceil_div(n, 256);
+  launch(k_uf_init, nb, 256, 0, h.stream, n, keys_out, kb);
+  GKW_CHECK_LAUNCH();
+  u64* buf[2] = {keys_out, kb};
+  i32* hp = (i32*)h.h_pinned;
+  i32 rounds = -1;
+  for (i32 batch = 0; rounds < 0; ++batch) {
+    // rounds 16b+1 .. 16b+16 use slots [16(b%2), 16(b%2)+16); the previous
+    // batch's slots (read by this batch's first round) stay intact
+    i32* slots = changed + (batch & 1) * kBatch;
+    GKW_CUDA(cudaMemsetAsync(slots, 0, sizeof(i32) * kBatch, h.stream));
+    for (i32 j = 0; j < kBatch; ++j) {
+      const i32 it = batch * kBatch + j + 1;
+      launch(k_uf_round, nb, 256, 0, h.stream, n, cand, buf[(it - 1) & 1], buf[it & 1], (u32)it, changed,
+             kRing);
+    }
+    GKW_CHECK_LAUNCH();
+    GKW_CUDA(cudaMemcpyAsync(hp, slots, sizeof(i32) * kBatch, cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+    for (i32 j = 0; j < kBatch; ++j)
+      if (hp[j] == 0) { rounds = batch * kBatch + j + 1; break; }
+    GKW_REQUIRE(batch < (1 << 26), GKW_E_INTERNAL, "union-find did not converge");
+  }
+  // After the first no-change round both buffers hold the fixed point, and
+  // rounds after it return at once, so keys_out (buffer 0) is final.
+  h.scratch.release(mk);
+  return rounds;
+}
+
+// ===========================================================================
+// Coarse ids (coarsen.hpp:351-421, 120-155, 474-481).  Sorted order is
+// (root, dist, id); each root's run is cut into chunks of group_cap.  A
+// group of size s gets ceil(s/cap) consecutive coarse ids starting at the
+// exclusive scan of chunk counts over roots in id order.  Groups larger than
+// the cap need the rank of each member in (dist, id) order: a warp sorts
+// groups of <= 32 members in registers, a CTA sorts groups up to
+// kGroupSmem members in shared memory, and bigger groups are sorted by a
+// global bitonic network.
+// ===========================================================================
+constexpr i32 kGroupSmem = 4096;
+
+__global__ void k_group_count(i32 n, const u64* __restrict__ keys, i32* __restrict__ gsize) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) atomicAdd(&gsize[(u32)(keys[v] >> 32)], 1);
+}
+
+__global__ void k_group_chunks(i32 n, const i32* __restrict__ gsize, i32 cap, i32* __restrict__ chunks,
+                               i32* __restrict__ bigsz) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) {
+    const i32 s = gsize[v];
+    chunks[v] = (s + cap - 1) / cap;
+    bigsz[v] = s > cap ? s : 0;
+  }
+}
+
+// big[] layout: [0] = number of big groups, [1] = number with > kGroupSmem members
+__global__ void k_group_scatter(i32 n, const u64* __restrict__ keys, const i32* __restrict__ gsize,
+                                const i32* __restrict__ cbase, const i32* __restrict__ goff,
+                                i32* __restrict__ gcur, i32 cap, i32* __restrict__ cmap,
+                                i32* __restrict__ members, i32* __restrict__ biglist,
+                                i32* __restrict__ giantlist, i32* __restrict__ counts) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const i32 r = (i32)(u32)(keys[v] >> 32);
+  const i32 s = gsize[r];
+  if (s <= cap) {
+    cmap[v] = cbase[r];
+  } else {
+    const i32 slot = atomicAdd(&gcur[r], 1);
+    members[goff[r] + slot] = (i32)v;
+    if (r == (i32)v) {
+      if (s <= kGroupSmem) biglist[atomicAdd(&counts[0], 1)] = r;
+      else giantlist[atomicAdd(&counts[1], 1)] = r;
+    }
+  }
+}
+
+__device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
+__device__ __forceinline__ u64 umax64(u64 a, u64 b) { return a < b ? b : a; }
+
+// one warp per big group with <= 32 members
+__global__ void k_group_sort_warp(const i32* __restrict__ biglist, const i32* __restrict__ counts,
+                                  const u64* __restrict__ keys, const i32* __restrict__ gsize,
+                                  const i32* __restrict__ goff, const i32* __restrict__ cbase,
+                                  const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap) {
+  const i32 nbig = counts[0];
+  const int lane = threadIdx.x & 31;
+  const i64 warp0 = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  for (i64 w = warp0; w < nbig; w += nwarps) {
+    const i32 r = biglist[w];
+    const i32 s = gsize[r];
+    if (s > 32) continue;   // warp-uniform
+    u64 key = ~0ull;
+    if (lane < s) {
+      const i32 m = members[goff[r] + lane];
+      key = ((keys[m] & 0xffffffffull) << 32) | (u32)m;   // (dist, id)
+    }
+#pragma unroll
+    for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        const u64 o = __shfl_xor_sync(kFull, key, j);
+        const bool up = (lane & kk) == 0;
+        const bool lower = (lane & j) == 0;
+        key = (lower == up) ? umin64(key, o) : umax64(key, o);
+      }
+    }
+    if (lane < s) cmap[(u32)key] = cbase[r] + lane / cap;
+  }
+}
+
+// Ascending bitonic sort of a[0..P) (P a power of two) by one CTA.
+__device__ void cta_bitonic_u64(u64* a, i32 P) {
+  for (i32 kk = 2; kk <= P; kk <<= 1) {
+    for (i32 j = kk >> 1; j > 0; j >>= 1) {
+      for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
+        const i32 l = i ^ j;
+        if (l > i) {
+          const u64 x = a[i], y = a[l];
+          const bool up = (i & kk) == 0;
+          if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// one CTA per big group with 33..kGroupSmem members
+__global__ void k_group_sort_cta(const i32* __restrict__ biglist, const i32* __restrict__ counts,
+                                 const u64* __restrict__ keys, const i32* __restrict__ gsize,
+                                 const i32* __restrict__ goff, const i32* __restrict__ cbase,
+                                 const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap) {
+  __shared__ u64 sk[kGroupSmem];
+  const i32 nbig = counts[0];
+  for (i32 b = blockIdx.x; b < nbig; b += gridDim.x) {
+    const i32 r = biglist[b];
+    const i32 s = gsize[r];
+    if (s <= 32) continue;   // block-uniform
+    i32 P = 64;
+    while (P < s) P <<= 1;
+    for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
+      u64 key = ~0ull;
+      if (i < s) {
+        const i32 m = members[goff[r] + i];
+        key = ((keys[m] & 0xffffffffull) << 32) | (u32)m;
+      }
+      sk[i] = key;
+    }
+    __syncthreads();
+    cta_bitonic_u64(sk, P);
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) cmap[(u32)sk[i]] = cbase[r] + i / cap;
+    __syncthreads();
+  }
+}
+
+// global bitonic network for one giant group (rare)
+__global__ void k_giant_load(i32 s, i32 P, const i32* __restrict__ mem, const u64* __restrict__ keys,
+                             u64* __restrict__ out) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  u64 key = ~0ull;
+  if (i < s) {
+    const i32 m = mem[i];
+    key = ((keys[m] & 0xffffffffull) << 32) | (u32)m;
+  }
+  out[i] = key;
+}
+
+__global__ void k_bitonic_step(u64* __restrict__ a, i32 P, i32 j, i32 kk) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const i64 l = i ^ j;
+  if (l > i) {
+    const u64 x = a[i], y = a[l];
+    const bool up = (i & kk) == 0;
+    if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
+  }
+}
+
+__global__ void k_giant_assign(i32 s, const u64* __restrict__ a, i32 base, i32 cap,
+                               i32* __restrict__ cmap) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < s) cmap[(u32)a[i]] = base + (i32)(i / cap);
+}
+
+i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap) {
+  GKW_REQUIRE(cap >= 1, GKW_E_INVALID, "group_cap must be >= 1");
+  if (n == 0) return 0;
+  Pool::Mark mk = h.scratch.mark();
+  const u32 nb = ceil_div(n, 256);
+  i32* gsize = h.scratch.alloc_n<i32>(n);
+  i32* chunks = h.scratch.alloc_n<i32>(n);
+  i32* bigsz = h.scratch.alloc_n<i32>(n);
+  i32* gcur = h.scratch.alloc_n<i32>(n);
+  i32* members = h.scratch.alloc_n<i32>(n);
+  i32* biglist = h.scratch.alloc_n<i32>(n);
+  i32* giantlist = h.scratch.alloc_n<i32>(n);
+  i32* counts = h.scratch.alloc_n<i32>(4);   // [0] big, [1] giant, [2] nc, [3] nbig members
+  GKW_CUDA(cudaMemsetAsync(gsize, 0, sizeof(i32) * n, h.stream));
+  GKW_CUDA(cudaMemsetAsync(gcur, 0, sizeof(i32) * n, h.stream));
+  GKW_CUDA(cudaMemsetAsync(counts, 0, sizeof(i32) * 4, h.stream));
+  launch(k_group_count, nb, 256, 0, h.stream, n, keys, gsize);
+  GKW_CHECK_LAUNCH();
+  launch(k_group_chunks, nb, 256, 0, h.stream, n, gsize, cap, chunks, bigsz);
+  GKW_CHECK_LAUNCH();
+  exclusive_scan_i32(h, chunks, chunks, n, counts + 2);   // chunks -> chunk base, total = nc
+  exclusive_scan_i32(h, bigsz, bigsz, n, counts + 3);     // member offsets of big groups
+  launch(k_group_scatter, nb, 256, 0, h.stream, n, keys, gsize, chunks, bigsz, gcur, cap, cmap, members,
+                                            biglist, giantlist, counts);
+  GKW_CHECK_LAUNCH();
+  const u32 ng = std::max<u32>(1, std::min<u32>(ceil_div(n, 8 * 32), (u32)h.sm_count * 16));
+  launch(k_group_sort_warp, ng, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz, chunks, members,
+                                              cap, cmap);
+  GKW_CHECK_LAUNCH();
+  launch(k_group_sort_cta, (u32)h.sm_count * 2, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz,
+                                                              chunks, members, cap, cmap);
+  GKW_CHECK_LAUNCH();
+  i32* hp = (i32*)h.h_pinned;
+  GKW_CUDA(cudaMemcpyAsync(hp, counts, sizeof(i32) * 4, cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  const i32 n_giant = hp[1];
+  const i32 nc = hp[2];
+  if (n_giant > 0) {
+    std::vector<i32> giants(n_giant);
+    GKW_CUDA(cudaMemcpy(giants.data(), giantlist, sizeof(i32) * n_giant, cudaMemcpyDeviceToHost));
+    std::vector<i32> gs(n), go(n), cb(n);
+    for (i32 r : giants) {
+      i32 s, off, base;
+      GKW_CUDA(cudaMemcpy(&s, gsize + r, sizeof(i32), cudaMemcpyDeviceToHost));
+      GKW_CUDA(cudaMemcpy(&off, bigsz + r, sizeof(i32), cudaMemcpyDeviceToHost));
+      GKW_CUDA(cudaMemcpy(&base, chunks + r, sizeof(i32), cudaMemcpyDeviceToHost));
+      i32 P = 1;
+      while (P < s) P <<= 1;
+      Pool::Mark m2 = h.scratch.mark();
+      u64* a = h.scratch.alloc_n<u64>(P);
+      const u32 pb = ceil_div(P, 256);
+      launch(k_giant_load, pb, 256, 0, h.stream, s, P, members + off, keys, a);
+      for (i32 kk = 2; kk <= P; kk <<= 1)
+        for (i32 j = kk >> 1; j > 0; j >>= 1) launch(k_bitonic_step, pb, 256, 0, h.stream, a, P, j, kk);
+      launch(k_giant_assign, ceil_div(s, 256), 256, 0, h.stream, s, a, base, cap, cmap);
+      GKW_CHECK_LAUNCH();
+      GKW_CUDA(cudaStreamSynchronize(h.stream));
+      h.scratch.release(m2);
+    }
+  }
+  h.scratch.release(mk);
+  return nc;
+}
+
+// ===========================================================================
+// Contraction (coarsen.hpp:157-349).  Members of each coarse vertex are
+// listed (at most group_cap of them); then one warp per coarse vertex hashes
+// the mapped neighbour ids of all its members into shared memory, summing
+// weights, drops the self id, sorts the distinct ids and writes the row to a
+// staging area at an upper-bound offset; a scan of the row lengths gives the
+// coarse xadj and a copy compacts the rows.  Rows longer than the warp's
+// table go to a CTA with a larger shared table, and rows longer than that to
+// a CTA with a table in global scratch.
+// ===========================================================================
+__global__ void k_coarse_accum(i32 n, const i32* __restrict__ xadj, const i32* __restrict__ vwgt,
+                               const i32* __restrict__ cmap, i32 cap, i32* __restrict__ cvwgt,
+                               i32* __restrict__ rowlen, i32* __restrict__ mcnt, i32* __restrict__ memtab) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const i32 c = cmap[v];
+  atomicAdd((u32*)&cvwgt[c], (u32)vwgt[v]);
+  atomicAdd(&rowlen[c], xadj[v + 1] - xadj[v]);
+  const i32 slot = atomicAdd(&mcnt[c], 1);
+  memtab[(i64)c * cap + slot] = (i32)v;
+}
+
+__device__ __forceinline__ u32 hash_u32(u32 x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+static constexpr u32 kEmpty = 0xffffffffu;
+
+// Insert (key, w) into an open-addressing table of size hsz (power of two).
+// The table always has free slots (hsz >= 2 * entries), so the probe ends;
+// the probe count is still bounded by hsz.
+__device__ __forceinline__ void table_add(u32* keys, u32* vals, u32 hsz, u32 key, u32 w) {
+  u32 s = hash_u32(key) & (hsz - 1);
+  for (u32 probe = 0; probe < hsz; ++probe) {
+    const u32 prev = atomicCAS(&keys[s], kEmpty, key);
+    if (prev == kEmpty || prev == key) {
+      atomicAdd(&vals[s], w);
+      return;
+    }
+    s = (s + 1) & (hsz - 1);
+  }
+}
+
+template <int WCAP>
+struct WarpTable {
+  u32 keys[2 * WCAP];
+  u32 vals[2 * WCAP];
+  u64 out[WCAP];
+};
+
+// Warp-level ascending bitonic sort of a[0..P) in shared memory, P power of 2 >= 32.
+__device__ void warp_bitonic_u64(u64* a, i32 P, int lane) {
+  for (i32 kk = 2; kk <= P; kk <<= 1) {
+    for (i32 j = kk >> 1; j > 0; j >>= 1) {
+      for (i32 i = lane; i < P; i += 32) {
+        const i32 l = i ^ j;
+        if (l > i) {
+          const u64 x = a[i], y = a[l];
+          const bool up = (i & kk) == 0;
+          if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+template <int WCAP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
+    i32 nc, const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
+    const i32* __restrict__ cmap, const i32* __restrict__ memtab, const i32* __restrict__ mcnt, i32 cap,
+    const i32* __restrict__ rowlen, const i32* __restrict__ ub, i32* __restrict__ sadj,
+    i32* __restrict__ swgt, i32* __restrict__ cnt, i32* __restrict__ heavy, i32* __restrict__ nheavy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpTable<WCAP>* tabs = reinterpret_cast<WarpTable<WCAP>*>(smem_raw);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  WarpTable<WCAP>& T = tabs[wid];
+  const i64 nw = (i64)gridDim.x * WARPS;
+  for (i64 c = (i64)blockIdx.x * WARPS + wid; c < nc; c += nw) {
+    const i32 L = rowlen[c];
+    if (L > WCAP) {
+      if (lane == 0) heavy[atomicAdd(nheavy, 1)] = (i32)c;
+      continue;
+    }
+    u32 hsz = 32;
+    while (hsz < 2u * (u32)L) hsz <<= 1;
+    for (u32 i = lane; i < hsz; i += 32) { T.keys[i] = kEmpty; T.vals[i] = 0; }
+    __syncwarp();
+    const i32 nm = mcnt[c];
+    for (i32 j = 0; j < nm; ++j) {
+      const i32 v = memtab[c * (i64)cap + j];
+      const i32 beg = xadj[v], end = xadj[v + 1];
+      for (i32 e = beg + lane; e < end; e += 32) {
+        const u32 key = (u32)cmap[adjncy[e]];
+        if (key != (u32)c) table_add(T.keys, T.vals, hsz, key, (u32)adjwgt[e]);
+      }
+    }
+    __syncwarp();
+    // compact occupied slots
+    i32 U = 0;
+    for (u32 base = 0; base < hsz; base += 32) {
+      const u32 s = base + lane;
+      const bool occ = T.keys[s] != kEmpty;
+      const u32 bal = __ballot_sync(kFull, occ);
+      if (occ) {
+        const i32 pos = U + __popc(bal & ((1u << lane) - 1));
+        T.out[pos] = ((u64)T.keys[s] << 32) | T.vals[s];
+      }
+      U += __popc(bal);
+    }
+    __syncwarp();
+    const i32 o = ub[c];
+    if (U <= 32) {
+      u64 key = lane < U ? T.out[lane] : ~0ull;
+#pragma unroll
+      for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+          const u64 ot = __shfl_xor_sync(kFull, key, j);
+          const bool up = (lane & kk) == 0;
+          const bool lower = (lane & j) == 0;
+          key = (lower == up) ? umin64(key, ot) : umax64(key, ot);
+        }
+      }
+      if (lane < U) {
+        sadj[o + lane] = (i32)(u32)(key >> 32);
+        swgt[o + lane] = (i32)(u32)key;
+      }
+    } else {
+      i32 P = 64;
+      while (P < U) P <<= 1;
+      for (i32 i = U + lane; i < P; i += 32) T.out[i] = ~0ull;
+      __syncwarp();
+      warp_bitonic_u64(T.out, P, lane);
+      for (i32 i = lane; i < U; i += 32) {
+        const u64 kv = T.out[i];
+        sadj[o + i] = (i32)(u32)(kv >> 32);
+        swgt[o + i] = (i32)(u32)kv;
+      }
+    }
+    if (lane == 0) cnt[c] = U;
+    __syncwarp();
+  }
+}
+
+// One CTA per heavy coarse row.  Table in dynamic shared memory when it fits,
+// otherwise in a global scratch slice (tab_keys/tab_vals/tab_out sized for the
+// largest heavy row).
+template <bool GLOBAL_TABLE>
+__global__ void __launch_bounds__(512) k_contract_cta(
+    const i32* __restrict__ heavy, const i32* __restrict__ nheavy, i32 cta_cap,
+    const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
+    const i32* __restrict__ cmap, const i32* __restrict__ memtab, const i32* __restrict__ mcnt, i32 cap,
+    const i32* __restrict__ rowlen, const i32* __restrict__ ub, i32* __restrict__ sadj,
+    i32* __restrict__ swgt, i32* __restrict__ cnt, u32* __restrict__ gkeys, u32* __restrict__ gvals,
+    u64* __restrict__ gout, i64 gstride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ i32 s_count;
+  const i32 nh = *nheavy;
+  for (i32 b = blockIdx.x; b < nh; b += gridDim.x) {
+    const i32 c = heavy[b];
+    const i32 L = rowlen[c];
+    const bool mine = GLOBAL_TABLE ? (L > cta_cap) : (L <= cta_cap);
+    if (!mine) continue;   // block-uniform
+    u32 hsz = 64;
+    while (hsz < 2u * (u32)L) hsz <<= 1;
+    u32 *keys, *vals;
+    u64* out;
+    if (GLOBAL_TABLE) {
+      keys = gkeys + (i64)blockIdx.x * gstride * 2;
+      vals = gvals + (i64)blockIdx.x * gstride * 2;
+      out = gout + (i64)blockIdx.x * gstride;
+    } else {
+      keys = reinterpret_cast<u32*>(smem_raw);
+      vals = keys + 2 * cta_cap;
+      out = reinterpret_cast<u64*>(vals + 2 * cta_cap);
+    }
+    for (u32 i = threadIdx.x; i < hsz; i += blockDim.x) { keys[i] = kEmpty; vals[i] = 0; }
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    const i32 nm = mcnt[c];
+    for (i32 j = 0; j < nm; ++j) {
+      const i32 v = memtab[c * (i64)cap + j];
+      const i32 beg = xadj[v], end = xadj[v + 1];
+      for (i32 e = beg + threadIdx.x; e < end; e += blockDim.x) {
+        const u32 key = (u32)cmap[adjncy[e]];
+        if (key != (u32)c) table_add(keys, vals, hsz, key, (u32)adjwgt[e]);
+      }
+    }
+    __syncthreads();
+    for (u32 s = threadIdx.x; s < hsz; s += blockDim.x) {
+      if (keys[s] != kEmpty) {
+        const i32 pos = atomicAdd(&s_count, 1);
+        out[pos] = ((u64)keys[s] << 32) | vals[s];
+      }
+    }
+    __syncthreads();
+    const i32 U = s_count;
+    i32 P = 64;
+    while (P < U) P <<= 1;
+    for (i32 i = U + threadIdx.x; i < P; i += blockDim.x) out[i] = ~0ull;
+    __syncthreads();
+    cta_bitonic_u64(out, P);
+    const i32 o = ub[c];
+    for (i32 i = threadIdx.x; i < U; i += blockDim.x) {
+      const u64 kv = out[i];
+      sadj[o + i] = (i32)(u32)(kv >> 32);
+      swgt[o + i] = (i32)(u32)kv;
+    }
+    if (threadIdx.x == 0) cnt[c] = U;
+    __syncthreads();
+  }
+}
+
+__global__ void k_max_heavy(const i32* __restrict__ heavy, const i32* __restrict__ nheavy,
+                            const i32* __restrict__ rowlen, i32* __restrict__ maxlen) {
+  const i32 nh = *nheavy;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += (i64)gridDim.x * blockDim.x)
+    atomicMax(maxlen, rowlen[heavy[i]]);
+}
+
+__global__ void k_copy_rows(i32 nc, const i32* __restrict__ ub, const i32* __restrict__ cnt,
+                            const i32* __restrict__ cx, const i32* __restrict__ sadj,
+                            const i32* __restrict__ swgt, i32* __restrict__ cadj, i32* __restrict__ cwgt) {
+  const int lane = threadIdx.x & 31;
+  const i64 w0 = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+  for (i64 c = w0; c < nc; c += nw) {
+    const i32 src = ub[c], dst = cx[c], len = cnt[c];
+    for (i32 i = lane; i < len; i += 32) {
+      cadj[dst + i] = sadj[src + i];
+      cwgt[dst + i] = swgt[src + i];
+    }
+  }
+}
+
+__global__ void k_set_last(i32* cx, i32 nc, const i32* total) { cx[nc] = *total; }
+
+void run_contract(Handle& h, const DevGraph& g, const i32* cmap, i32 nc, i32 cap, i32* cxadj,
+                  i32** cadjncy, i32** cadjwgt, i32* cvwgt, i64* mc, Pool& out_pool) {
+  Pool::Mark mk = h.scratch.mark();
+  const i32 n = g.n;
+  const u32 nb = ceil_div(std::max(n, 1), 256);
+  i32* rowlen = h.scratch.alloc_n<i32>(nc + 1);
+  i32* ub = h.scratch.alloc_n<i32>(nc + 1);
+  i32* mcnt = h.scratch.alloc_n<i32>(nc + 1);
+  i32* memtab = h.scratch.alloc_n<i32>((i64)nc * cap + 1);
+  i32* cnt = h.scratch.alloc_n<i32>(nc + 1);
+  i32* heavy = h.scratch.alloc_n<i32>(nc + 1);
+  i32* misc = h.scratch.alloc_n<i32>(8);   // [0] nheavy, [1] ub total, [2] mc, [3] max heavy len
+  i32* sadj = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
+  i32* swgt = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
+  GKW_CUDA(cudaMemsetAsync(cvwgt, 0, sizeof(i32) * std::max(nc, 1), h.stream));
+  GKW_CUDA(cudaMemsetAsync(rowlen, 0, sizeof(i32) * (nc + 1), h.stream));
+  GKW_CUDA(cudaMemsetAsync(mcnt, 0, sizeof(i32) * (nc + 1), h.stream));
+  GKW_CUDA(cudaMemsetAsync(misc, 0, sizeof(i32) * 8, h.stream));
+  if (n > 0) {
+    launch(k_coarse_accum, nb, 256, 0, h.stream, n, g.xadj, g.vwgt, cmap, cap, cvwgt, rowlen, mcnt, memtab);
+    GKW_CHECK_LAUNCH();
+  }
+  exclusive_scan_i32(h, rowlen, ub, nc, misc + 1);
+  // warp kernel: table capacity from the average row length
+  const double avgL = nc ? (double)g.m / nc : 0.0;
+  const u32 gridw = std::max<u32>(1, std::min<u32>(ceil_div(nc, 8), (u32)h.sm_count * 32));
+  if (nc > 0) {
+    if (avgL <= 48) {
+      constexpr int W = 128, WARPS = 8;
+      const size_t sm = sizeof(WarpTable<W>) * WARPS;
+      GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, 
+          nc, g.xadj, g.adjncy, g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
+    } else {
+      constexpr int W = 512, WARPS = 8;
+      const size_t sm = sizeof(WarpTable<W>) * WARPS;
+      GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, 
+          nc, g.xadj, g.adjncy, g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
+    }
+    GKW_CHECK_LAUNCH();
+    // heavy rows: shared-memory CTA table up to kCtaCap entries
+    // table of 2*kCtaCap slots (a power of two, so any L <= kCtaCap hashes
+    // into <= 2*kCtaCap slots) + kCtaCap sorted outputs: 96 KB
+    constexpr i32 kCtaCap = 4096;
+    const size_t csm = (size_t)kCtaCap * 2 * 4 * 2 + (size_t)kCtaCap * 8;
+    GKW_CUDA(cudaFuncSetAttribute(k_contract_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+    launch(k_contract_cta<false>, (u32)h.sm_count * 2, 512, csm, h.stream, 
+        heavy, misc, kCtaCap, g.xadj, g.adjncy, g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt,
+        cnt, nullptr, nullptr, nullptr, 0);
+    GKW_CHECK_LAUNCH();
+    // rows beyond the CTA table: global tables sized by the longest such row
+    launch(k_max_heavy, 64, 256, 0, h.stream, heavy, misc, rowlen, misc + 3);
+    GKW_CHECK_LAUNCH();
+    i32* hp = (i32*)h.h_pinned;
+    GKW_CUDA(cudaMemcpyAsync(hp, misc, sizeof(i32) * 4, cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+    const i32 maxL = hp[3];
+    if (maxL > kCtaCap) {
+      i64 stride = 64;
+      while (stride < 2 * (i64)maxL) stride <<= 1;   // table size; out needs <= stride/2
+      const u32 nblk = (u32)h.sm_count;
+      u32* gk = h.scratch.alloc_n<u32>(nblk * stride * 2);
+      u32* gv = h.scratch.alloc_n<u32>(nblk * stride * 2);
+      u64* go = h.scratch.alloc_n<u64>(nblk * stride);
+      launch(k_contract_cta<true>, nblk, 512, 0, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy, g.adjwgt,
+                                                       cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt,
+                                                       cnt, gk, gv, go, stride);
+      GKW_CHECK_LAUNCH();
+    }
+  }
+  exclusive_scan_i32(h, cnt, cxadj, nc, misc + 2);
+  launch(k_set_last, 1, 1, 0, h.stream, cxadj, nc, misc + 2);
+  GKW_CHECK_LAUNCH();
+  i32* hp = (i32*)h.h_pinned;
+  GKW_CUDA(cudaMemcpyAsync(hp, misc + 2, sizeof(i32), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  *mc = hp[0];
+  if (*cadjncy == nullptr) {
+    *cadjncy = out_pool.alloc_n<i32>(std::max<i64>(*mc, 1));
+    *cadjwgt = out_pool.alloc_n<i32>(std::max<i64>(*mc, 1));
+  }
+  if (nc > 0) {
+    launch(k_copy_rows, std::max<u32>(1, std::min<u32>(ceil_div(nc, 8), (u32)h.sm_count * 16)), 256, 0, h.stream, nc, ub, cnt, cxadj, sadj, swgt, *cadjncy, *cadjwgt);
+    GKW_CHECK_LAUNCH();
+  }
+  h.scratch.release(mk);
+}
+
+void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
+  Pool::Mark mk = h.scratch.mark();
+  i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
+  u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
+  run_match(h, g, cand);
+  out.uf_rounds = run_union_find(h, g.n, cand, keys);
+  out.cmap = h.hier.alloc_n<i32>(std::max(g.n, 1));
+  out.nc = run_group_map(h, g.n, keys, cap, out.cmap);
+  h.scratch.release(mk);
+  if (out.nc == g.n) return;   // caller discards the level
+  out.cxadj = h.hier.alloc_n<i32>(out.nc + 1);
+  out.cvwgt = h.hier.alloc_n<i32>(std::max(out.nc, 1));
+  out.cadjncy = nullptr;
+  out.cadjwgt = nullptr;
+  run_contract(h, g, out.cmap, out.nc, cap, out.cxadj, &out.cadjncy, &out.cadjwgt, out.cvwgt, &out.mc,
+               h.hier);
+}
+
+}  // namespace gkw

@@ -1,0 +1,189 @@
+// Internal declarations shared by the partitioner's CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/gkway.h"
+
+namespace gkw {
+
+typedef int32_t i32;
+typedef uint32_t u32;
+typedef int64_t i64;
+typedef uint64_t u64;
+
+constexpr int kMaxLevels = GKW_MAX_LEVELS;
+
+// ---------------------------------------------------------------------------
+// Errors: C-ABI calls return a status; the message is kept per host thread.
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+struct Error {
+  gkw_status st;
+  std::string msg;
+};
+
+#define GKW_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw ::gkw::Error{GKW_E_CUDA, std::string(#call " failed: ") + cudaGetErrorString(e_) + \
+                                         " (" __FILE__ ":" + std::to_string(__LINE__) + ")"}; \
+  } while (0)
+
+#define GKW_CHECK_LAUNCH() GKW_CUDA(cudaGetLastError())
+
+#define GKW_REQUIRE(cond, code, msg)                   \
+  do {                                                 \
+    if (!(cond)) throw ::gkw::Error{(code), (msg)};    \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Device memory: a chunked bump allocator.  Chunks are kept across calls; a
+// mark/release pair frees everything allocated after the mark.
+// ---------------------------------------------------------------------------
+class Pool {
+ public:
+  explicit Pool(size_t min_chunk = size_t(64) << 20) : min_chunk_(min_chunk) {}
+  ~Pool();
+  void* alloc(size_t bytes);
+  template <class T>
+  T* alloc_n(size_t n) { return static_cast<T*>(alloc(n * sizeof(T))); }
+  struct Mark { size_t chunk; size_t top; };
+  Mark mark() const { return {cur_, chunks_.empty() ? 0 : chunks_[cur_].top}; }
+  void release(Mark m);
+  void reset() { release({0, 0}); }
+  size_t capacity() const;
+  void reserve(size_t bytes);   // make sure one chunk of at least `bytes` exists at the front
+
+ private:
+  struct Chunk { char* base; size_t cap; size_t top; };
+  std::vector<Chunk> chunks_;
+  size_t cur_ = 0;
+  size_t min_chunk_;
+};
+
+// ---------------------------------------------------------------------------
+// Device-side CSR view of one level (0-based ids).
+// ---------------------------------------------------------------------------
+struct DevGraph {
+  i32 n = 0;
+  i64 m = 0;
+  const i32* xadj = nullptr;
+  const i32* adjncy = nullptr;
+  const i32* adjwgt = nullptr;
+  const i32* vwgt = nullptr;
+};
+
+struct Level {
+  DevGraph g;
+  i32* cmap = nullptr;   // to the next coarser level (n entries), null at the coarsest
+};
+
+// Per-level result of one coarsening step.
+struct CoarsenOut {
+  i32 nc = 0;
+  i64 mc = 0;
+  i32* cmap = nullptr;
+  i32* cxadj = nullptr;
+  i32* cadjncy = nullptr;
+  i32* cadjwgt = nullptr;
+  i32* cvwgt = nullptr;
+  i32 uf_rounds = 0;
+};
+
+// The library handle: one stream, two pools (level hierarchy and scratch),
+// small pinned host staging, the device id.
+struct Handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Pool hier;
+  Pool scratch;
+  i64* h_pinned = nullptr;      // 64 pinned i64 slots for scalar readbacks
+  i32 sm_count = 148;
+  Handle() : hier(size_t(256) << 20), scratch(size_t(256) << 20) {}
+};
+
+// ---- kernel launches ----
+// Every kernel of the library is launched through launch(), which counts the
+// launches (gkw_kernel_launches() reports the total).
+void count_launch();
+uint64_t launch_total();
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                   Args&&... args) {
+  kern<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+  count_launch();
+}
+
+// ---- device primitives (scan.cu) ----
+// Exclusive scan of `in` (n entries) into `out` (n entries); if `total` is not
+// null, the grand total is stored there (device pointer).  `in` may equal `out`.
+void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total);
+
+// ---- coarsening (coarsen.cu) ----
+void run_match(Handle& h, const DevGraph& g, i32* cand);
+// returns the number of round launches the reference's loop would make
+i32 run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out);
+i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 group_cap, i32* cmap);
+void run_contract(Handle& h, const DevGraph& g, const i32* cmap, i32 nc, i32 group_cap,
+                  i32* cxadj, i32** cadjncy, i32** cadjwgt, i32* cvwgt, i64* mc, Pool& out_pool);
+void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out);
+
+// ---- refinement (refine.cu) ----
+struct RefineCtx;   // opaque
+struct RefineParams {
+  i32 k = 2;
+  float maxw = 0.f;
+  i32 move_cap = 1024;
+};
+struct RefineLevelStats {
+  i32 rounds = 0;
+  i64 moves = 0;
+  i64 gain_sum = 0;
+};
+RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap);
+void refine_destroy(RefineCtx* c);
+// device arrays owned by the context (n_max entries each)
+i32* refine_part(RefineCtx* c);
+i32* refine_boundary(RefineCtx* c);
+i32* refine_gain(RefineCtx* c);
+i32* refine_target(RefineCtx* c);
+u32* refine_pw(RefineCtx* c);
+// Coarsest level: part given; computes boundary flags and part weights.
+void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_part_in);
+// Projects from the coarser level (state in the context) to `fine` via cmap and
+// refines `fine`.
+void refine_project(Handle& h, RefineCtx* c, const DevGraph& fine, const i32* cmap, i32 nc);
+void refine_update_flagged(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_updated);
+RefineLevelStats refine_level(Handle& h, RefineCtx* c, const DevGraph& g, const RefineParams& p);
+
+// ---- metrics (refine.cu) ----
+// d_cut needs 2 slots ([0] cut, [1] nonzero if a part id was out of range);
+// d_pw needs k.
+void compute_cut_pw(Handle& h, const DevGraph& g, const i32* part, i32 k, i64* d_cut, i64* d_pw);
+void check_parts(Handle& h, i32 n, const i32* part, i32 k);
+
+// ---- initial partition (initpart.cu) ----
+void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 seed, i32 trials,
+                           i32* d_part);
+
+// ---- driver (partitioner.cu) ----
+i64 validate(Handle& h, const DevGraph& g);   // total vertex weight; throws on malformed input
+void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
+                    i64* cut_out, gkw_stats* stats);
+RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
+                             i32* target);
+const char* last_error_cstr();
+
+// ---- host helpers ----
+float max_part_weight(i64 total_vwgt, i32 k, double eps);
+inline u32 ceil_div(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
+
+}  // namespace gkw

@@ -1,0 +1,337 @@
+// Host side of the C++ API: the METIS .graph parser, the output writer, the
+// GraphPartitioner class and the reference-compatible graph_partitioner().
+#include <dlfcn.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <fstream>
+#include <iostream>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gkway.hpp"
+
+extern "C" void gkw_io_set_error(const std::string& msg);
+
+namespace gk {
+
+namespace {
+
+std::string read_file(const std::string& path) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) throw std::runtime_error("cannot open graph file: " + path);
+  std::string buf;
+  fseek(f, 0, SEEK_END);
+  long sz = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  if (sz > 0) {
+    buf.resize((size_t)sz);
+    size_t got = fread(&buf[0], 1, (size_t)sz, f);
+    buf.resize(got);
+  }
+  fclose(f);
+  return buf;
+}
+
+struct Cursor {
+  const char* p;
+  const char* end;
+  // next line (without the newline); returns false at end of input
+  bool line(const char*& b, const char*& e) {
+    if (p >= end) return false;
+    b = p;
+    const char* q = (const char*)memchr(p, '\n', (size_t)(end - p));
+    e = q ? q : end;
+    p = q ? q + 1 : end;
+    if (e > b && e[-1] == '\r') --e;
+    return true;
+  }
+};
+
+// parse unsigned/negative decimal integers from [b, e)
+inline bool next_int(const char*& b, const char* e, long long& out) {
+  while (b < e && (*b == ' ' || *b == '\t')) ++b;
+  if (b >= e) return false;
+  bool neg = false;
+  if (*b == '-') { neg = true; ++b; }
+  if (b >= e || *b < '0' || *b > '9') throw std::runtime_error("graph file: bad token");
+  long long v = 0;
+  while (b < e && *b >= '0' && *b <= '9') v = v * 10 + (*b++ - '0');
+  out = neg ? -v : v;
+  return true;
+}
+
+}  // namespace
+
+Graph::Graph(const std::string& input_path, bool reference_quirks) {
+  const std::string buf = read_file(input_path);
+  Cursor c{buf.data(), buf.data() + buf.size()};
+  const char *b, *e;
+  // header (skip comment lines)
+  for (;;) {
+    if (!c.line(b, e)) throw std::runtime_error("graph file: missing header");
+    const char* t = b;
+    while (t < e && (*t == ' ' || *t == '\t')) ++t;
+    if (t < e && *t == '%') continue;
+    if (t == e) continue;
+    break;
+  }
+  long long n = 0, m = 0, fmt = 0, ncon = 1;
+  if (!next_int(b, e, n) || !next_int(b, e, m)) throw std::runtime_error("graph file: bad header");
+  std::string fmt_s;
+  {
+    const char* t = b;
+    while (t < e && (*t == ' ' || *t == '\t')) ++t;
+    const char* s = t;
+    while (t < e && *t >= '0' && *t <= '9') ++t;
+    fmt_s.assign(s, t);
+    b = t;
+    if (!fmt_s.empty()) fmt = std::atoll(fmt_s.c_str());
+    long long nc;
+    if (next_int(b, e, nc)) ncon = nc;
+  }
+  if (n < 0 || m < 0 || n >= (1LL << 31) || 2 * m >= (1LL << 31))
+    throw std::runtime_error("graph file: sizes out of range");
+  if (ncon != 1) throw std::runtime_error("graph file: only ncon = 1 is supported");
+  bool has_vsize = (fmt / 100) % 10 == 1;
+  bool has_vw = (fmt / 10) % 10 == 1;
+  bool has_ew = fmt % 10 == 1;
+  bool pairs_only = false;
+  if (reference_quirks) {
+    // graph.hpp:93-97,125-137: "11" means neighbour/weight pairs, nothing else is read
+    pairs_only = (fmt_s == "11");
+    has_vsize = has_vw = false;
+    has_ew = pairs_only;
+  }
+  xadj_.assign((size_t)n + 1, 0);
+  vwgt_.assign((size_t)n, 1);
+  adjncy_.clear();
+  adjwgt_.clear();
+  adjncy_.reserve((size_t)(2 * m));
+  adjwgt_.reserve((size_t)(2 * m));
+  long long v = 0;
+  while (v < n) {
+    if (!c.line(b, e)) break;
+    const char* t = b;
+    while (t < e && (*t == ' ' || *t == '\t')) ++t;
+    if (t < e && *t == '%') continue;
+    long long x;
+    if (has_vsize && !next_int(b, e, x)) throw std::runtime_error("graph file: missing vertex size");
+    if (has_vw) {
+      if (!next_int(b, e, x)) throw std::runtime_error("graph file: missing vertex weight");
+      vwgt_[(size_t)v] = (int32_t)x;
+    }
+    while (next_int(b, e, x)) {
+      if (x < 1 || x > n) throw std::runtime_error("graph file: neighbour id out of range");
+      adjncy_.push_back((int32_t)(x - 1));
+      long long w = 1;
+      if (has_ew && !next_int(b, e, w)) throw std::runtime_error("graph file: missing edge weight");
+      adjwgt_.push_back((int32_t)w);
+    }
+    ++v;
+    xadj_[(size_t)v] = (int32_t)adjncy_.size();
+  }
+  for (; v < n; ++v) xadj_[(size_t)v + 1] = (int32_t)adjncy_.size();   // missing trailing lines: isolated
+  if (!reference_quirks && (long long)adjncy_.size() != 2 * m)
+    throw std::runtime_error("graph file: header says " + std::to_string(m) + " edges, found " +
+                             std::to_string(adjncy_.size()) + " adjacency entries (expected 2m)");
+}
+
+Graph::Graph(std::vector<int32_t> xadj, std::vector<int32_t> adjncy0, std::vector<int32_t> adjwgt,
+             std::vector<int32_t> vwgt)
+    : xadj_(std::move(xadj)), adjncy_(std::move(adjncy0)), adjwgt_(std::move(adjwgt)), vwgt_(std::move(vwgt)) {
+  if (adjwgt_.empty()) adjwgt_.assign(adjncy_.size(), 1);
+  if (vwgt_.empty() && !xadj_.empty()) vwgt_.assign(xadj_.size() - 1, 1);
+}
+
+Graph::~Graph() = default;
+
+const int* Graph::get_adjncy() {
+  if (adjncy1_.size() != adjncy_.size()) {
+    adjncy1_.resize(adjncy_.size());
+    for (size_t i = 0; i < adjncy_.size(); ++i) adjncy1_[i] = adjncy_[i] + 1;
+  }
+  return adjncy1_.data();
+}
+const int* Graph::get_adjp() { return xadj_.data(); }
+const int* Graph::get_adjwgt() { return adjwgt_.data(); }
+const int* Graph::get_vwgt() { return vwgt_.data(); }
+size_t Graph::get_num_vertex() { return xadj_.empty() ? 0 : xadj_.size() - 1; }
+size_t Graph::get_num_edge() { return adjncy_.size(); }
+int Graph::get_total_vertex_weight() { return std::accumulate(vwgt_.begin(), vwgt_.end(), 0); }
+
+void Graph::dump_result(const std::vector<int>& vertex_partition, const std::string& file_name) {
+  char cwd[4096];
+  std::string dir = getcwd(cwd, sizeof(cwd)) ? std::string(cwd) : std::string(".");
+  const std::string out_path = dir + "/" + file_name + ".out";
+  std::cout << "out_path:" << out_path << "\n";
+  FILE* f = fopen(out_path.c_str(), "wb");
+  if (!f) throw std::runtime_error("cannot open output file " + out_path);
+  std::string buf;
+  buf.reserve(vertex_partition.size() * 4);
+  char tmp[16];
+  for (int p : vertex_partition) {
+    int len = snprintf(tmp, sizeof(tmp), "%d\n", p);
+    buf.append(tmp, (size_t)len);
+  }
+  fwrite(buf.data(), 1, buf.size(), f);
+  fclose(f);
+}
+
+gkw_csr Graph::csr() const {
+  gkw_csr c;
+  c.n = (int32_t)(xadj_.empty() ? 0 : xadj_.size() - 1);
+  c.nnz = (int64_t)adjncy_.size();
+  c.xadj = xadj_.data();
+  c.adjncy = adjncy_.data();
+  c.adjwgt = adjwgt_.data();
+  c.vwgt = vwgt_.data();
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+GraphPartitioner::GraphPartitioner(const gkw_options* opt, int device) {
+  if (opt) opt_ = *opt;
+  else gkw_default_options(&opt_);
+  if (gkw_create(&h_, device) != GKW_OK) throw std::runtime_error(std::string("gkw_create: ") + gkw_last_error());
+}
+
+GraphPartitioner::~GraphPartitioner() { gkw_destroy(h_); }
+
+PartitionResult GraphPartitioner::partition_with_stats(const Graph& g, int k) {
+  PartitionResult r;
+  gkw_csr c = g.csr();
+  r.part.assign((size_t)c.n, 0);
+  gkw_status st = gkw_partition(h_, &c, k, &opt_, r.part.data(), &r.cut, &r.stats);
+  if (st != GKW_OK) throw std::runtime_error(std::string("gkw_partition: ") + gkw_last_error());
+  return r;
+}
+
+std::vector<int> GraphPartitioner::partition(const Graph& g, int k) { return partition_with_stats(g, k).part; }
+
+// ---------------------------------------------------------------------------
+// METIS as the initial partitioner (the reference's behaviour), loaded at run
+// time.  idx_t is 64-bit in the reference's bundled METIS (metis.h:33).
+namespace {
+typedef int (*metis_kway_fn)(int64_t*, int64_t*, int64_t*, int64_t*, int64_t*, int64_t*, int64_t*, int64_t*,
+                             double*, double*, int64_t*, int64_t*, int64_t*);
+
+int32_t metis_init_cb(void* user, int32_t n, const int32_t* xadj, const int32_t* adjncy, const int32_t* adjwgt,
+                      const int32_t* vwgt, int32_t k, int32_t* part_out) {
+  metis_kway_fn fn = (metis_kway_fn)user;
+  const int64_t m = xadj[n];
+  std::vector<int64_t> x(n + 1), a(std::max<int64_t>(m, 1)), w(std::max<int64_t>(m, 1)),
+      vw(std::max<int32_t>(n, 1)), p(std::max<int32_t>(n, 1));
+  for (int32_t i = 0; i <= n; ++i) x[i] = xadj[i];
+  for (int64_t e = 0; e < m; ++e) { a[e] = adjncy[e]; w[e] = adjwgt[e]; }
+  for (int32_t i = 0; i < n; ++i) vw[i] = vwgt[i];
+  int64_t nv = n, ncon = 1, np = k, cut = 0;
+  int rc = fn(&nv, &ncon, x.data(), a.data(), vw.data(), nullptr, w.data(), &np, nullptr, nullptr, nullptr, &cut,
+              p.data());
+  if (rc != 1) return -1;
+  for (int32_t i = 0; i < n; ++i) part_out[i] = (int32_t)p[i];
+  return 0;
+}
+}  // namespace
+
+bool use_metis_init(gkw_options* opt, const std::string& path) {
+  void* h = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL);
+  if (!h) return false;
+  void* fn = dlsym(h, "METIS_PartGraphKway");
+  if (!fn) return false;
+  opt->init_method = GKW_INIT_CALLBACK;
+  opt->init_fn = metis_init_cb;
+  opt->init_user = fn;
+  return true;
+}
+
+}  // namespace gk
+
+// ---------------------------------------------------------------------------
+// C ABI helpers for files.
+extern "C" {
+
+gkw_status gkw_read_metis(const char* path, int32_t reference_quirks, int32_t* n_out, int64_t* nnz_out,
+                          int32_t** xadj, int32_t** adjncy, int32_t** adjwgt, int32_t** vwgt) {
+  if (!path || !n_out || !nnz_out || !xadj || !adjncy || !adjwgt || !vwgt) return GKW_E_INVALID;
+  try {
+    gk::Graph g(path, reference_quirks != 0);
+    const size_t n = g.get_num_vertex(), m = g.get_num_edge();
+    auto dup = [](const std::vector<int32_t>& v) {
+      int32_t* p = (int32_t*)std::malloc(std::max<size_t>(v.size(), 1) * sizeof(int32_t));
+      if (!p) throw std::bad_alloc();
+      if (!v.empty()) std::memcpy(p, v.data(), v.size() * sizeof(int32_t));
+      return p;
+    };
+    *xadj = dup(g.xadj());
+    *adjncy = dup(g.adjncy0());
+    *adjwgt = dup(g.adjwgt());
+    *vwgt = dup(g.vwgt());
+    *n_out = (int32_t)n;
+    *nnz_out = (int64_t)m;
+    return GKW_OK;
+  } catch (const std::bad_alloc&) {
+    return GKW_E_NOMEM;
+  } catch (const std::exception& e) {
+    gkw_io_set_error(e.what());
+    return GKW_E_INVALID;
+  }
+}
+
+gkw_status gkw_write_partition(const char* path, int32_t n, const int32_t* part) {
+  if (!path || n < 0 || (n > 0 && !part)) return GKW_E_INVALID;
+  FILE* f = fopen(path, "wb");
+  if (!f) {
+    gkw_io_set_error(std::string("cannot open ") + path);
+    return GKW_E_INVALID;
+  }
+  std::string buf;
+  buf.reserve((size_t)n * 4);
+  char tmp[16];
+  for (int32_t i = 0; i < n; ++i) {
+    int len = snprintf(tmp, sizeof(tmp), "%d\n", part[i]);
+    buf.append(tmp, (size_t)len);
+  }
+  size_t wr = fwrite(buf.data(), 1, buf.size(), f);
+  fclose(f);
+  return wr == buf.size() ? GKW_OK : GKW_E_INVALID;
+}
+
+void gkw_free(void* p) { std::free(p); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// graph_partitioner.hpp:222-365: parse, partition, print the four phase
+// timers and the cut, write <cwd>/<out>.out.  Environment:
+//   GKW_METIS_LIB=<path to libmetis.so>  initial partition by METIS, as the
+//                                        reference does (default: on device)
+//   GKW_SEED=<n>                         seed of the device initial partition
+void graph_partitioner(const std::string& GRAPH_FILE, const std::string& OUT_FILE, const int NUM_PARTITIONS) {
+  gk::Graph graph(GRAPH_FILE);
+  gkw_options opt;
+  gkw_default_options(&opt);
+  if (const char* s = std::getenv("GKW_SEED")) opt.seed = std::strtoull(s, nullptr, 10);
+  if (const char* lib = std::getenv("GKW_METIS_LIB")) {
+    if (!gk::use_metis_init(&opt, lib)) throw std::runtime_error(std::string("cannot load METIS from ") + lib);
+  }
+  gk::GraphPartitioner gp(&opt);
+  gk::PartitionResult r = gp.partition_with_stats(graph, NUM_PARTITIONS);
+  const gkw_stats& s = r.stats;
+  std::cout << "#################### Execution Time ################# \n";
+  std::cout << "Total time: " << s.ms_total / 1000.0 << "s\n";
+  std::cout << "Coarsen time: " << s.ms_coarsen / 1000.0 << "s\n";
+  std::cout << "Init partition time: " << s.ms_init / 1000.0 << "s\n";
+  std::cout << "Refinement time: " << s.ms_refine / 1000.0 << "s\n";
+  std::cout << "#################### Partition Summary ################# \n";
+  std::cout << "***** h_cutsize " << r.cut << '\n';
+  if ((double)s.max_part_weight > (double)s.maxw)
+    std::cout << "!!!@@@ ERROR, max part weight " << s.max_part_weight << " is above " << s.maxw << '\n';
+  graph.dump_result(r.part, OUT_FILE);
+}

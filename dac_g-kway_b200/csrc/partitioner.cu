@@ -1,0 +1,220 @@
+// The multilevel driver and the C ABI.
+//
+// graph_partitioner() of the reference (gkway/graph_partitioner.hpp:222-365)
+// runs coarsening (:14-123), the initial partition (:125-131) and the
+// uncoarsening loop (:133-220); partition_impl below does the same on
+// device-resident levels kept in the handle's hierarchy pool.
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <new>
+
+#include "gkw_internal.cuh"
+
+namespace gkw {
+
+// ---------------------------------------------------------------------------
+// Input validation on the device: xadj monotone from 0 to nnz, neighbour ids
+// in range and not the vertex itself, weights >= 0.  Also sums vertex weights.
+// flags[0] bit0 bad xadj, bit1 bad id, bit2 self loop, bit3 negative weight.
+// ---------------------------------------------------------------------------
+__global__ void k_validate(i32 n, i64 m, const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
+                           const i32* __restrict__ adjwgt, const i32* __restrict__ vwgt,
+                           i32* __restrict__ flags, unsigned long long* __restrict__ wsum) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  i32 f = 0;
+  u64 w = 0;
+  if (v < n) {
+    const i32 b = xadj[v], e = xadj[v + 1];
+    if (e < b || b < 0 || (i64)e > m) f |= 1;
+    if (v == 0 && b != 0) f |= 1;
+    if (v == n - 1 && (i64)e != m) f |= 1;
+    if (vwgt[v] < 0) f |= 8;
+    w = (u32)vwgt[v];
+    if (!(f & 1)) {
+      for (i32 j = b; j < e; ++j) {
+        const i32 u = adjncy[j];
+        if (u < 0 || u >= n) f |= 2;
+        else if (u == v) f |= 4;
+        if (adjwgt[j] < 0) f |= 8;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    f |= __shfl_xor_sync(0xffffffffu, f, o);
+    w += __shfl_xor_sync(0xffffffffu, w, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (f) atomicOr(flags, f);
+    if (w) atomicAdd(wsum, (unsigned long long)w);
+  }
+}
+
+__global__ void k_fill_i32(i32* p, i64 n, i32 v) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// returns total vertex weight; throws on malformed input
+i64 validate(Handle& h, const DevGraph& g) {
+  Pool::Mark mk = h.scratch.mark();
+  i32* flags = h.scratch.alloc_n<i32>(4);
+  unsigned long long* ws = h.scratch.alloc_n<unsigned long long>(1);
+  GKW_CUDA(cudaMemsetAsync(flags, 0, sizeof(i32) * 4, h.stream));
+  GKW_CUDA(cudaMemsetAsync(ws, 0, sizeof(u64), h.stream));
+  if (g.n > 0) {
+    launch(k_validate, ceil_div(g.n, 256), 256, 0, h.stream, g.n, g.m, g.xadj, g.adjncy, g.adjwgt, g.vwgt,
+                                                         flags, ws);
+    GKW_CHECK_LAUNCH();
+  }
+  GKW_CUDA(cudaMemcpyAsync(h.h_pinned, flags, sizeof(i32), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaMemcpyAsync(h.h_pinned + 1, ws, sizeof(u64), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  const i32 f = (i32)(h.h_pinned[0] & 0xffffffff);
+  const i64 W = h.h_pinned[1];
+  h.scratch.release(mk);
+  if (f & 1) throw Error{GKW_E_INVALID, "malformed xadj (must rise from 0 to nnz)"};
+  if (f & 2) throw Error{GKW_E_INVALID, "neighbour id out of range"};
+  if (f & 4) throw Error{GKW_E_INVALID, "self loop in the graph"};
+  if (f & 8) throw Error{GKW_E_INVALID, "negative weight"};
+  return W;
+}
+
+struct PhaseTimer {
+  cudaEvent_t ev[5];
+  explicit PhaseTimer(cudaStream_t s) {
+    for (auto& e : ev) GKW_CUDA(cudaEventCreate(&e));
+    (void)s;
+  }
+  ~PhaseTimer() {
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+};
+
+void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
+                           i64* cut_out, gkw_stats* stats) {
+  GKW_REQUIRE(k >= 1, GKW_E_INVALID, "k must be >= 1");
+  GKW_REQUIRE(g0.n >= 0 && g0.m >= 0 && g0.m < ((i64)1 << 31), GKW_E_UNSUPPORTED,
+              "graphs need n >= 0 and nnz < 2^31");
+  GKW_REQUIRE(opt.group_cap >= 1, GKW_E_INVALID, "group_cap must be >= 1");
+  GKW_REQUIRE(opt.threshold_factor >= 0, GKW_E_INVALID, "threshold_factor must be >= 0");
+  GKW_REQUIRE(opt.init_method == GKW_INIT_DEVICE || (opt.init_method == GKW_INIT_CALLBACK && opt.init_fn),
+              GKW_E_INVALID, "init_method CALLBACK needs init_fn");
+  PhaseTimer tm(h.stream);
+  GKW_CUDA(cudaEventRecord(tm.ev[0], h.stream));
+  const i64 W = validate(h, g0);
+  const float maxw = max_part_weight(W, k, opt.eps);
+  const i64 threshold = (i64)opt.threshold_factor * k;
+
+  // ---- coarsening (graph_partitioner.hpp:66-105) ----
+  std::vector<Level> lv(1);
+  lv[0].g = g0;
+  std::vector<i32> uf_rounds;
+  while ((i64)lv.back().g.n > threshold && (i32)lv.size() < kMaxLevels) {
+    CoarsenOut co;
+    coarsen_level(h, lv.back().g, opt.group_cap, co);
+    if (co.nc == lv.back().g.n || co.nc < k + 1) break;   // level discarded (:93-96)
+    lv.back().cmap = co.cmap;
+    Level nl;
+    nl.g.n = co.nc;
+    nl.g.m = co.mc;
+    nl.g.xadj = co.cxadj;
+    nl.g.adjncy = co.cadjncy;
+    nl.g.adjwgt = co.cadjwgt;
+    nl.g.vwgt = co.cvwgt;
+    uf_rounds.push_back(co.uf_rounds);
+    lv.push_back(nl);
+  }
+  GKW_CUDA(cudaEventRecord(tm.ev[1], h.stream));
+
+  // ---- initial partition of the coarsest level ----
+  const DevGraph& cg = lv.back().g;
+  RefineCtx* rc = refine_create(h, std::max(g0.n, 1), k, opt.move_cap);
+  struct CtxGuard {
+    RefineCtx* c;
+    ~CtxGuard() { refine_destroy(c); }
+  } cguard{rc};
+  i32* cpart = refine_part(rc);
+  if (opt.init_method == GKW_INIT_CALLBACK) {
+    std::vector<i32> hx(cg.n + 1), ha(cg.m), hw(cg.m), hv(cg.n), hp(cg.n);
+    GKW_CUDA(cudaMemcpyAsync(hx.data(), cg.xadj, sizeof(i32) * (cg.n + 1), cudaMemcpyDeviceToHost, h.stream));
+    if (cg.m) {
+      GKW_CUDA(cudaMemcpyAsync(ha.data(), cg.adjncy, sizeof(i32) * cg.m, cudaMemcpyDeviceToHost, h.stream));
+      GKW_CUDA(cudaMemcpyAsync(hw.data(), cg.adjwgt, sizeof(i32) * cg.m, cudaMemcpyDeviceToHost, h.stream));
+    }
+    if (cg.n) GKW_CUDA(cudaMemcpyAsync(hv.data(), cg.vwgt, sizeof(i32) * cg.n, cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+    const i32 rcb = opt.init_fn(opt.init_user, cg.n, hx.data(), ha.data(), hw.data(), hv.data(), k, hp.data());
+    if (rcb != 0) throw Error{GKW_E_INIT, "initial-partition callback returned " + std::to_string(rcb)};
+    for (i32 v = 0; v < cg.n; ++v)
+      if (hp[v] < 0 || hp[v] >= k) throw Error{GKW_E_INIT, "initial-partition callback gave a part out of range"};
+    if (cg.n) GKW_CUDA(cudaMemcpyAsync(cpart, hp.data(), sizeof(i32) * cg.n, cudaMemcpyHostToDevice, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+  } else {
+    device_init_partition(h, cg, k, opt.eps, opt.seed, std::max(1, std::min(8, opt.init_trials)), cpart);
+  }
+  refine_init_coarsest(h, rc, cg, cpart);
+  i64* d_metrics = h.hier.alloc_n<i64>(k + 2);   // [0] cut, [1] bad-part flag, [2..k+2) part weights
+  i64 init_cut = 0;
+  if (stats) {
+    compute_cut_pw(h, cg, refine_part(rc), k, d_metrics, d_metrics + 2);
+    GKW_CUDA(cudaMemcpyAsync(h.h_pinned, d_metrics, sizeof(i64), cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+    init_cut = h.h_pinned[0];
+  }
+  GKW_CUDA(cudaEventRecord(tm.ev[2], h.stream));
+
+  // ---- uncoarsening (graph_partitioner.hpp:174-192) ----
+  RefineParams rp;
+  rp.k = k;
+  rp.maxw = maxw;
+  rp.move_cap = opt.move_cap;
+  std::vector<RefineLevelStats> rs(lv.size());
+  for (i32 L = (i32)lv.size() - 2; L >= 0; --L) {
+    refine_project(h, rc, lv[L].g, lv[L].cmap, lv[L + 1].g.n);
+    rs[L] = refine_level(h, rc, lv[L].g, rp);
+  }
+  GKW_CUDA(cudaEventRecord(tm.ev[3], h.stream));
+  // ---- output and final metrics (graph_partitioner.hpp:194-202) ----
+  if (g0.n) {
+    GKW_CUDA(cudaMemcpyAsync(d_part_out, refine_part(rc), sizeof(i32) * g0.n, cudaMemcpyDeviceToDevice,
+                             h.stream));
+  }
+  compute_cut_pw(h, g0, d_part_out, k, d_metrics, d_metrics + 2);
+  std::vector<i64> hm(k + 2);
+  GKW_CUDA(cudaMemcpyAsync(hm.data(), d_metrics, sizeof(i64) * (k + 2), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaEventRecord(tm.ev[4], h.stream));
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  GKW_REQUIRE(hm[1] == 0, GKW_E_INTERNAL, "partition produced a part id out of range");
+  if (cut_out) *cut_out = hm[0];
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->n_levels = (i32)lv.size();
+    for (size_t i = 0; i < lv.size(); ++i) {
+      stats->level_n[i] = lv[i].g.n;
+      stats->level_m[i] = lv[i].g.m;
+    }
+    for (size_t i = 0; i < uf_rounds.size(); ++i) stats->uf_rounds[i] = uf_rounds[i];
+    for (size_t i = 0; i + 1 < lv.size(); ++i) {
+      stats->refine_rounds[i] = rs[i].rounds;
+      stats->refine_moves[i] = rs[i].moves;
+    }
+    stats->init_cut = init_cut;
+    stats->cut = hm[0];
+    i64 mx = 0;
+    for (i32 p = 0; p < k; ++p) mx = std::max(mx, hm[2 + p]);
+    stats->max_part_weight = mx;
+    stats->maxw = maxw;
+    float a = 0, b = 0, c = 0, d = 0;
+    cudaEventElapsedTime(&a, tm.ev[0], tm.ev[1]);
+    cudaEventElapsedTime(&b, tm.ev[1], tm.ev[2]);
+    cudaEventElapsedTime(&c, tm.ev[2], tm.ev[3]);
+    cudaEventElapsedTime(&d, tm.ev[0], tm.ev[4]);
+    stats->ms_coarsen = a;
+    stats->ms_init = b;
+    stats->ms_refine = c;
+    stats->ms_total = d;
+  }
+}
+
+}  // namespace gkw

@@ -1,0 +1,189 @@
+/*
+ * gkway.h -- C ABI of the B200 multilevel k-way graph partitioner.
+ *
+ * Drop-in for the G-kway (wanluanlee/DAC_g-kway) partitioning path.  The
+ * reference has no library target: its stages are C++ functions over raw
+ * device pointers, included as headers.  Each entry point below names the
+ * reference function it replaces (file:line in the reference tree).
+ *
+ * Conventions
+ *   - Graphs are CSR with int32 arrays and 0-based neighbour ids (the
+ *     reference keeps 1-based ids on the device; gk::Graph converts).
+ *     xadj[n+1], adjncy[nnz], adjwgt[nnz], vwgt[n]; nnz = xadj[n] = 2|E|.
+ *     The graph must be symmetric, without self loops; weights >= 0.
+ *   - "host" entry points take host pointers and copy; "_device" and the
+ *     per-phase entry points take device pointers on the handle's device and
+ *     run on the handle's stream; they return after that stream is idle.
+ *   - Every call returns a gkw_status; gkw_last_error() gives the message of
+ *     the last failure on the calling thread.  No C++ exception crosses the ABI.
+ *   - A handle is not re-entrant: one host thread per handle at a time.
+ */
+#ifndef GKWAY_H_
+#define GKWAY_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GKW_MAX_LEVELS 64
+
+typedef enum gkw_status {
+  GKW_OK = 0,
+  GKW_E_INVALID = 1,      /* bad argument or malformed graph */
+  GKW_E_CUDA = 2,         /* CUDA runtime error */
+  GKW_E_NOMEM = 3,        /* device allocation failed */
+  GKW_E_UNSUPPORTED = 4,  /* input outside the supported range (e.g. k too large) */
+  GKW_E_INIT = 5,         /* the initial-partition callback failed */
+  GKW_E_INTERNAL = 6
+} gkw_status;
+
+typedef struct gkw_handle gkw_handle;
+
+typedef struct gkw_csr {
+  int32_t n;
+  int64_t nnz;
+  const int32_t* xadj;
+  const int32_t* adjncy;
+  const int32_t* adjwgt; /* may be NULL: unit edge weights (host calls only) */
+  const int32_t* vwgt;   /* may be NULL: unit vertex weights (host calls only) */
+} gkw_csr;
+
+/* Initial partition of the coarsest graph.  Host arrays, 0-based; fill
+ * part_out[n] with values in [0,k) and return 0.  The reference calls host
+ * METIS here (gkway/metis_partition.hpp:4-99); a caller that wants the
+ * reference's exact behaviour passes a callback that calls METIS. */
+typedef int32_t (*gkw_init_fn)(void* user, int32_t n, const int32_t* xadj, const int32_t* adjncy,
+                               const int32_t* adjwgt, const int32_t* vwgt, int32_t k,
+                               int32_t* part_out);
+
+enum { GKW_INIT_DEVICE = 0, GKW_INIT_CALLBACK = 1 };
+
+typedef struct gkw_options {
+  double eps;               /* imbalance, 0.03 (declarations.h:17) */
+  int32_t group_cap;        /* max fine vertices per coarse vertex, 6 (graph_partitioner.hpp:229) */
+  int32_t threshold_factor; /* coarsen while n > threshold_factor*k, 20 (graph_partitioner.hpp:22) */
+  int32_t move_cap;         /* moves applied per refinement round, 1024 (uncoarsen.hpp:475) */
+  int32_t init_method;      /* GKW_INIT_DEVICE (default) or GKW_INIT_CALLBACK */
+  gkw_init_fn init_fn;
+  void* init_user;
+  uint64_t seed;            /* seed of the device initial partitioner */
+  int32_t init_trials;      /* independent device initial-partition trials (best cut kept) */
+  int32_t reserved[7];
+} gkw_options;
+
+typedef struct gkw_stats {
+  int32_t n_levels;                     /* levels kept, the input graph included */
+  int64_t level_n[GKW_MAX_LEVELS];
+  int64_t level_m[GKW_MAX_LEVELS];      /* directed CSR entries */
+  int32_t uf_rounds[GKW_MAX_LEVELS];    /* union-find round launches, per coarsening step */
+  int32_t refine_rounds[GKW_MAX_LEVELS];
+  int64_t refine_moves[GKW_MAX_LEVELS];
+  int64_t init_cut;
+  int64_t cut;                          /* exact weighted edge cut of the output */
+  int64_t max_part_weight;
+  float maxw;                           /* MAX_PARTITION_WGT (graph_partitioner.hpp:230) */
+  double ms_coarsen, ms_init, ms_refine, ms_total;   /* device time per phase */
+} gkw_stats;
+
+/* ---- handle ---------------------------------------------------------- */
+gkw_status gkw_create(gkw_handle** out, int32_t device);
+gkw_status gkw_destroy(gkw_handle* h);
+/* Use the caller's CUDA stream (a cudaStream_t) instead of the handle's own. */
+gkw_status gkw_set_stream(gkw_handle* h, void* stream);
+void* gkw_get_stream(gkw_handle* h);
+const char* gkw_last_error(void);
+void gkw_default_options(gkw_options* opt);
+const char* gkw_version(void);
+/* Kernels this library has launched in the process so far (all handles).
+ * Diagnostic, no counterpart in the reference. */
+uint64_t gkw_kernel_launches(void);
+
+/* ---- whole partitioner ------------------------------------------------
+ * Replaces graph_partitioner() (gkway/graph_partitioner.hpp:222-365):
+ * coarsening (:14-123), init_partition (:125-131), uncoarsening (:133-220).
+ * part_out receives n part ids in [0,k). cut_out and stats may be NULL. */
+gkw_status gkw_partition(gkw_handle* h, const gkw_csr* graph, int32_t k, const gkw_options* opt,
+                         int32_t* part_out, int64_t* cut_out, gkw_stats* stats);
+/* Same with device-resident input and output (d_part_out on the device). */
+gkw_status gkw_partition_device(gkw_handle* h, const gkw_csr* d_graph, int32_t k,
+                                const gkw_options* opt, int32_t* d_part_out, int64_t* cut_out,
+                                gkw_stats* stats);
+
+/* ---- per-phase entry points (device pointers) --------------------------
+ * Heavy-edge candidate per vertex.  Replaces gk::matching_with_score
+ * (gkway/coarsen.hpp:39-78).  d_cand[n] (0-based; a vertex with no positive
+ * edge weight is its own candidate). */
+gkw_status gkw_match(gkw_handle* h, const gkw_csr* d_graph, int32_t* d_cand);
+
+/* Union-find over the edges {v, cand(v)} in the deterministic (Jacobi)
+ * schedule.  Replaces the HEC_union_find loop (gkway/coarsen.hpp:80-118,
+ * 461-469).  d_root[v] = max id of v's component, d_dist[v] = hop distance
+ * from that root.  rounds_out: round launches of the loop (may be NULL). */
+gkw_status gkw_union_find(gkw_handle* h, int32_t n, const int32_t* d_cand, int32_t* d_root,
+                          int32_t* d_dist, int32_t* rounds_out);
+
+/* Coarse ids: order (root, dist, id), groups cut into chunks of group_cap.
+ * Replaces constraint_group_size + count_num_coarsen_vertex + construct_cmap
+ * (gkway/coarsen.hpp:408-421, 120-155, 474-481). */
+gkw_status gkw_group_map(gkw_handle* h, int32_t n, const int32_t* d_root, const int32_t* d_dist,
+                         int32_t group_cap, int32_t* d_cmap, int32_t* nc_out);
+
+/* Contraction: coarse CSR with sorted rows, self loops removed, parallel
+ * edges merged with summed weights; coarse vertex weights.  Replaces
+ * gk::contraction + cal_coarsen_vwgt (gkway/coarsen.hpp:302-349, 157-171).
+ * d_cxadj[nc+1]; d_cadjncy/d_cadjwgt need room for d_graph->nnz entries;
+ * d_cvwgt[nc]. */
+gkw_status gkw_contract(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_cmap, int32_t nc,
+                        int32_t* d_cxadj, int32_t* d_cadjncy, int32_t* d_cadjwgt, int32_t* d_cvwgt,
+                        int64_t* mc_out);
+
+/* Gains and targets of the flagged vertices (d_updated[v] != 0).  Replaces
+ * gk::update_vertex_info (gkway/uncoarsen.hpp:175-237), including its unsigned
+ * comparison of gains.  d_boundary, d_gain, d_target are in-out. */
+gkw_status gkw_update_vertex_info(gkw_handle* h, const gkw_csr* d_graph, int32_t k,
+                                  const int32_t* d_part, const int32_t* d_updated,
+                                  int32_t* d_boundary, int32_t* d_gain, int32_t* d_target);
+
+/* One level of independent-set refinement, in place, until no move is left.
+ * Replaces gk::refinement (gkway/uncoarsen.hpp:427-506).  If initial_update,
+ * the flagged vertices are first passed through update_vertex_info (as
+ * gk::uncoarsen does, gkway/uncoarsen.hpp:385-386).  d_pw[k] holds the part
+ * weights (in-out).  rounds_out/moves_out may be NULL. */
+gkw_status gkw_refine(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float maxw,
+                      int32_t move_cap, int32_t* d_part, int32_t* d_boundary, int32_t* d_gain,
+                      int32_t* d_target, const int32_t* d_updated, int32_t* d_pw,
+                      int32_t initial_update, int32_t* rounds_out, int64_t* moves_out);
+
+/* Device initial partition of a (coarsest) graph: recursive bisection by greedy
+ * graph growing.  Replaces the host METIS call of metis_init_partition
+ * (gkway/metis_partition.hpp:46-47). */
+gkw_status gkw_init_partition(gkw_handle* h, const gkw_csr* d_graph, int32_t k, double eps,
+                              uint64_t seed, int32_t trials, int32_t* d_part);
+
+/* Exact weighted edge cut and part weights.  Replaces gk::calculate_cutsize
+ * and calculate_partition_wgt (gkway/uncoarsen.hpp:398-424,
+ * gkway/cuda_check.hpp:61-73).  pw_out: host array of k entries (may be NULL). */
+gkw_status gkw_cut(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_part, int32_t k,
+                   int64_t* cut_out, int64_t* pw_out);
+
+/* Read a METIS .graph file (standard format: "n m [fmt [ncon]]", '%'
+ * comments, ncon 1).  reference_quirks != 0 reads a format field of "11" as
+ * neighbour/weight pairs without vertex weights, as the reference parser does
+ * (gkway/graph.hpp:70-152).  The four arrays are allocated with malloc and
+ * released with gkw_free; ids are 0-based.  No device is touched. */
+gkw_status gkw_read_metis(const char* path, int32_t reference_quirks, int32_t* n_out, int64_t* nnz_out,
+                          int32_t** xadj, int32_t** adjncy, int32_t** adjwgt, int32_t** vwgt);
+/* Write one part id per line to `path` (gkway/graph.hpp:227-240 writes
+ * <cwd>/<name>.out this way). */
+gkw_status gkw_write_partition(const char* path, int32_t n, const int32_t* part);
+void gkw_free(void* p);
+
+/* MAX_PARTITION_WGT as the reference computes it (graph_partitioner.hpp:230). */
+float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GKWAY_H_ */

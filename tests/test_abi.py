@@ -1,0 +1,122 @@
+"""The C-ABI library (CPU only): loads, exports every declared symbol, parses
+METIS files, writes partitions; the CLI's argument handling."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    L = pkg.lib()
+    syms = pkg.exported_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_version_and_defaults(pkg):
+    assert pkg.lib().gkw_version().startswith(b"gkway-b200")
+    o = pkg.default_options()
+    assert (o.eps, o.group_cap, o.threshold_factor, o.move_cap) == (0.03, 6, 20, 1024)
+    assert o.init_method == pkg.INIT_DEVICE
+
+
+def test_max_part_weight_matches_oracle(pkg):
+    for W, k in [(2048, 8), (1048576, 64), (960000, 64), (10000000, 256), (17, 3)]:
+        assert pkg.max_part_weight(W, k) == oracle.max_part_weight(W, k)
+
+
+def write_graph(path, header, lines):
+    with open(path, "w") as f:
+        f.write(header + "\n")
+        for ln in lines:
+            f.write(ln + "\n")
+
+
+def test_reader_formats(pkg, tmp_path):
+    # triangle 1-2-3 plus pendant 4 on 3
+    p = str(tmp_path / "a.graph")
+    write_graph(p, "% comment\n4 4", ["2 3", "1 3", "1 2 4", "3"])
+    x, a, w, vw = pkg.read_metis(p)
+    assert list(x) == [0, 2, 4, 7, 8] and list(a) == [1, 2, 0, 2, 0, 1, 3, 2]
+    assert np.all(w == 1) and np.all(vw == 1)
+    # fmt 1: edge weights
+    write_graph(p, "4 4 1", ["2 5 3 1", "1 5 3 2", "1 1 2 2 4 7", "3 7"])
+    x, a, w, vw = pkg.read_metis(p)
+    assert list(w) == [5, 1, 5, 2, 1, 2, 7, 7]
+    # fmt 10: vertex weights
+    write_graph(p, "4 4 10", ["3 2 3", "1 1 3", "2 1 2 4", "9 3"])
+    x, a, w, vw = pkg.read_metis(p)
+    assert list(vw) == [3, 1, 2, 9] and list(a) == [1, 2, 0, 2, 0, 1, 3, 2]
+    # fmt 011: both
+    write_graph(p, "4 4 011", ["3 2 5 3 1", "1 1 5 3 2", "2 1 1 2 2 4 7", "9 3 7"])
+    x, a, w, vw = pkg.read_metis(p)
+    assert list(vw) == [3, 1, 2, 9] and list(w) == [5, 1, 5, 2, 1, 2, 7, 7]
+    # the reference's reading of "11": neighbour/weight pairs, no vertex weights
+    write_graph(p, "4 4 11", ["2 5 3 1", "1 5 3 2", "1 1 2 2 4 7", "3 7"])
+    x, a, w, vw = pkg.read_metis(p, reference_quirks=True)
+    assert list(w) == [5, 1, 5, 2, 1, 2, 7, 7] and np.all(vw == 1)
+
+
+def test_reader_errors(pkg, tmp_path):
+    p = str(tmp_path / "b.graph")
+    write_graph(p, "3 2", ["2", "1 3", "9"])        # id out of range
+    with pytest.raises(pkg.GkwError):
+        pkg.read_metis(p)
+    write_graph(p, "3 5", ["2", "1 3", "2"])        # edge count mismatch
+    with pytest.raises(pkg.GkwError):
+        pkg.read_metis(p)
+    write_graph(p, "3 2 0 2", ["2", "1 3", "2"])    # ncon 2
+    with pytest.raises(pkg.GkwError):
+        pkg.read_metis(p)
+    with pytest.raises(pkg.GkwError):
+        pkg.read_metis(str(tmp_path / "missing.graph"))
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.N11_PATH), reason="reference fixture not available")
+def test_reader_matches_checker_on_n11(pkg):
+    x, a, w, vw = pkg.read_metis(oracle.N11_PATH)
+    g = oracle.read_metis_graph(oracle.N11_PATH)
+    assert np.array_equal(x, g.xadj) and np.array_equal(a, g.adjncy)
+    assert np.array_equal(w, g.adjwgt) and np.array_equal(vw, g.vwgt)
+
+
+def test_write_partition(pkg, tmp_path):
+    p = str(tmp_path / "o.out")
+    pkg.write_partition(p, np.array([3, 0, 1, 2], np.int32))
+    assert open(p).read() == "3\n0\n1\n2\n"
+
+
+def test_cli_usage_and_missing_file(pkg, tmp_path):
+    cli = pkg.CLI_PATH
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = subprocess.run([cli, str(tmp_path / "nope.graph"), "4", "out"], capture_output=True, text=True,
+                       cwd=tmp_path)
+    assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+def test_generators(gen):
+    g = gen.grid27(4, 3, 5)
+    gen.check_csr(g)
+    # 27-point stencil: undirected edges = sum over the 13 forward offsets of prod(n_i - |d_i|)
+    def count(nx, ny, nz):
+        tot = 0
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    if (dz, dy, dx) <= (0, 0, 0):
+                        continue
+                    tot += (nx - abs(dx)) * (ny - abs(dy)) * (nz - abs(dz))
+        return tot
+    assert g.n_edges == count(4, 3, 5)
+    assert count(100, 100, 96) == 12218972
+    d = gen.delaunay(2048, 1)
+    gen.check_csr(d)
+    assert 6000 < d.n_edges < 6200
+    c = gen.circuit(20000, seed=3, levels=50, hub_max=2000)
+    gen.check_csr(c)
+    assert c.adjwgt.min() >= 1 and c.adjwgt.max() <= 8 and c.vwgt.min() >= 1 and c.vwgt.max() <= 4
