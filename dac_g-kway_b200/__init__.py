@@ -68,7 +68,8 @@ class Options(ctypes.Structure):
         ("init_user", ctypes.c_void_p),
         ("seed", ctypes.c_uint64),
         ("init_trials", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("enforce_balance", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -80,6 +81,8 @@ class Stats(ctypes.Structure):
         ("uf_rounds", ctypes.c_int32 * MAX_LEVELS),
         ("refine_rounds", ctypes.c_int32 * MAX_LEVELS),
         ("refine_moves", ctypes.c_int64 * MAX_LEVELS),
+        ("balance_rounds", ctypes.c_int32 * MAX_LEVELS),
+        ("balance_moves", ctypes.c_int64 * MAX_LEVELS),
         ("init_cut", ctypes.c_int64),
         ("cut", ctypes.c_int64),
         ("max_part_weight", ctypes.c_int64),
@@ -99,6 +102,8 @@ class Stats(ctypes.Structure):
             uf_rounds=list(self.uf_rounds[: max(nl - 1, 0)]),
             refine_rounds=list(self.refine_rounds[: max(nl - 1, 0)]),
             refine_moves=list(self.refine_moves[: max(nl - 1, 0)]),
+            balance_rounds=list(self.balance_rounds[:nl]),
+            balance_moves=list(self.balance_moves[:nl]),
             init_cut=int(self.init_cut), cut=int(self.cut), max_part_weight=int(self.max_part_weight),
             maxw=float(self.maxw), ms_coarsen=self.ms_coarsen, ms_init=self.ms_init,
             ms_refine=self.ms_refine, ms_total=self.ms_total,
@@ -135,6 +140,9 @@ _SIGS = [
     ("gkw_write_partition", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _i32p]),
     ("gkw_free", None, [_VP]),
     ("gkw_max_part_weight", ctypes.c_float, [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]),
+    ("gkw_balance_cap", ctypes.c_float, [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]),
+    ("gkw_balance", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.c_float, ctypes.c_int32, _VP,
+                                   _VP, _VP, _VP, _VP, _i32p, _i64p]),
 ]
 
 _lib = None
@@ -185,6 +193,10 @@ def default_options(**kw) -> Options:
 
 def max_part_weight(total_vwgt: int, k: int, eps: float = 0.03) -> float:
     return float(lib().gkw_max_part_weight(int(total_vwgt), int(k), float(eps)))
+
+
+def balance_cap(total_vwgt: int, k: int, eps: float = 0.03) -> float:
+    return float(lib().gkw_balance_cap(int(total_vwgt), int(k), float(eps)))
 
 
 def _i32(a) -> np.ndarray:
@@ -353,6 +365,15 @@ class Handle:
                                int(initial_update), ctypes.byref(r), ctypes.byref(mv)))
         return int(r.value), int(mv.value)
 
+    def balance(self, g, k, cap, move_cap, part, boundary, gain, target, pw):
+        c = _csr_dev(*g)
+        r = ctypes.c_int32()
+        mv = ctypes.c_int64()
+        check(lib().gkw_balance(self._h, ctypes.byref(c), int(k), float(cap), int(move_cap), part.data_ptr(),
+                                boundary.data_ptr(), gain.data_ptr(), target.data_ptr(), pw.data_ptr(),
+                                ctypes.byref(r), ctypes.byref(mv)))
+        return int(r.value), int(mv.value)
+
     def init_partition(self, g, k, eps=0.03, seed=1, trials=8):
         import torch
         part = torch.empty(max(int(g[0].shape[0]) - 1, 1), dtype=torch.int32, device=g[0].device)
@@ -375,9 +396,13 @@ def _make_init_cb(init):
         try:
             x = np.ctypeslib.as_array(xadj, (n + 1,)).copy()
             m = int(x[-1])
-            a = np.ctypeslib.as_array(adjncy, (max(m, 1),))[:m].copy()
-            w = np.ctypeslib.as_array(adjwgt, (max(m, 1),))[:m].copy()
-            vw = np.ctypeslib.as_array(vwgt, (max(n, 1),))[:n].copy()
+            if m:
+                a = np.ctypeslib.as_array(adjncy, (m,)).copy()
+                w = np.ctypeslib.as_array(adjwgt, (m,)).copy()
+            else:
+                a = np.zeros(0, np.int32)
+                w = np.zeros(0, np.int32)
+            vw = np.ctypeslib.as_array(vwgt, (n,)).copy() if n else np.zeros(0, np.int32)
             p = np.asarray(init(x, a, w, vw, k), dtype=np.int32)
             if n:
                 np.ctypeslib.as_array(part, (n,))[:] = p

@@ -104,6 +104,7 @@ void gkw_default_options(gkw_options* o) {
   o->init_user = nullptr;
   o->seed = 1;
   o->init_trials = 8;
+  o->enforce_balance = 1;
 }
 
 float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps) {
@@ -341,6 +342,32 @@ gkw_status gkw_refine(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float ma
     if (moves_out) *moves_out = s.moves;
   });
 }
+
+gkw_status gkw_balance(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float cap, int32_t move_cap,
+                       int32_t* d_part, int32_t* d_boundary, int32_t* d_gain, int32_t* d_target, int32_t* d_pw,
+                       int32_t* rounds_out, int64_t* moves_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    hh.scratch.reset();
+    check_parts(hh, g.n, d_part, k);
+    RefineCtx* c = refine_create_ext(hh, g.n, k, move_cap, d_part, d_boundary, d_gain, d_target);
+    struct G {
+      RefineCtx* c;
+      ~G() { refine_destroy(c); }
+    } gg{c};
+    GKW_CUDA(cudaMemcpyAsync(refine_pw(c), d_pw, sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
+    refine_update_flagged(hh, c, g, nullptr);   // empty U, P from the caller's gains
+    RefineLevelStats s = balance_level(hh, c, g, cap, move_cap);
+    GKW_CUDA(cudaMemcpyAsync(d_pw, refine_pw(c), sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
+    sync(hh);
+    if (rounds_out) *rounds_out = s.rounds;
+    if (moves_out) *moves_out = s.moves;
+  });
+}
+
+float gkw_balance_cap(int64_t total_vwgt, int32_t k, double eps) { return balance_cap(total_vwgt, k, eps); }
 
 gkw_status gkw_init_partition(gkw_handle* h, const gkw_csr* d_graph, int32_t k, double eps, uint64_t seed,
                               int32_t trials, int32_t* d_part) {

@@ -137,7 +137,8 @@ i32 run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out) {
     GKW_CUDA(cudaStreamSynchronize(h.stream));
     for (i32 j = 0; j < kBatch; ++j)
       if (hp[j] == 0) { rounds = batch * kBatch + j + 1; break; }
-    GKW_REQUIRE(batch < (1 << 26), GKW_E_INTERNAL, "union-find did not converge");
+    // Jacobi rounds raise a label at most once per hop of the longest path
+    GKW_REQUIRE((i64)batch * kBatch <= (i64)n + 2 * kBatch, GKW_E_INTERNAL, "union-find did not converge");
   }
   // After the first no-change round both buffers hold the fixed point, and
   // rounds after it return at once, so keys_out (buffer 0) is final.

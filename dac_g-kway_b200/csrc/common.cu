@@ -212,6 +212,10 @@ void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total) {
   h.scratch.release(mk);   // stream-ordered reuse is safe: later kernels run after these
 }
 
+float balance_cap(i64 total_vwgt, i32 k, double eps) {
+  return (float)((1.0 + eps) * (double)total_vwgt / (double)k);
+}
+
 float max_part_weight(i64 total_vwgt, i32 k, double eps) {
   // graph_partitioner.hpp:230: (float)W/(float)k * (1.0f + IMBALANCE_RATIO) + 1,
   // IMBALANCE_RATIO a double literal, result stored as float.

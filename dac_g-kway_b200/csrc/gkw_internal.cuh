@@ -163,6 +163,10 @@ void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32*
 void refine_project(Handle& h, RefineCtx* c, const DevGraph& fine, const i32* cmap, i32 nc);
 void refine_update_flagged(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_updated);
 RefineLevelStats refine_level(Handle& h, RefineCtx* c, const DevGraph& g, const RefineParams& p);
+// Balance rounds until no part exceeds cap (or no move is possible).
+RefineLevelStats balance_level(Handle& h, RefineCtx* c, const DevGraph& g, float cap, i32 move_cap);
+// (1 + eps) * W / k, the default-mode weight cap (no "+1").
+float balance_cap(i64 total_vwgt, i32 k, double eps);
 
 // ---- metrics (refine.cu) ----
 // d_cut needs 2 slots ([0] cut, [1] nonzero if a part id was out of range);

@@ -103,7 +103,8 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   PhaseTimer tm(h.stream);
   GKW_CUDA(cudaEventRecord(tm.ev[0], h.stream));
   const i64 W = validate(h, g0);
-  const float maxw = max_part_weight(W, k, opt.eps);
+  // the reference's MAX_PARTITION_WGT, or the default mode's strict cap
+  const float maxw = opt.enforce_balance ? balance_cap(W, k, opt.eps) : max_part_weight(W, k, opt.eps);
   const i64 threshold = (i64)opt.threshold_factor * k;
 
   // ---- coarsening (graph_partitioner.hpp:66-105) ----
@@ -156,12 +157,14 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   refine_init_coarsest(h, rc, cg, cpart);
   i64* d_metrics = h.hier.alloc_n<i64>(k + 2);   // [0] cut, [1] bad-part flag, [2..k+2) part weights
   i64 init_cut = 0;
-  if (stats) {
+  if (stats) {   // cut of the initial partition itself (before any balance move)
     compute_cut_pw(h, cg, refine_part(rc), k, d_metrics, d_metrics + 2);
     GKW_CUDA(cudaMemcpyAsync(h.h_pinned, d_metrics, sizeof(i64), cudaMemcpyDeviceToHost, h.stream));
     GKW_CUDA(cudaStreamSynchronize(h.stream));
     init_cut = h.h_pinned[0];
   }
+  std::vector<RefineLevelStats> bs(lv.size());
+  if (opt.enforce_balance) bs[lv.size() - 1] = balance_level(h, rc, cg, maxw, opt.move_cap);
   GKW_CUDA(cudaEventRecord(tm.ev[2], h.stream));
 
   // ---- uncoarsening (graph_partitioner.hpp:174-192) ----
@@ -172,6 +175,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   std::vector<RefineLevelStats> rs(lv.size());
   for (i32 L = (i32)lv.size() - 2; L >= 0; --L) {
     refine_project(h, rc, lv[L].g, lv[L].cmap, lv[L + 1].g.n);
+    if (opt.enforce_balance) bs[L] = balance_level(h, rc, lv[L].g, maxw, opt.move_cap);
     rs[L] = refine_level(h, rc, lv[L].g, rp);
   }
   GKW_CUDA(cudaEventRecord(tm.ev[3], h.stream));
@@ -198,6 +202,10 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     for (size_t i = 0; i + 1 < lv.size(); ++i) {
       stats->refine_rounds[i] = rs[i].rounds;
       stats->refine_moves[i] = rs[i].moves;
+    }
+    for (size_t i = 0; i < lv.size(); ++i) {
+      stats->balance_rounds[i] = bs[i].rounds;
+      stats->balance_moves[i] = bs[i].moves;
     }
     stats->init_cut = init_cut;
     stats->cut = hm[0];

@@ -70,7 +70,10 @@ typedef struct gkw_options {
   void* init_user;
   uint64_t seed;            /* seed of the device initial partitioner */
   int32_t init_trials;      /* independent device initial-partition trials (best cut kept) */
-  int32_t reserved[7];
+  int32_t enforce_balance;  /* 1 (default): every part <= (1+eps)W/k, balance rounds at each
+                               level; 0: the reference's behaviour (MAX_PARTITION_WGT =
+                               (1+eps)W/k + 1 checked on move destinations only) */
+  int32_t reserved[6];
 } gkw_options;
 
 typedef struct gkw_stats {
@@ -80,6 +83,8 @@ typedef struct gkw_stats {
   int32_t uf_rounds[GKW_MAX_LEVELS];    /* union-find round launches, per coarsening step */
   int32_t refine_rounds[GKW_MAX_LEVELS];
   int64_t refine_moves[GKW_MAX_LEVELS];
+  int32_t balance_rounds[GKW_MAX_LEVELS];   /* per level, the coarsest included */
+  int64_t balance_moves[GKW_MAX_LEVELS];
   int64_t init_cut;
   int64_t cut;                          /* exact weighted edge cut of the output */
   int64_t max_part_weight;
@@ -155,6 +160,18 @@ gkw_status gkw_refine(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float ma
                       int32_t move_cap, int32_t* d_part, int32_t* d_boundary, int32_t* d_gain,
                       int32_t* d_target, const int32_t* d_updated, int32_t* d_pw,
                       int32_t initial_update, int32_t* rounds_out, int64_t* moves_out);
+
+/* Balance rounds on one level, in place: moves boundary vertices out of parts
+ * heavier than cap (float compare) until none is, or no move is possible.  No
+ * counterpart in the reference, which only reports an overweight part
+ * (gkway/cuda_check.hpp:105-113); gkw_partition runs it at every level when
+ * enforce_balance is set.  d_boundary must be exact for d_part; d_gain and
+ * d_target are refreshed for the vertices it touches.  d_pw[k] in-out. */
+gkw_status gkw_balance(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float cap, int32_t move_cap,
+                       int32_t* d_part, int32_t* d_boundary, int32_t* d_gain, int32_t* d_target,
+                       int32_t* d_pw, int32_t* rounds_out, int64_t* moves_out);
+/* The default-mode cap (1+eps)W/k. */
+float gkw_balance_cap(int64_t total_vwgt, int32_t k, double eps);
 
 /* Device initial partition of a (coarsest) graph: recursive bisection by greedy
  * graph growing.  Replaces the host METIS call of metis_init_partition

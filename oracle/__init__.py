@@ -35,6 +35,7 @@ class Opts(ctypes.Structure):
         ("init_method", ctypes.c_int32),
         ("init_fn", INIT_FN),
         ("init_user", ctypes.c_void_p),
+        ("enforce_balance", ctypes.c_int32),
     ]
 
 
@@ -46,6 +47,8 @@ class Result(ctypes.Structure):
         ("uf_launches", ctypes.c_int32 * MAX_LEVELS),
         ("refine_rounds", ctypes.c_int32 * MAX_LEVELS),
         ("refine_moves", ctypes.c_int64 * MAX_LEVELS),
+        ("balance_rounds", ctypes.c_int32 * MAX_LEVELS),
+        ("balance_moves", ctypes.c_int64 * MAX_LEVELS),
         ("init_cut", ctypes.c_int64),
         ("cut", ctypes.c_int64),
         ("max_part_weight", ctypes.c_int64),
@@ -174,6 +177,13 @@ def max_part_weight(total_vwgt: int, k: int, eps: float = 0.03) -> float:
     return float(lib().orc_max_part_weight(total_vwgt, k, eps))
 
 
+def balance_cap(total_vwgt: int, k: int, eps: float = 0.03) -> float:
+    L = lib()
+    L.orc_balance_cap.restype = ctypes.c_float
+    L.orc_balance_cap.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]
+    return float(L.orc_balance_cap(total_vwgt, k, eps))
+
+
 def update_vertex_info(g, k, part, updated, boundary, gain, target):
     part, updated = _c(part), _c(updated)
     boundary, gain, target = _c(boundary).copy(), _c(gain).copy(), _c(target).copy()
@@ -195,7 +205,8 @@ def refine(g, k, maxw, part, boundary, gain, target, updated, pw, move_cap=1024,
                 rounds=int(rounds), moves=int(moves.value), gain_sum=int(gsum.value))
 
 
-def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_cap=1024, eps=0.03):
+def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_cap=1024, eps=0.03,
+              enforce_balance=False):
     """Run the whole reference algorithm.
 
     ``init``: None -> the bundled METIS (the reference's initial partitioner);
@@ -207,6 +218,7 @@ def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_ca
     opts.threshold_factor = threshold_factor
     opts.move_cap = move_cap
     opts.eps = eps
+    opts.enforce_balance = int(enforce_balance)
     keep = None
     if init is None:
         if not has_metis():
@@ -217,12 +229,16 @@ def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_ca
         def cb(user, n, xadj, adjncy, adjwgt, vwgt, kk, part):
             x = np.ctypeslib.as_array(xadj, (n + 1,)).copy()
             m = int(x[-1])
-            a = np.ctypeslib.as_array(adjncy, (max(m, 1),))[:m].copy()
-            w = np.ctypeslib.as_array(adjwgt, (max(m, 1),))[:m].copy()
-            vw = np.ctypeslib.as_array(vwgt, (n,)).copy()
+            if m:
+                a = np.ctypeslib.as_array(adjncy, (m,)).copy()
+                w = np.ctypeslib.as_array(adjwgt, (m,)).copy()
+            else:
+                a = np.zeros(0, np.int32)
+                w = np.zeros(0, np.int32)
+            vw = np.ctypeslib.as_array(vwgt, (n,)).copy() if n else np.zeros(0, np.int32)
             p = np.asarray(init(x, a, w, vw, kk), dtype=np.int32)
-            out = np.ctypeslib.as_array(part, (n,))
-            out[:] = p
+            if n:
+                np.ctypeslib.as_array(part, (n,))[:] = p
             return 0
         keep = INIT_FN(cb)
         opts.init_method = 1
@@ -242,6 +258,8 @@ def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_ca
         uf_launches=list(res.uf_launches[: max(nl - 1, 0)]),
         refine_rounds=list(res.refine_rounds[: max(nl - 1, 0)]),
         refine_moves=list(res.refine_moves[: max(nl - 1, 0)]),
+        balance_rounds=list(res.balance_rounds[:nl]),
+        balance_moves=list(res.balance_moves[:nl]),
         init_cut=int(res.init_cut), cut=int(res.cut), max_part_weight=int(res.max_part_weight),
         maxw=float(res.maxw),
     )
@@ -303,3 +321,18 @@ def init_partition(g, k: int, eps: float = 0.03, seed: int = 1, trials: int = 8)
     L.orc_init_partition(g.n, _p(g.xadj), _p(g.adjncy), _p(g.adjwgt), _p(g.vwgt), int(k), float(eps),
                          int(seed), int(trials), _p(part))
     return part
+
+
+def balance(g, k, cap, part, boundary, gain, target, pw, move_cap=1024):
+    """Balance rounds alone (default mode), in the oracle."""
+    part, boundary, gain, target = (_c(a).copy() for a in (part, boundary, gain, target))
+    pw = np.ascontiguousarray(pw, dtype=np.int64).copy()
+    moves = ctypes.c_int64(0)
+    L = lib()
+    L.orc_balance.restype = ctypes.c_int32
+    L.orc_balance.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, ctypes.c_int32, ctypes.c_float,
+                              ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, _i64p, _i64p]
+    rounds = L.orc_balance(g.n, _p(g.xadj), _p(g.adjncy), _p(g.adjwgt), _p(g.vwgt), int(k), float(cap),
+                           int(move_cap), _p(part), _p(boundary), _p(gain), _p(target), _p(pw), ctypes.byref(moves))
+    return dict(part=part, boundary=boundary, gain=gain, target=target, pw=pw, rounds=int(rounds),
+                moves=int(moves.value))

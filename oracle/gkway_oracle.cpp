@@ -395,6 +395,113 @@ static i32 refine_level(RefineState& s, i32 move_cap, i64* moves, i64* gain_sum)
 }
 
 // ---------------------------------------------------------------------------
+// Balance rounds (default mode only; not in the reference, whose refinement
+// never repairs an overweight part, cuda_check.hpp:105-113 only prints it).
+// A round: every boundary vertex of an overweight part (float(pw) > cap)
+// picks the neighbouring part q != p with room (float(pw[q] + w) <= cap) that
+// maximises the signed connection gain ed_q - id (ties: smaller q); if no
+// neighbouring part has room, the lightest part (ties: smaller id) if it has
+// room, with gain ed - id.  Candidates yield to a smaller-id neighbouring
+// candidate; the rest are sorted by (gain desc, id asc), capped, and the
+// longest prefix is applied in which every move's source is still overweight
+// before the move and every destination stays within cap after it.
+// ---------------------------------------------------------------------------
+struct BalMove { i64 g; u32 v, src, des; };
+
+static i32 balance_level(RefineState& s, float cap, i32 move_cap, i64* moves_out) {
+  i32 rounds = 0;
+  std::vector<u32> ed(s.k, 0);
+  std::vector<char> seen(s.k, 0);
+  std::vector<i32> touched;
+  std::vector<char> isc(s.n, 0);
+  std::vector<u32> bt(s.n, 0);
+  std::vector<i64> bg(s.n, 0);
+  std::vector<i32> cand;
+  std::vector<BalMove> buf;
+  for (;;) {
+    // lightest part
+    u32 light = 0;
+    for (i32 p = 1; p < s.k; ++p)
+      if (s.pw[p] < s.pw[light]) light = (u32)p;
+    cand.clear();
+    for (i32 v = 0; v < s.n; ++v) {
+      isc[v] = 0;
+      const u32 p = s.part[v];
+      if (!s.boundary[v] || !((float)s.pw[p] > cap)) continue;
+      const u32 w = (u32)s.vwgt[v];
+      touched.clear();
+      u32 id = 0;
+      for (i32 e = s.xadj[v]; e < s.xadj[v + 1]; ++e) {
+        const u32 q = s.part[s.adjncy[e]];
+        if (q == p) id += (u32)s.adjwgt[e];
+        if (!seen[q]) { seen[q] = 1; ed[q] = 0; touched.push_back((i32)q); }
+        ed[q] += (u32)s.adjwgt[e];
+      }
+      bool found = false;
+      i64 bestg = 0;
+      u32 bestq = 0;
+      for (i32 q : touched) {
+        if ((u32)q == p) continue;
+        if ((float)(u32)(s.pw[q] + w) > cap) continue;
+        const i64 g = (i64)(i32)(ed[q] - id);
+        if (!found || g > bestg || (g == bestg && (u32)q < bestq)) { found = true; bestg = g; bestq = (u32)q; }
+      }
+      if (!found && light != p && !((float)(u32)(s.pw[light] + w) > cap)) {
+        found = true;
+        bestq = light;
+        bestg = (i64)(i32)((seen[light] ? ed[light] : 0u) - id);
+      }
+      for (i32 q : touched) seen[q] = 0;
+      if (!found) continue;
+      isc[v] = 1; bt[v] = bestq; bg[v] = bestg;
+      cand.push_back(v);
+    }
+    buf.clear();
+    for (i32 v : cand) {
+      bool yield = false;
+      for (i32 e = s.xadj[v]; e < s.xadj[v + 1]; ++e)
+        if (s.adjncy[e] < v && isc[s.adjncy[e]]) { yield = true; break; }
+      if (!yield) buf.push_back({bg[v], (u32)v, s.part[v], bt[v]});
+    }
+    if (buf.empty()) break;
+    std::sort(buf.begin(), buf.end(), [](const BalMove& a, const BalMove& b) {
+      if (a.g != b.g) return a.g > b.g;
+      return a.v < b.v;
+    });
+    const i32 B = (i32)std::min<size_t>(buf.size(), (size_t)move_cap);
+    std::vector<u32> outw(s.k, 0), inw(s.k, 0);
+    i32 pos = B - 1;
+    for (i32 t = 0; t < B; ++t) {
+      const u32 w = (u32)s.vwgt[buf[t].v];
+      const bool src_over = (float)(u32)(s.pw[buf[t].src] - outw[buf[t].src]) > cap;
+      const bool des_ok = !((float)(u32)(s.pw[buf[t].des] + inw[buf[t].des] + w) > cap);
+      if (!src_over || !des_ok) { pos = t - 1; break; }
+      outw[buf[t].src] += w;
+      inw[buf[t].des] += w;
+    }
+    for (i32 t = 0; t <= pos; ++t) {
+      const u32 v = buf[t].v, w = (u32)s.vwgt[v];
+      s.pw[buf[t].src] -= w;
+      s.pw[buf[t].des] += w;
+      s.part[v] = buf[t].des;
+      s.updated[v] = 1;
+      for (i32 e = s.xadj[v]; e < s.xadj[v + 1]; ++e) s.updated[s.adjncy[e]] = 1;
+    }
+    *moves_out += pos + 1;
+    ++rounds;
+    update_all_flagged(s);
+    std::fill(s.updated.begin(), s.updated.end(), 0u);
+  }
+  return rounds;
+}
+
+// Default-mode weight cap: (1 + eps) * W / k without the reference's "+1",
+// so that every part weight <= cap means balance <= 1 + eps.
+float orc_balance_cap(i64 total_vwgt, i32 k, double eps) {
+  return (float)((1.0 + eps) * (double)total_vwgt / (double)k);
+}
+
+// ---------------------------------------------------------------------------
 // Whole partitioner.  graph_partitioner.hpp:222-365 (graph_partitioner),
 // 14-123 (coarsening loop), 125-131 (init_partition), 133-220 (uncoarsening),
 // uncoarsen.hpp:325-387 (expand_partition / uncoarsen).
@@ -411,6 +518,7 @@ typedef struct {
   int (*init_fn)(void* user, i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt,
                  const i32* vwgt, i32 k, i32* part);
   void* init_user;
+  i32 enforce_balance;   // 0 = the reference's behaviour; 1 = default mode (balance rounds, cap without +1)
 } orc_opts;
 
 typedef struct {
@@ -420,6 +528,8 @@ typedef struct {
   i32 uf_launches[ORC_MAX_LEVELS];
   i32 refine_rounds[ORC_MAX_LEVELS];
   i64 refine_moves[ORC_MAX_LEVELS];
+  i32 balance_rounds[ORC_MAX_LEVELS];   // per level; index n_levels-1 = coarsest
+  i64 balance_moves[ORC_MAX_LEVELS];
   i64 init_cut;
   i64 cut;
   i64 max_part_weight;
@@ -443,7 +553,7 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
   lv[0].vwgt.assign(vwgt, vwgt + n);
   i64 total = 0;
   for (i32 v = 0; v < n; ++v) total += (u32)vwgt[v];
-  float maxw = orc_max_part_weight(total, k, opt->eps);
+  float maxw = opt->enforce_balance ? orc_balance_cap(total, k, opt->eps) : orc_max_part_weight(total, k, opt->eps);
   res->maxw = maxw;
   const i64 threshold = (i64)opt->threshold_factor * k;
 
@@ -505,6 +615,18 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
       if (part[cs.adjncy[e]] != part[v]) { boundary[v] = 1; break; }
   std::vector<u32> pw(k, 0);
   for (i32 v = 0; v < cs.n; ++v) pw[part[v]] += (u32)cs.vwgt[v];
+  if (opt->enforce_balance) {
+    RefineState s;
+    s.n = cs.n; s.k = k;
+    s.xadj = cs.xadj.data(); s.adjncy = cs.adjncy.data(); s.adjwgt = cs.adjwgt.data(); s.vwgt = cs.vwgt.data();
+    s.maxw = maxw;
+    s.part = part; s.boundary = boundary; s.pw = pw;
+    s.updated.assign(cs.n, 0); s.target = part; s.gain.assign(cs.n, 0);
+    i64 bm = 0;
+    res->balance_rounds[lv.size() - 1] = balance_level(s, maxw, opt->move_cap, &bm);
+    res->balance_moves[lv.size() - 1] = bm;
+    part.swap(s.part); boundary.swap(s.boundary); pw.swap(s.pw);
+  }
 
   // uncoarsening (graph_partitioner.hpp:174-192); no refinement at the coarsest level
   for (i32 L = (i32)lv.size() - 2; L >= 0; --L) {
@@ -525,6 +647,12 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
     }
     s.pw = pw;
     update_all_flagged(s);                               // uncoarsen.hpp:385-386
+    if (opt->enforce_balance) {
+      std::fill(s.updated.begin(), s.updated.end(), 0u);
+      i64 bm = 0;
+      res->balance_rounds[L] = balance_level(s, maxw, opt->move_cap, &bm);
+      res->balance_moves[L] = bm;
+    }
     i64 moves = 0, gsum = 0;
     i32 rounds = refine_level(s, opt->move_cap, &moves, &gsum);
     res->refine_rounds[L] = rounds;
@@ -708,5 +836,26 @@ void orc_init_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* ad
   for (i32 v = 0; v < n; ++v) part[v] = lo[v];
 }
 
+
+// Balance rounds alone on one level (per-phase check of gkw_balance).
+i32 orc_balance(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, const i32* vwgt, i32 k, float cap,
+                i32 move_cap, i32* part, i32* boundary, i32* gain, i32* target, i64* pw, i64* moves) {
+  RefineState s;
+  s.n = n; s.k = k; s.xadj = xadj; s.adjncy = adjncy; s.adjwgt = adjwgt; s.vwgt = vwgt; s.maxw = cap;
+  s.part.assign(part, part + n);
+  s.boundary.assign(boundary, boundary + n);
+  s.gain.assign(gain, gain + n);
+  s.target.assign(target, target + n);
+  s.updated.assign(n, 0);
+  s.pw.resize(k);
+  for (i32 p = 0; p < k; ++p) s.pw[p] = (u32)pw[p];
+  *moves = 0;
+  i32 rounds = balance_level(s, cap, move_cap, moves);
+  for (i32 v = 0; v < n; ++v) {
+    part[v] = (i32)s.part[v]; boundary[v] = (i32)s.boundary[v]; gain[v] = s.gain[v]; target[v] = (i32)s.target[v];
+  }
+  for (i32 p = 0; p < k; ++p) pw[p] = s.pw[p];
+  return rounds;
+}
 
 }  // extern "C"

@@ -124,18 +124,67 @@ def _gggp(orc, gen):
     return lambda x, a, w, vw, kk: orc.init_partition(gen.Csr(x, a, w, vw), kk)
 
 
+def _exact_boundary(g, part):
+    src = np.repeat(np.arange(g.n), np.diff(g.xadj))
+    diff = part[src] != part[g.adjncy]
+    b = np.zeros(g.n, np.int32)
+    np.logical_or.at(b, src[diff], True)
+    return b.astype(np.int32)
+
+
+def test_balance_level(handle, orc, pkg, cases):
+    import torch
+    rng = np.random.default_rng(12)
+    for name, g in cases:
+        for k in (4, 32):
+            part = np.minimum((np.arange(g.n) * k) // max(g.n, 1), k - 1).astype(np.int32)
+            # overload: move a block of part 1 into part 0 and a random 10% into part k-1
+            part[(part == 1) & (rng.random(g.n) < 0.5)] = 0
+            part[rng.random(g.n) < 0.1] = k - 1
+            bnd = _exact_boundary(g, part)
+            gain = np.zeros(g.n, np.int32)
+            target = part.copy()
+            pw = orc.part_weights(g, part, k)
+            cap = orc.balance_cap(int(g.vwgt.astype(np.int64).sum()), k)
+            assert cap == pkg.balance_cap(int(g.vwgt.astype(np.int64).sum()), k)
+            for mc in (1024, 7):
+                ref = orc.balance(g, k, cap, part, bnd, gain, target, pw, move_cap=mc)
+                dv = [torch.from_numpy(a.copy()).cuda() for a in (part, bnd, gain, target)]
+                dpw = torch.from_numpy(pw.astype(np.int32)).cuda()
+                rounds, moves = handle.balance(to_dev(g), k, cap, mc, dv[0], dv[1], dv[2], dv[3], dpw)
+                assert (rounds, moves) == (ref["rounds"], ref["moves"]), (name, k, mc)
+                assert np.array_equal(_np(dv[0]), ref["part"]), (name, k, mc)
+                assert np.array_equal(_np(dv[1]), ref["boundary"]), (name, k, mc)
+                assert np.array_equal(_np(dpw).astype(np.int64), ref["pw"]), (name, k, mc)
+
+
 def test_partition_device_init_matches_oracle(handle, orc, gen, cases):
+    """Default mode: device initial partition, balance rounds, strict cap."""
     for name, g in cases:
         for k in (2, 8, 64):
             part, cut, st = handle.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k)
-            ref, info = orc.partition(g, k, init=_gggp(orc, gen))
+            ref, info = orc.partition(g, k, init=_gggp(orc, gen), enforce_balance=True)
             assert np.array_equal(part, ref), (name, k)
             assert cut == info["cut"] == orc.cut(g, part), (name, k)
             assert st["level_n"] == info["level_n"] and st["level_m"] == info["level_m"], (name, k)
             assert st["uf_rounds"] == info["uf_launches"], (name, k)
             assert st["refine_rounds"] == info["refine_rounds"], (name, k)
             assert st["refine_moves"] == info["refine_moves"], (name, k)
+            assert st["balance_rounds"] == info["balance_rounds"], (name, k)
+            assert st["balance_moves"] == info["balance_moves"], (name, k)
             assert st["init_cut"] == info["init_cut"], (name, k)
+
+
+def test_partition_reference_mode_matches_oracle(handle, orc, gen, pkg, cases):
+    """The reference's own rules (MAX_PARTITION_WGT with +1, no balance rounds)."""
+    for name, g in cases:
+        for k in (8, 64):
+            o = pkg.default_options(enforce_balance=0)
+            part, cut, st = handle.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k, o)
+            ref, info = orc.partition(g, k, init=_gggp(orc, gen))
+            assert np.array_equal(part, ref), (name, k)
+            assert cut == info["cut"], (name, k)
+            assert st["refine_rounds"] == info["refine_rounds"], (name, k)
 
 
 @pytest.mark.skipif("not __import__('oracle').has_metis()")
@@ -145,7 +194,8 @@ def test_partition_metis_init_matches_oracle(handle, orc, gen, cases, pkg):
         return orc.metis_kway(gen.Csr(x, a, w, vw), kk)[0]
     for name, g in cases:
         for k in (8, 64):
-            part, cut, st = handle.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k, init=metis_init)
+            o = pkg.default_options(enforce_balance=0)
+            part, cut, st = handle.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k, o, init=metis_init)
             ref, info = orc.partition(g, k)
             assert np.array_equal(part, ref), (name, k)
             assert cut == info["cut"], (name, k)
@@ -157,9 +207,10 @@ def test_n11_fixture(handle, orc, gen, pkg):
     g = gen.Csr(x, a, w, vw)
     for k in (8, 64):
         part, cut, st = handle.partition(x, a, w, vw, k)
-        ref, info = orc.partition(g, k, init=_gggp(orc, gen))
+        ref, info = orc.partition(g, k, init=_gggp(orc, gen), enforce_balance=True)
         assert np.array_equal(part, ref)
         assert cut == info["cut"]
+        assert orc.part_weights(g, part, k).max() * k <= 1.03 * g.n
 
 
 def test_device_resident_partition_is_deterministic(handle, orc, gen):
@@ -175,7 +226,8 @@ def test_device_resident_partition_is_deterministic(handle, orc, gen):
     assert out[0][1] == orc.cut(g, out[0][0])
     pw = orc.part_weights(g, out[0][0], 64)
     assert pw.sum() == g.vwgt.sum()
-    ref, info = orc.partition(g, 64, init=_gggp(orc, gen))
+    assert pw.max() * 64 <= 1.03 * g.vwgt.sum()
+    ref, info = orc.partition(g, 64, init=_gggp(orc, gen), enforce_balance=True)
     assert np.array_equal(out[0][0], ref)
 
 
