@@ -301,6 +301,7 @@ gkw_status gkw_update_vertex_info(gkw_handle* h, const gkw_csr* d_graph, int32_t
     Handle& hh = H(h);
     DevGraph g = dev_view(d_graph);
     GKW_REQUIRE(g.m == 0 || g.adjwgt, GKW_E_INVALID, "adjwgt is NULL");
+    GKW_REQUIRE(g.n == 0 || d_updated, GKW_E_INVALID, "updated is NULL");
     hh.scratch.reset();
     check_parts(hh, g.n, d_part, k);
     RefineCtx* c = refine_create_ext(hh, g.n, k, 1024, const_cast<i32*>(d_part), d_boundary, d_gain, d_target);
@@ -308,8 +309,11 @@ gkw_status gkw_update_vertex_info(gkw_handle* h, const gkw_csr* d_graph, int32_t
       RefineCtx* c;
       ~G() { refine_destroy(c); }
     } gg{c};
-    refine_update_flagged(hh, c, g, d_updated);
-    sync(hh);
+    LevelJob j;
+    j.lists = true;
+    j.updated = d_updated;
+    level_run(hh, c, g, j, 0);
+    level_stats(hh, c, 1);
   });
 }
 
@@ -330,14 +334,15 @@ gkw_status gkw_refine(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float ma
       ~G() { refine_destroy(c); }
     } gg{c};
     GKW_CUDA(cudaMemcpyAsync(refine_pw(c), d_pw, sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
-    refine_update_flagged(hh, c, g, initial_update ? d_updated : nullptr);
-    RefineParams p;
-    p.k = k;
-    p.maxw = maxw;
-    p.move_cap = move_cap;
-    RefineLevelStats s = refine_level(hh, c, g, p);
+    LevelJob j;
+    j.lists = true;
+    j.updated = initial_update ? d_updated : nullptr;
+    j.refine = true;
+    j.maxw = maxw;
+    j.move_cap = move_cap;
+    level_run(hh, c, g, j, 0);
     GKW_CUDA(cudaMemcpyAsync(d_pw, refine_pw(c), sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
-    sync(hh);
+    RefineLevelStats s = level_stats(hh, c, 1)[0];
     if (rounds_out) *rounds_out = s.rounds;
     if (moves_out) *moves_out = s.moves;
   });
@@ -358,12 +363,16 @@ gkw_status gkw_balance(gkw_handle* h, const gkw_csr* d_graph, int32_t k, float c
       ~G() { refine_destroy(c); }
     } gg{c};
     GKW_CUDA(cudaMemcpyAsync(refine_pw(c), d_pw, sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
-    refine_update_flagged(hh, c, g, nullptr);   // empty U, P from the caller's gains
-    RefineLevelStats s = balance_level(hh, c, g, cap, move_cap);
+    LevelJob j;
+    j.lists = true;   // empty U, P from the caller's gains
+    j.balance = true;
+    j.bcap = cap;
+    j.move_cap = move_cap;
+    level_run(hh, c, g, j, 0);
     GKW_CUDA(cudaMemcpyAsync(d_pw, refine_pw(c), sizeof(i32) * k, cudaMemcpyDeviceToDevice, hh.stream));
-    sync(hh);
-    if (rounds_out) *rounds_out = s.rounds;
-    if (moves_out) *moves_out = s.moves;
+    RefineLevelStats s = level_stats(hh, c, 1)[0];
+    if (rounds_out) *rounds_out = s.brounds;
+    if (moves_out) *moves_out = s.bmoves;
   });
 }
 

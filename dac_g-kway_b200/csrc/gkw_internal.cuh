@@ -138,19 +138,32 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out)
 
 // ---- refinement (refine.cu) ----
 struct RefineCtx;   // opaque
-struct RefineParams {
-  i32 k = 2;
-  float maxw = 0.f;
-  i32 move_cap = 1024;
-};
 struct RefineLevelStats {
   i32 rounds = 0;
   i64 moves = 0;
   i64 gain_sum = 0;
+  i32 brounds = 0;
+  i64 bmoves = 0;
+};
+// One persistent launch over one level.  With cmap: project the state held in
+// the context (the coarser level) onto this level and update the gains of its
+// boundary vertices.  With lists: take the caller's state, U from `updated`,
+// P from the current gains, update U.  Then balance rounds (balance) and/or
+// refinement rounds (refine).
+struct LevelJob {
+  const i32* cmap = nullptr;
+  const i32* updated = nullptr;
+  bool lists = false;
+  bool balance = false;
+  float bcap = 0.f;
+  bool refine = false;
+  float maxw = 0.f;
+  i32 move_cap = 1024;
 };
 RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap);
+RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
+                             i32* target);
 void refine_destroy(RefineCtx* c);
-// device arrays owned by the context (n_max entries each)
 i32* refine_part(RefineCtx* c);
 i32* refine_boundary(RefineCtx* c);
 i32* refine_gain(RefineCtx* c);
@@ -158,13 +171,10 @@ i32* refine_target(RefineCtx* c);
 u32* refine_pw(RefineCtx* c);
 // Coarsest level: part given; computes boundary flags and part weights.
 void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_part_in);
-// Projects from the coarser level (state in the context) to `fine` via cmap and
-// refines `fine`.
-void refine_project(Handle& h, RefineCtx* c, const DevGraph& fine, const i32* cmap, i32 nc);
-void refine_update_flagged(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_updated);
-RefineLevelStats refine_level(Handle& h, RefineCtx* c, const DevGraph& g, const RefineParams& p);
-// Balance rounds until no part exceeds cap (or no move is possible).
-RefineLevelStats balance_level(Handle& h, RefineCtx* c, const DevGraph& g, float cap, i32 move_cap);
+void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i32 stats_slot);
+// Reads the per-level statistics of slots [0, nslots) (one host sync); throws
+// if a level kernel reported an error.
+std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots);
 // (1 + eps) * W / k, the default-mode weight cap (no "+1").
 float balance_cap(i64 total_vwgt, i32 k, double eps);
 
@@ -182,8 +192,6 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
 i64 validate(Handle& h, const DevGraph& g);   // total vertex weight; throws on malformed input
 void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
                     i64* cut_out, gkw_stats* stats);
-RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
-                             i32* target);
 const char* last_error_cstr();
 
 // ---- host helpers ----

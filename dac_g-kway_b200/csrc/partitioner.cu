@@ -163,22 +163,29 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     GKW_CUDA(cudaStreamSynchronize(h.stream));
     init_cut = h.h_pinned[0];
   }
-  std::vector<RefineLevelStats> bs(lv.size());
-  if (opt.enforce_balance) bs[lv.size() - 1] = balance_level(h, rc, cg, maxw, opt.move_cap);
+  const i32 nl = (i32)lv.size();
+  if (opt.enforce_balance) {
+    LevelJob j;
+    j.balance = true;
+    j.bcap = maxw;
+    j.move_cap = opt.move_cap;
+    level_run(h, rc, cg, j, nl - 1);
+  }
   GKW_CUDA(cudaEventRecord(tm.ev[2], h.stream));
 
-  // ---- uncoarsening (graph_partitioner.hpp:174-192) ----
-  RefineParams rp;
-  rp.k = k;
-  rp.maxw = maxw;
-  rp.move_cap = opt.move_cap;
-  std::vector<RefineLevelStats> rs(lv.size());
-  for (i32 L = (i32)lv.size() - 2; L >= 0; --L) {
-    refine_project(h, rc, lv[L].g, lv[L].cmap, lv[L + 1].g.n);
-    if (opt.enforce_balance) bs[L] = balance_level(h, rc, lv[L].g, maxw, opt.move_cap);
-    rs[L] = refine_level(h, rc, lv[L].g, rp);
+  // ---- uncoarsening (graph_partitioner.hpp:174-192): one launch per level ----
+  for (i32 L = nl - 2; L >= 0; --L) {
+    LevelJob j;
+    j.cmap = lv[L].cmap;
+    j.balance = opt.enforce_balance != 0;
+    j.bcap = maxw;
+    j.refine = true;
+    j.maxw = maxw;
+    j.move_cap = opt.move_cap;
+    level_run(h, rc, lv[L].g, j, L);
   }
   GKW_CUDA(cudaEventRecord(tm.ev[3], h.stream));
+  std::vector<RefineLevelStats> rs = level_stats(h, rc, nl);
   // ---- output and final metrics (graph_partitioner.hpp:194-202) ----
   if (g0.n) {
     GKW_CUDA(cudaMemcpyAsync(d_part_out, refine_part(rc), sizeof(i32) * g0.n, cudaMemcpyDeviceToDevice,
@@ -204,8 +211,8 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
       stats->refine_moves[i] = rs[i].moves;
     }
     for (size_t i = 0; i < lv.size(); ++i) {
-      stats->balance_rounds[i] = bs[i].rounds;
-      stats->balance_moves[i] = bs[i].moves;
+      stats->balance_rounds[i] = rs[i].brounds;
+      stats->balance_moves[i] = rs[i].bmoves;
     }
     stats->init_cut = init_cut;
     stats->cut = hm[0];

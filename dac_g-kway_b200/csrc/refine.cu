@@ -1,13 +1,22 @@
-// Projection and independent-set refinement (gkway/uncoarsen.hpp).
+// Projection, balance rounds and independent-set refinement of one level
+// (gkway/uncoarsen.hpp), as ONE persistent cooperative kernel per level.
 //
-// The reference scans every vertex of the level in each refinement round.
-// Here a round only touches two short lists: P, the vertices whose gain is
-// positive (the only ones that can move or block a neighbour), and U, the
-// vertices whose gain must be recomputed (moved vertices and their
-// neighbours).  Both lists are maintained on the device; a round is five
-// kernels and rounds are launched in batches with one host read per batch.
+// The reference runs each refinement round as ~9 launches plus 3 blocking
+// device-to-host reads and scans every vertex of the level per round.  Here a
+// level is one launch: all CTAs stay resident and step through the phases of
+// every round, separated by a grid barrier, until no move is left.  A round
+// only touches two short lists: P, the vertices whose gain is positive (the
+// only ones that can move or block a neighbour), and U, the vertices whose
+// gain must be recomputed (moved vertices and their neighbours).
+//
+// The grid barrier is a counter + generation word; a CTA that waits longer
+// than kBarrierCycles sets the error word and every CTA leaves the kernel, so
+// a fault in the round logic ends the launch with an error status instead of
+// a hang.  Data written by other CTAs within the launch is read with
+// ld.global.cg (L2, coherent) after the barrier.
 #include <algorithm>
 #include <climits>
+#include <cstring>
 
 #include "gkw_internal.cuh"
 
@@ -17,6 +26,9 @@ static constexpr u32 kFullMask = 0xffffffffu;
 constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pass
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
 constexpr i32 kBadWords = kMaxMoveCap / 32;
+constexpr int kLevelThreads = 512;
+constexpr long long kBarrierCycles = 4000000000ll;   // ~2 s at 2 GHz
+constexpr i32 kStatSlots = GKW_MAX_LEVELS + 2;
 
 struct RoundState {
   i32 pcount[2];
@@ -29,7 +41,6 @@ struct RoundState {
   i64 moves;
   i64 gain_sum;
   u32 bad[kBadWords];
-  // balance rounds
   i32 bdone;
   i32 brounds;
   i64 bmoves;
@@ -37,6 +48,18 @@ struct RoundState {
   i32 firstbad;
   i32 light;
   u32 epoch;
+};
+
+struct GridBarrier {
+  u32 count;
+  u32 gen;
+};
+
+struct LevelStatsDev {
+  i32 rounds, brounds;
+  i64 moves, gain_sum, bmoves;
+  i32 err;
+  i32 pad;
 };
 
 struct RefineCtx {
@@ -54,100 +77,63 @@ struct RefineCtx {
   u64* top = nullptr;
   u32* pw = nullptr;
   RoundState* st = nullptr;
-  i32 upd_warps = 8;
-  // balance rounds: candidate mark (round epoch), destination, gain, list
   u32* bmark = nullptr;
   i32* btarget = nullptr;
   i32* bgain = nullptr;
   i32* blist = nullptr;
-  u32* epoch = nullptr;   // never reset: the marks of earlier rounds stay stale
+  u32* epoch = nullptr;   // never reset: marks of earlier rounds stay stale
+  GridBarrier* bar = nullptr;
+  i32* err = nullptr;
+  LevelStatsDev* stats = nullptr;
+  i32 acc_warps = 16;
+  size_t smem = 0;
+  i32 grid = 0;
 };
 
-static void alloc_balance(Handle& h, Pool& P, RefineCtx* c, size_t n) {
-  c->bmark = P.alloc_n<u32>(n);
-  c->btarget = P.alloc_n<i32>(n);
-  c->bgain = P.alloc_n<i32>(n);
-  c->blist = P.alloc_n<i32>(n);
-  c->epoch = P.alloc_n<u32>(1);
-  GKW_CUDA(cudaMemsetAsync(c->bmark, 0, sizeof(u32) * n, h.stream));
-  GKW_CUDA(cudaMemsetAsync(c->epoch, 0, sizeof(u32), h.stream));
-}
+struct LevelArgs {
+  i32 n, k;
+  const i32* __restrict__ xadj;
+  const i32* __restrict__ adjncy;
+  const i32* __restrict__ adjwgt;
+  const i32* __restrict__ vwgt;
+  float maxw, bcap;
+  i32 move_cap;
+  i32 flags;
+  i64 max_rounds;
+  const i32* cmap;       // projection source
+  const i32* part_c;
+  const i32* bnd_c;
+  const i32* updated_in;
+  i32 *part, *bnd, *gain, *target, *updflag, *inP, *U, *P0, *P1;
+  u64 *cands, *top;
+  u32* pw;
+  RoundState* st;
+  u32* bmark;
+  i32 *btarget, *bgain, *blist;
+  u32* epoch;
+  GridBarrier* bar;
+  i32* err;
+  LevelStatsDev* stat_slot;
+  i32 acc_warps;
+};
 
-RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap) {
-  GKW_REQUIRE(move_cap >= 1 && move_cap <= kMaxMoveCap, GKW_E_UNSUPPORTED,
-              "move_cap must be in [1, 2048]");
-  GKW_REQUIRE(k >= 1 && k <= 12288, GKW_E_UNSUPPORTED, "k must be in [1, 12288]");
-  RefineCtx* c = new RefineCtx();
-  c->n_max = n_max;
-  c->k = k;
-  c->cap = move_cap;
-  const size_t n = std::max(n_max, 1);
-  Pool& P = h.hier;
-  c->part[0] = P.alloc_n<i32>(n);
-  c->part[1] = P.alloc_n<i32>(n);
-  c->bnd[0] = P.alloc_n<i32>(n);
-  c->bnd[1] = P.alloc_n<i32>(n);
-  c->gain = P.alloc_n<i32>(n);
-  c->target = P.alloc_n<i32>(n);
-  c->updflag = P.alloc_n<i32>(n);
-  c->inP = P.alloc_n<i32>(n);
-  c->U = P.alloc_n<i32>(n);
-  c->P[0] = P.alloc_n<i32>(n);
-  c->P[1] = P.alloc_n<i32>(n);
-  c->cands = P.alloc_n<u64>(n);
-  c->top = P.alloc_n<u64>(kMaxMoveCap);
-  c->pw = P.alloc_n<u32>(k);
-  c->st = P.alloc_n<RoundState>(1);
-  alloc_balance(h, P, c, n);
-  i32 w = (48 * 1024) / (4 * k);
-  c->upd_warps = std::max(1, std::min(8, w));
-  return c;
-}
+enum : i32 { LF_PROJECT = 1, LF_LISTS = 2, LF_UPDATE = 4, LF_BALANCE = 8, LF_REFINE = 16 };
 
-// A context over caller-owned state arrays (per-phase entry points).
-RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
-                             i32* target) {
-  GKW_REQUIRE(move_cap >= 1 && move_cap <= kMaxMoveCap, GKW_E_UNSUPPORTED,
-              "move_cap must be in [1, 2048]");
-  GKW_REQUIRE(k >= 1 && k <= 12288, GKW_E_UNSUPPORTED, "k must be in [1, 12288]");
-  RefineCtx* c = new RefineCtx();
-  c->n_max = n;
-  c->k = k;
-  c->cap = move_cap;
-  const size_t nn = std::max(n, 1);
-  Pool& P = h.scratch;
-  c->part[0] = part;
-  c->bnd[0] = bnd;
-  c->part[1] = nullptr;
-  c->bnd[1] = nullptr;
-  c->gain = gain;
-  c->target = target;
-  c->updflag = P.alloc_n<i32>(nn);
-  c->inP = P.alloc_n<i32>(nn);
-  c->U = P.alloc_n<i32>(nn);
-  c->P[0] = P.alloc_n<i32>(nn);
-  c->P[1] = P.alloc_n<i32>(nn);
-  c->cands = P.alloc_n<u64>(nn);
-  c->top = P.alloc_n<u64>(kMaxMoveCap);
-  c->pw = P.alloc_n<u32>(k);
-  c->st = P.alloc_n<RoundState>(1);
-  alloc_balance(h, P, c, nn);
-  i32 w = (48 * 1024) / (4 * k);
-  c->upd_warps = std::max(1, std::min(8, w));
-  return c;
+// ---------------------------------------------------------------------------
+// small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ i32 ldc(const i32* p) { return __ldcg(p); }
+__device__ __forceinline__ u32 ldc(const u32* p) { return __ldcg(p); }
+__device__ __forceinline__ u64 ldc(const u64* p) {
+  return (u64)__ldcg(reinterpret_cast<const unsigned long long*>(p));
 }
-
-void refine_destroy(RefineCtx* c) { delete c; }
-i32* refine_part(RefineCtx* c) { return c->part[c->cur]; }
-i32* refine_boundary(RefineCtx* c) { return c->bnd[c->cur]; }
-i32* refine_gain(RefineCtx* c) { return c->gain; }
-i32* refine_target(RefineCtx* c) { return c->target; }
-u32* refine_pw(RefineCtx* c) { return c->pw; }
+__device__ __forceinline__ i64 ldc(const i64* p) { return (i64)__ldcg(reinterpret_cast<const long long*>(p)); }
 
 // uncoarsen.hpp:10-21 (is_valid_move): (float)(u32)(dest + vwgt) > MAXW is invalid
 __device__ __forceinline__ bool valid_move(u32 dest_w, u32 vw, float maxw) {
   return !(__uint2float_rn(dest_w + vw) > maxw);
 }
+__device__ __forceinline__ bool over_cap(u32 w, float cap) { return __uint2float_rn(w) > cap; }
 
 // candidate key: ascending order = gain descending, vertex id ascending
 // (INT_MAX - gain fits in 32 bits for every int32 gain)
@@ -156,8 +142,676 @@ __device__ __forceinline__ u64 move_key(i32 gain, i32 v) {
 }
 __device__ __forceinline__ i32 key_gain(u64 key) { return (i32)((i64)INT_MAX - (i64)(u32)(key >> 32)); }
 
-static void reset_state(Handle& h, RefineCtx* c) {
-  GKW_CUDA(cudaMemsetAsync(c->st, 0, sizeof(RoundState), h.stream));
+// Warp-aggregated append: every lane of the warp calls it together.
+__device__ __forceinline__ void warp_append(bool pred, i32 val, i32* list, i32* counter) {
+  const u32 mask = __ballot_sync(kFullMask, pred);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  i32 base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(kFullMask, base, leader);
+  if (pred) list[base + __popc(mask & ((1u << lane) - 1))] = val;
+}
+__device__ __forceinline__ void warp_append64(bool pred, u64 val, u64* list, i32* counter) {
+  const u32 mask = __ballot_sync(kFullMask, pred);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  i32 base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(kFullMask, base, leader);
+  if (pred) list[base + __popc(mask & ((1u << lane) - 1))] = val;
+}
+
+// Grid barrier (all CTAs of a cooperative launch).  Returns false when any
+// CTA has timed out; the caller then leaves the kernel.
+__device__ bool grid_barrier(GridBarrier* b, i32* err, i32* s_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile u32* vgen = &b->gen;
+    const u32 g = *vgen;
+    __threadfence();
+    const u32 arrived = atomicAdd(&b->count, 1u);
+    if (arrived == gridDim.x - 1) {
+      b->count = 0;
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*vgen == g) {
+        if (clock64() - t0 > kBarrierCycles) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+    *s_flag = *(volatile i32*)err;
+  }
+  __syncthreads();
+  return *s_flag == 0;
+}
+
+// ---------------------------------------------------------------------------
+// Phases.  `base` of every grid-stride loop is warp-uniform so that warp
+// collectives run converged.
+// ---------------------------------------------------------------------------
+
+// Projection (uncoarsen.hpp:325-356, expand_partition): part and boundary
+// inherited from the coarse vertex, gain 0, target = part, boundary vertices
+// flagged for the gain update.
+__device__ void ph_project(const LevelArgs& a) {
+  const int lane = threadIdx.x & 31;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += stride) {
+    const i64 v = base + lane;
+    bool b = false;
+    if (v < a.n) {
+      const i32 c = a.cmap[v];
+      const i32 p = a.part_c[c];
+      const i32 bc = a.bnd_c[c];
+      a.part[v] = p;
+      a.bnd[v] = bc;
+      a.gain[v] = 0;
+      a.target[v] = p;
+      a.inP[v] = 0;
+      a.updflag[v] = bc ? 1 : 0;
+      b = bc != 0;
+    }
+    warp_append(b, (i32)v, a.U, &a.st->ucount);
+  }
+}
+
+// U from the caller's flags, P from the current gains (per-phase entry points).
+__device__ void ph_lists(const LevelArgs& a) {
+  const int lane = threadIdx.x & 31;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += stride) {
+    const i64 v = base + lane;
+    bool u = false, pos = false;
+    if (v < a.n) {
+      u = a.updated_in ? (a.updated_in[v] != 0) : false;
+      pos = a.gain[v] > 0;
+      a.updflag[v] = u ? 1 : 0;
+      a.inP[v] = pos ? 1 : 0;
+    }
+    warp_append(u, (i32)v, a.U, &a.st->ucount);
+    warp_append(pos, (i32)v, a.P0, &a.st->pcount[0]);
+  }
+}
+
+// Gain update (uncoarsen.hpp:175-237, update_vertex_info + calculate_gain).
+// One warp per vertex of U, per-part connection weights in a per-warp shared
+// row of k words (only touched entries are cleared afterwards).  The best part
+// is the max of the UNSIGNED value (ed - id) over neighbouring parts other
+// than the own part, ties to the smaller part id, taken only if that value is
+// > 0 -- the reference's `if (gain > max_gain)` with an unsigned max_gain.
+// Vertices whose new gain is positive join P.
+__device__ void ph_update(const LevelArgs& a, u32* acc_all) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (wid >= a.acc_warps) return;
+  u32* acc = acc_all + (size_t)wid * a.k;
+  RoundState* st = a.st;
+  const i32 nU = ldc(&st->ucount);
+  const i32 pc = ldc(&st->pcur);
+  i32* Pout = pc ? a.P1 : a.P0;
+  i32* pcount = &st->pcount[pc];
+  const i64 nw = (i64)gridDim.x * a.acc_warps;
+  for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nU; i += nw) {
+    const i32 v = ldc(a.U + i);
+    const i32 p = ldc(a.part + v);
+    const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+    bool bl = false;
+    for (i32 e = beg + lane; e < end; e += 32) {
+      const i32 q = ldc(a.part + a.adjncy[e]);
+      atomicAdd(&acc[q], (u32)a.adjwgt[e]);
+      bl |= (q != p);
+    }
+    const bool b = __any_sync(kFullMask, bl);
+    __syncwarp();
+    u32 g = 0, q_best = (u32)p;
+    if (b) {
+      const u32 id = acc[p];
+      u64 best = 0;
+      for (i32 e = beg + lane; e < end; e += 32) {
+        const i32 q = ldc(a.part + a.adjncy[e]);
+        if (q != p) {
+          const u64 key = ((u64)(acc[q] - id) << 32) | (u32)(~(u32)q);
+          best = best > key ? best : key;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const u64 ot = __shfl_xor_sync(kFullMask, best, o);
+        best = best > ot ? best : ot;
+      }
+      const u32 gb = (u32)(best >> 32);
+      if (gb > 0) { g = gb; q_best = ~(u32)best; }
+    }
+    if (lane == 0) {
+      a.updflag[v] = 0;
+      a.bnd[v] = b ? 1 : 0;
+      a.gain[v] = (i32)g;
+      a.target[v] = (i32)q_best;
+      if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) Pout[atomicAdd(pcount, 1)] = v;
+    }
+    __syncwarp();
+    for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
+    __syncwarp();
+  }
+}
+
+// Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
+// boundary, gain > 0, a valid destination by weight, and no neighbour with a
+// smaller id that is itself positive and valid.  P is compacted on the way.
+__device__ void ph_candidates(const LevelArgs& a) {
+  RoundState* st = a.st;
+  const int lane = threadIdx.x & 31;
+  const i32 pc = ldc(&st->pcur);
+  const i32 nP = ldc(&st->pcount[pc]);
+  const i32* Pin = pc ? a.P1 : a.P0;
+  i32* Pout = pc ? a.P0 : a.P1;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nP; base += stride) {
+    const i64 i = base + lane;
+    bool keep = false, cand = false;
+    i32 v = 0, g = 0;
+    if (i < nP) {
+      v = ldc(Pin + i);
+      g = ldc(a.gain + v);
+      if (g <= 0) {
+        a.inP[v] = 0;
+      } else {
+        keep = true;
+        if (ldc(a.bnd + v)) {
+          const i32 t = ldc(a.target + v);
+          if (valid_move(ldc(a.pw + t), (u32)a.vwgt[v], a.maxw)) {
+            cand = true;
+            for (i32 e = a.xadj[v]; e < a.xadj[v + 1]; ++e) {
+              const i32 u = a.adjncy[e];
+              if (u < v && ldc(a.gain + u) > 0 &&
+                  valid_move(ldc(a.pw + ldc(a.target + u)), (u32)a.vwgt[u], a.maxw)) {
+                cand = false;
+                break;
+              }
+            }
+          }
+        }
+      }
+    }
+    warp_append(keep, v, Pout, &st->pcount[pc ^ 1]);
+    warp_append64(cand, move_key(g, v), a.cands, &st->ccount);
+  }
+}
+
+// Sort the candidates by (gain desc, id asc) and keep the first min(cnt, cap)
+// (uncoarsen.hpp:471-476 with move_request.hpp:36-41).  Block 0 only; more than
+// kSortMax candidates are streamed through shared memory keeping the running
+// top `cap`.  Resets the per-round counters.
+__device__ void ph_select(const LevelArgs& a, u64* s, bool balance_mode) {
+  if (blockIdx.x != 0) return;
+  RoundState* st = a.st;
+  const i32 cnt = ldc(&st->ccount);
+  if (cnt == 0) {
+    if (threadIdx.x == 0) {
+      if (balance_mode) st->bdone = 1;
+      else st->done = 1;
+    }
+    return;
+  }
+  const i32 cap = a.move_cap;
+  const i32 B = cnt < cap ? cnt : cap;
+  auto bitonic = [&](i32 P) {
+    for (i32 kk = 2; kk <= P; kk <<= 1)
+      for (i32 j = kk >> 1; j > 0; j >>= 1) {
+        for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
+          const i32 l = i ^ j;
+          if (l > i) {
+            const u64 x = s[i], y = s[l];
+            const bool up = (i & kk) == 0;
+            if (up ? (x > y) : (x < y)) { s[i] = y; s[l] = x; }
+          }
+        }
+        __syncthreads();
+      }
+  };
+  if (cnt <= kSortMax) {
+    i32 P = 32;
+    while (P < cnt) P <<= 1;
+    for (i32 i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cnt ? ldc(a.cands + i) : ~0ull;
+    __syncthreads();
+    bitonic(P);
+  } else {
+    i32 next = 0;
+    bool first = true;
+    while (next < cnt) {
+      const i32 lo = first ? 0 : cap;
+      for (i32 i = lo + threadIdx.x; i < kSortMax; i += blockDim.x) {
+        const i32 src = next + (i - lo);
+        s[i] = src < cnt ? ldc(a.cands + src) : ~0ull;
+      }
+      next += kSortMax - lo;
+      first = false;
+      __syncthreads();
+      bitonic(kSortMax);
+    }
+  }
+  for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
+  if (!balance_mode)
+    for (i32 i = threadIdx.x; i < (B + 31) / 32; i += blockDim.x) st->bad[i] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st->B = B;
+    st->ccount = 0;
+    st->ucount = 0;
+    if (balance_mode) {
+      st->firstbad = B;
+    } else {
+      st->pcount[st->pcur] = 0;
+      st->pcur ^= 1;
+    }
+  }
+}
+
+// Block-wide exclusive scan of one u32 per thread (blockDim <= 1024).
+__device__ __forceinline__ u32 block_exscan_u32(u32 x, u32* s_warp, u32& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  u32 inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(kFullMask, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_warp[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    const u32 w = lane < nw ? s_warp[lane] : 0;
+    u32 wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 y = __shfl_up_sync(kFullMask, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < nw) s_warp[lane] = wi - w;
+    if (lane == nw - 1) s_warp[32] = wi;
+  }
+  __syncthreads();
+  const u32 r = inc - x + s_warp[wid];
+  total = s_warp[32];
+  __syncthreads();
+  return r;
+}
+
+constexpr int kIT = kMaxMoveCap / kLevelThreads;   // moves per thread in the per-part checks
+
+// Refinement balance check (uncoarsen.hpp:239-288): part p's weight change
+// prefix over the sorted moves; every prefix index j whose change is positive
+// and pushes p over MAXW is flagged.  A prefix is balanced when no part flags it.
+__device__ void ph_check_refine(const LevelArgs& a, u32* s_warp) {
+  RoundState* st = a.st;
+  const i32 B = ldc(&st->B);
+  for (i32 p = blockIdx.x; p < a.k; p += gridDim.x) {
+    i32 e[kIT];
+    i32 sum = 0;
+#pragma unroll
+    for (int i = 0; i < kIT; ++i) {
+      const i32 j = threadIdx.x * kIT + i;
+      i32 d = 0;
+      if (j < B) {
+        const i32 v = (i32)(u32)ldc(a.top + j);
+        const i32 w = a.vwgt[v];
+        if (ldc(a.target + v) == p) d += w;
+        if (ldc(a.part + v) == p) d -= w;
+      }
+      e[i] = d;
+      sum += d;
+    }
+    u32 tot;
+    i32 run = (i32)block_exscan_u32((u32)sum, s_warp, tot);
+    const u32 base = ldc(a.pw + p);
+#pragma unroll
+    for (int i = 0; i < kIT; ++i) {
+      const i32 j = threadIdx.x * kIT + i;
+      run += e[i];
+      if (j < B && run > 0 && __uint2float_rn((u32)run + base) > a.maxw) atomicOr(&st->bad[j >> 5], 1u << (j & 31));
+    }
+  }
+}
+
+// Apply the moves 0..pos, pos = the largest balanced prefix index
+// (uncoarsen.hpp:284-286 keep the max balanced index; prefix 0 is always
+// balanced).  Part weights change by the same sums as pw[p] += D[p][pos]; moved
+// vertices and their neighbours are flagged and appended to U
+// (uncoarsen.hpp:290-323).  One warp per move.
+__device__ void ph_apply_refine(const LevelArgs& a) {
+  RoundState* st = a.st;
+  const i32 B = ldc(&st->B);
+  i32 pos = 0;
+  const i32 nwords = (B + 31) >> 5;
+  for (i32 w = nwords - 1; w >= 0; --w) {
+    u32 valid = kFullMask;
+    if (w == nwords - 1 && (B & 31)) valid = (1u << (B & 31)) - 1;
+    const u32 zeros = ~ldc(&st->bad[w]) & valid;
+    if (zeros) {
+      pos = w * 32 + 31 - __clz(zeros);
+      break;
+    }
+  }
+  const int lane = threadIdx.x & 31;
+  const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  if (warp == 0 && lane == 0) {
+    st->rounds += 1;
+    st->moves += pos + 1;
+  }
+  for (i64 j = warp; j <= pos; j += nwarps) {
+    const u64 key = ldc(a.top + j);
+    const i32 v = (i32)(u32)key;
+    const i32 s = ldc(a.part + v), d = ldc(a.target + v);
+    if (lane == 0) {
+      const u32 w = (u32)a.vwgt[v];
+      atomicAdd(&a.pw[d], w);
+      atomicSub(&a.pw[s], w);
+      a.part[v] = d;
+      atomicAdd((unsigned long long*)&st->gain_sum, (unsigned long long)(i64)key_gain(key));
+    }
+    const bool first = lane == 0 && atomicExch(&a.updflag[v], 1) == 0;
+    warp_append(first, v, a.U, &st->ucount);
+    const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+    for (i32 e0 = beg; e0 < end; e0 += 32) {
+      const i32 e = e0 + lane;
+      bool add = false;
+      i32 u = 0;
+      if (e < end) {
+        u = a.adjncy[e];
+        add = atomicExch(&a.updflag[u], 1) == 0;
+      }
+      warp_append(add, u, a.U, &st->ucount);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Balance rounds (default mode; the reference has none -- an overweight part
+// is only reported, cuda_check.hpp:105-113).
+//   prep      lightest part (ties: smaller id), new round epoch   (block 0)
+//   eval      boundary vertices of overweight parts: best neighbouring part
+//             with room by signed gain ed_q - id (ties: smaller q), else the
+//             lightest part if it has room; marks candidates
+//   emit      candidates without a smaller-id candidate neighbour -> keys
+//   select    sort by (gain desc, id asc), cap
+//   check     per part: first move index whose source is no longer
+//             overweight before it or whose destination overflows
+//   apply     the prefix before that index, flag U; then the gain update
+// ---------------------------------------------------------------------------
+__device__ void ph_bal_prep(const LevelArgs& a, u64* s_tmp) {
+  if (blockIdx.x != 0) return;
+  u64 best = ~0ull;
+  for (i32 p = threadIdx.x; p < a.k; p += blockDim.x) {
+    const u64 key = ((u64)ldc(a.pw + p) << 32) | (u32)p;
+    best = key < best ? key : best;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const u64 y = __shfl_xor_sync(kFullMask, best, o);
+    best = y < best ? y : best;
+  }
+  if ((threadIdx.x & 31) == 0) s_tmp[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) best = s_tmp[w] < best ? s_tmp[w] : best;
+    a.st->light = (i32)(u32)best;
+    a.st->epoch = ++(*a.epoch);
+    a.st->lcount = 0;
+  }
+  __syncthreads();
+}
+
+__device__ void ph_bal_eval(const LevelArgs& a, u32* acc_all) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (wid >= a.acc_warps) return;
+  u32* acc = acc_all + (size_t)wid * a.k;
+  RoundState* st = a.st;
+  const u32 ep = ldc(&st->epoch);
+  const i32 light = ldc(&st->light);
+  const float cap = a.bcap;
+  const i64 nw = (i64)gridDim.x * a.acc_warps;
+  for (i64 chunk = (i64)blockIdx.x * a.acc_warps + wid; chunk * 32 < a.n; chunk += nw) {
+    const i64 v0 = chunk * 32 + lane;
+    bool want = false;
+    if (v0 < a.n) want = ldc(a.bnd + v0) && over_cap(ldc(a.pw + ldc(a.part + v0)), cap);
+    u32 mask = __ballot_sync(kFullMask, want);
+    while (mask) {
+      const int bit = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const i32 v = (i32)(chunk * 32 + bit);
+      const i32 p = ldc(a.part + v);
+      const u32 w = (u32)a.vwgt[v];
+      const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+      for (i32 e = beg + lane; e < end; e += 32) atomicAdd(&acc[ldc(a.part + a.adjncy[e])], (u32)a.adjwgt[e]);
+      __syncwarp();
+      const u32 id = acc[p];
+      u64 best = 0;
+      for (i32 e = beg + lane; e < end; e += 32) {
+        const i32 q = ldc(a.part + a.adjncy[e]);
+        if (q == p || over_cap(ldc(a.pw + q) + w, cap)) continue;
+        const i32 g = (i32)(acc[q] - id);
+        const u64 key = (1ull << 63) | ((u64)((u32)g ^ 0x80000000u) << 31) | (u64)(0x7fffffffu - (u32)q);
+        best = best > key ? best : key;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const u64 y = __shfl_xor_sync(kFullMask, best, o);
+        best = best > y ? best : y;
+      }
+      i32 q_best = -1, g_best = 0;
+      if (best) {
+        q_best = (i32)(0x7fffffffu - (u32)(best & 0x7fffffffu));
+        g_best = (i32)((u32)(best >> 31) ^ 0x80000000u);
+      } else if (light != p && !over_cap(ldc(a.pw + light) + w, cap)) {
+        q_best = light;
+        g_best = (i32)(acc[light] - id);
+      }
+      if (lane == 0 && q_best >= 0) {
+        a.bmark[v] = ep;
+        a.btarget[v] = q_best;
+        a.bgain[v] = g_best;
+        a.blist[atomicAdd(&st->lcount, 1)] = v;
+      }
+      __syncwarp();
+      for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
+      __syncwarp();
+    }
+  }
+}
+
+__device__ void ph_bal_emit(const LevelArgs& a) {
+  RoundState* st = a.st;
+  const int lane = threadIdx.x & 31;
+  const i32 nl = ldc(&st->lcount);
+  const u32 ep = ldc(&st->epoch);
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nl; base += stride) {
+    const i64 i = base + lane;
+    bool emit = false;
+    i32 v = 0, g = 0;
+    if (i < nl) {
+      v = ldc(a.blist + i);
+      g = ldc(a.bgain + v);
+      emit = true;
+      for (i32 e = a.xadj[v]; e < a.xadj[v + 1]; ++e) {
+        const i32 u = a.adjncy[e];
+        if (u < v && ldc(a.bmark + u) == ep) { emit = false; break; }
+      }
+    }
+    warp_append64(emit, move_key(g, v), a.cands, &st->ccount);
+  }
+}
+
+// Part p: exclusive prefix of weight leaving p, inclusive prefix of weight
+// entering p, over the sorted moves; the first move that leaves p while p is
+// no longer overweight, or enters p beyond the cap, bounds the applied prefix.
+__device__ void ph_check_balance(const LevelArgs& a, u32* s_warp) {
+  RoundState* st = a.st;
+  const i32 B = ldc(&st->B);
+  const float cap = a.bcap;
+  for (i32 p = blockIdx.x; p < a.k; p += gridDim.x) {
+    u32 o_e[kIT], i_e[kIT];
+    bool o_f[kIT], i_f[kIT];
+    u32 so = 0, si = 0;
+#pragma unroll
+    for (int i = 0; i < kIT; ++i) {
+      const i32 j = threadIdx.x * kIT + i;
+      o_e[i] = 0;
+      i_e[i] = 0;
+      o_f[i] = false;
+      i_f[i] = false;
+      if (j < B) {
+        const i32 v = (i32)(u32)ldc(a.top + j);
+        const u32 w = (u32)a.vwgt[v];
+        if (ldc(a.part + v) == p) { o_e[i] = w; o_f[i] = true; }
+        if (ldc(a.btarget + v) == p) { i_e[i] = w; i_f[i] = true; }
+      }
+      so += o_e[i];
+      si += i_e[i];
+    }
+    u32 t1, t2;
+    u32 out_ex = block_exscan_u32(so, s_warp, t1);
+    u32 in_in = block_exscan_u32(si, s_warp, t2);
+    const u32 base = ldc(a.pw + p);
+    i32 first = INT_MAX;
+#pragma unroll
+    for (int i = 0; i < kIT; ++i) {
+      const i32 j = threadIdx.x * kIT + i;
+      in_in += i_e[i];
+      if (j < B) {
+        if (o_f[i] && !over_cap(base - out_ex, cap)) first = j < first ? j : first;
+        if (i_f[i] && over_cap(base + in_in, cap)) first = j < first ? j : first;
+      }
+      out_ex += o_e[i];
+    }
+    if (first != INT_MAX) atomicMin(&st->firstbad, first);
+  }
+}
+
+__device__ void ph_apply_balance(const LevelArgs& a) {
+  RoundState* st = a.st;
+  const i32 pos = ldc(&st->firstbad) - 1;
+  const int lane = threadIdx.x & 31;
+  const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  if (warp == 0 && lane == 0) {
+    st->brounds += 1;
+    st->bmoves += pos + 1;
+  }
+  for (i64 j = warp; j <= pos; j += nwarps) {
+    const i32 v = (i32)(u32)ldc(a.top + j);
+    const i32 s = ldc(a.part + v), d = ldc(a.btarget + v);
+    if (lane == 0) {
+      const u32 w = (u32)a.vwgt[v];
+      atomicAdd(&a.pw[d], w);
+      atomicSub(&a.pw[s], w);
+      a.part[v] = d;
+    }
+    const bool first = lane == 0 && atomicExch(&a.updflag[v], 1) == 0;
+    warp_append(first, v, a.U, &st->ucount);
+    const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+    for (i32 e0 = beg; e0 < end; e0 += 32) {
+      const i32 e = e0 + lane;
+      bool add = false;
+      i32 u = 0;
+      if (e < end) {
+        u = a.adjncy[e];
+        add = atomicExch(&a.updflag[u], 1) == 0;
+      }
+      warp_append(add, u, a.U, &st->ucount);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The level kernel.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  u64* s_sort = reinterpret_cast<u64*>(smem_raw);                  // kSortMax u64
+  u32* acc_all = reinterpret_cast<u32*>(smem_raw + kSortMax * 8);  // acc_warps * k u32
+  __shared__ u32 s_warp[33];
+  __shared__ u64 s_tmp[32];
+  __shared__ i32 s_flag;
+  {
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (wid < a.acc_warps)
+      for (i32 q = lane; q < a.k; q += 32) acc_all[(size_t)wid * a.k + q] = 0;
+  }
+  __syncthreads();
+  RoundState* st = a.st;
+  if (a.flags & LF_PROJECT) {
+    ph_project(a);
+    if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  }
+  if (a.flags & LF_LISTS) {
+    ph_lists(a);
+    if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  }
+  if (a.flags & LF_UPDATE) ph_update(a, acc_all);
+  if (a.flags & LF_BALANCE) ph_bal_prep(a, s_tmp);
+  if (a.flags & (LF_UPDATE | LF_BALANCE)) {
+    if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  }
+  if (a.flags & LF_BALANCE) {
+    for (i64 r = 0;; ++r) {
+      if (r > a.max_rounds) {   // uniform: every CTA counts the same rounds
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 2);
+        return;
+      }
+      ph_bal_eval(a, acc_all);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_bal_emit(a);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_select(a, s_sort, true);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      if (ldc(&st->bdone)) break;
+      ph_check_balance(a, s_warp);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_apply_balance(a);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_update(a, acc_all);
+      ph_bal_prep(a, s_tmp);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    }
+  }
+  if (a.flags & LF_REFINE) {
+    for (i64 r = 0;; ++r) {
+      if (r > a.max_rounds) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 3);
+        return;
+      }
+      ph_candidates(a);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_select(a, s_sort, false);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      if (ldc(&st->done)) break;
+      ph_check_refine(a, s_warp);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_apply_refine(a);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      ph_update(a, acc_all);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    LevelStatsDev* o = a.stat_slot;
+    o->rounds = ldc(&st->rounds);
+    o->moves = ldc(&st->moves);
+    o->gain_sum = ldc(&st->gain_sum);
+    o->brounds = ldc(&st->brounds);
+    o->bmoves = ldc(&st->bmoves);
+    o->err = *(volatile i32*)a.err;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -182,14 +836,91 @@ __global__ void k_copy_i32(i32 n, const i32* __restrict__ src, i32* __restrict__
   if (v < n) dst[v] = src[v];
 }
 
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
+  c->updflag = P.alloc_n<i32>(n);
+  c->inP = P.alloc_n<i32>(n);
+  c->U = P.alloc_n<i32>(n);
+  c->P[0] = P.alloc_n<i32>(n);
+  c->P[1] = P.alloc_n<i32>(n);
+  c->cands = P.alloc_n<u64>(n);
+  c->top = P.alloc_n<u64>(kMaxMoveCap);
+  c->pw = P.alloc_n<u32>(c->k);
+  c->st = P.alloc_n<RoundState>(1);
+  c->bmark = P.alloc_n<u32>(n);
+  c->btarget = P.alloc_n<i32>(n);
+  c->bgain = P.alloc_n<i32>(n);
+  c->blist = P.alloc_n<i32>(n);
+  c->epoch = P.alloc_n<u32>(1);
+  c->bar = P.alloc_n<GridBarrier>(1);
+  c->err = P.alloc_n<i32>(1);
+  c->stats = P.alloc_n<LevelStatsDev>(kStatSlots);
+  GKW_CUDA(cudaMemsetAsync(c->bmark, 0, sizeof(u32) * n, h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->epoch, 0, sizeof(u32), h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(GridBarrier), h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->err, 0, sizeof(i32), h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->stats, 0, sizeof(LevelStatsDev) * kStatSlots, h.stream));
+  // per-warp part-connection rows: as many warps as fit beside the sort buffer
+  const size_t budget = 160 * 1024;
+  const i32 w = (i32)std::min<size_t>(kLevelThreads / 32, budget / (4 * (size_t)c->k));
+  c->acc_warps = std::max(1, w);
+  c->smem = (size_t)kSortMax * 8 + (size_t)c->acc_warps * c->k * 4;
+  GKW_CUDA(cudaFuncSetAttribute(k_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+  int bps = 0;
+  GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_level, kLevelThreads, c->smem));
+  GKW_REQUIRE(bps >= 1, GKW_E_UNSUPPORTED, "level kernel does not fit on an SM");
+  c->grid = h.sm_count * std::min(bps, 2);
+}
+
+RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap) {
+  GKW_REQUIRE(move_cap >= 1 && move_cap <= kMaxMoveCap, GKW_E_UNSUPPORTED, "move_cap must be in [1, 2048]");
+  GKW_REQUIRE(k >= 1 && k <= 40000, GKW_E_UNSUPPORTED, "k must be in [1, 40000]");
+  RefineCtx* c = new RefineCtx();
+  c->n_max = n_max;
+  c->k = k;
+  c->cap = move_cap;
+  const size_t n = std::max(n_max, 1);
+  Pool& P = h.hier;
+  c->part[0] = P.alloc_n<i32>(n);
+  c->part[1] = P.alloc_n<i32>(n);
+  c->bnd[0] = P.alloc_n<i32>(n);
+  c->bnd[1] = P.alloc_n<i32>(n);
+  c->gain = P.alloc_n<i32>(n);
+  c->target = P.alloc_n<i32>(n);
+  ctx_common(h, P, c, n);
+  return c;
+}
+
+// A context over caller-owned state arrays (per-phase entry points).
+RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
+                             i32* target) {
+  GKW_REQUIRE(move_cap >= 1 && move_cap <= kMaxMoveCap, GKW_E_UNSUPPORTED, "move_cap must be in [1, 2048]");
+  GKW_REQUIRE(k >= 1 && k <= 40000, GKW_E_UNSUPPORTED, "k must be in [1, 40000]");
+  RefineCtx* c = new RefineCtx();
+  c->n_max = n;
+  c->k = k;
+  c->cap = move_cap;
+  c->part[0] = part;
+  c->bnd[0] = bnd;
+  c->gain = gain;
+  c->target = target;
+  ctx_common(h, h.scratch, c, std::max(n, 1));
+  return c;
+}
+
+void refine_destroy(RefineCtx* c) { delete c; }
+i32* refine_part(RefineCtx* c) { return c->part[c->cur]; }
+i32* refine_boundary(RefineCtx* c) { return c->bnd[c->cur]; }
+i32* refine_gain(RefineCtx* c) { return c->gain; }
+i32* refine_target(RefineCtx* c) { return c->target; }
+u32* refine_pw(RefineCtx* c) { return c->pw; }
+
 void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_part_in) {
   c->cur = 0;
-  reset_state(h, c);
   GKW_CUDA(cudaMemsetAsync(c->pw, 0, sizeof(u32) * c->k, h.stream));
   if (g.n == 0) return;
-  GKW_CUDA(cudaMemsetAsync(c->updflag, 0, sizeof(i32) * g.n, h.stream));
-  GKW_CUDA(cudaMemsetAsync(c->inP, 0, sizeof(i32) * g.n, h.stream));
-  GKW_CUDA(cudaMemsetAsync(c->gain, 0, sizeof(i32) * g.n, h.stream));
   const u32 nb = ceil_div(g.n, 256);
   if (d_part_in != c->part[0]) {
     launch(k_copy_i32, nb, 256, 0, h.stream, g.n, d_part_in, c->part[0]);
@@ -197,702 +928,137 @@ void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32*
   }
   launch(k_boundary_pw, nb, 256, 0, h.stream, g.n, g.xadj, g.adjncy, g.vwgt, c->part[0], c->bnd[0], c->pw);
   GKW_CHECK_LAUNCH();
+  GKW_CUDA(cudaMemsetAsync(c->updflag, 0, sizeof(i32) * g.n, h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->inP, 0, sizeof(i32) * g.n, h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->gain, 0, sizeof(i32) * g.n, h.stream));
 }
 
-// ---------------------------------------------------------------------------
-// Projection (uncoarsen.hpp:325-356, expand_partition): part and boundary
-// inherited from the coarse vertex, gain 0, target = part, boundary vertices
-// flagged for update (appended to U).
-// ---------------------------------------------------------------------------
-__global__ void k_project(i32 n, const i32* __restrict__ cmap, const i32* __restrict__ part_c,
-                          const i32* __restrict__ bnd_c, i32* __restrict__ part_f, i32* __restrict__ bnd_f,
-                          i32* __restrict__ gain, i32* __restrict__ target, i32* __restrict__ updflag,
-                          i32* __restrict__ inP, i32* __restrict__ U, RoundState* __restrict__ st) {
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  const i32 c = cmap[v];
-  const i32 p = part_c[c];
-  const i32 b = bnd_c[c];
-  part_f[v] = p;
-  bnd_f[v] = b;
-  gain[v] = 0;
-  target[v] = p;
-  inP[v] = 0;
-  updflag[v] = b ? 1 : 0;
-  if (b) U[atomicAdd(&st->ucount, 1)] = (i32)v;
+void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i32 slot) {
+  GKW_REQUIRE(j.move_cap >= 1 && j.move_cap <= c->cap, GKW_E_INVALID, "move_cap out of range");
+  GKW_REQUIRE(slot >= 0 && slot < kStatSlots, GKW_E_INTERNAL, "stats slot out of range");
+  GKW_CUDA(cudaMemsetAsync(c->st, 0, sizeof(RoundState), h.stream));
+  // barrier words start from zero for every launch; an error of an earlier
+  // level stays in c->err, so every later level leaves at its first barrier
+  GKW_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(GridBarrier), h.stream));
+  LevelArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n = g.n;
+  a.k = c->k;
+  a.xadj = g.xadj;
+  a.adjncy = g.adjncy;
+  a.adjwgt = g.adjwgt;
+  a.vwgt = g.vwgt;
+  a.maxw = j.maxw;
+  a.bcap = j.bcap;
+  a.move_cap = j.move_cap;
+  a.max_rounds = 4 * (i64)g.n + 64;
+  i32 flags = 0;
+  const i32 src = c->cur;
+  i32 dst = c->cur;
+  if (j.cmap) {
+    flags |= LF_PROJECT | LF_UPDATE;
+    dst = c->cur ^ 1;
+    a.cmap = j.cmap;
+    a.part_c = c->part[src];
+    a.bnd_c = c->bnd[src];
+  }
+  if (j.lists) {
+    flags |= LF_LISTS | LF_UPDATE;
+    a.updated_in = j.updated;
+  }
+  if (j.balance) flags |= LF_BALANCE;
+  if (j.refine) flags |= LF_REFINE;
+  a.flags = flags;
+  a.part = c->part[dst];
+  a.bnd = c->bnd[dst];
+  a.gain = c->gain;
+  a.target = c->target;
+  a.updflag = c->updflag;
+  a.inP = c->inP;
+  a.U = c->U;
+  a.P0 = c->P[0];
+  a.P1 = c->P[1];
+  a.cands = c->cands;
+  a.top = c->top;
+  a.pw = c->pw;
+  a.st = c->st;
+  a.bmark = c->bmark;
+  a.btarget = c->btarget;
+  a.bgain = c->bgain;
+  a.blist = c->blist;
+  a.epoch = c->epoch;
+  a.bar = c->bar;
+  a.err = c->err;
+  a.stat_slot = c->stats + slot;
+  a.acc_warps = c->acc_warps;
+  void* args[] = {&a};
+  GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_level, dim3(c->grid), dim3(kLevelThreads), args, c->smem,
+                                       h.stream));
+  count_launch();
+  c->cur = dst;
 }
 
-// ---------------------------------------------------------------------------
-// Gain update (uncoarsen.hpp:175-237, update_vertex_info + calculate_gain).
-// One warp per vertex of U.  Per-part connection weights accumulate in a
-// per-warp shared array of k words (only the touched entries are cleared
-// afterwards).  The best part is the max of the UNSIGNED value (ed - id)
-// over neighbouring parts other than the own part, ties to the smaller part
-// id, and it is taken only if that unsigned value is > 0 -- the reference's
-// `if (gain > max_gain)` with an unsigned max_gain.  Vertices whose new gain
-// is positive join P.
-// ---------------------------------------------------------------------------
-__global__ void k_update(const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
-                         const i32* __restrict__ adjwgt, i32 k, const i32* __restrict__ part,
-                         i32* __restrict__ bnd, i32* __restrict__ gain, i32* __restrict__ target,
-                         i32* __restrict__ updflag, i32* __restrict__ inP, const i32* __restrict__ U,
-                         i32* __restrict__ P0, i32* __restrict__ P1, RoundState* __restrict__ st) {
-  extern __shared__ u32 acc_all[];
-  if (st->done || st->bdone == 1) return;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int wpb = blockDim.x >> 5;
-  u32* acc = acc_all + (size_t)wid * k;
-  for (i32 q = lane; q < k; q += 32) acc[q] = 0;
-  __syncwarp();
-  const i32 nU = st->ucount;
-  i32* Pout = st->pcur ? P1 : P0;
-  i32* pcount = &st->pcount[st->pcur];
-  const i64 nw = (i64)gridDim.x * wpb;
-  for (i64 i = (i64)blockIdx.x * wpb + wid; i < nU; i += nw) {
-    const i32 v = U[i];
-    const i32 p = part[v];
-    const i32 beg = xadj[v], end = xadj[v + 1];
-    bool bl = false;
-    for (i32 e = beg + lane; e < end; e += 32) {
-      const i32 q = part[adjncy[e]];
-      atomicAdd(&acc[q], (u32)adjwgt[e]);
-      bl |= (q != p);
-    }
-    const bool b = __any_sync(kFullMask, bl);
-    __syncwarp();
-    u32 g = 0, q_best = (u32)p;
-    if (b) {
-      const u32 id = acc[p];
-      u64 best = 0;
-      for (i32 e = beg + lane; e < end; e += 32) {
-        const i32 q = part[adjncy[e]];
-        if (q != p) {
-          const u64 key = ((u64)(acc[q] - id) << 32) | (u32)(~(u32)q);
-          best = best > key ? best : key;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const u64 ot = __shfl_xor_sync(kFullMask, best, o);
-        best = best > ot ? best : ot;
-      }
-      const u32 gb = (u32)(best >> 32);
-      if (gb > 0) { g = gb; q_best = ~(u32)best; }
-    }
-    if (lane == 0) {
-      updflag[v] = 0;
-      bnd[v] = b ? 1 : 0;
-      gain[v] = (i32)g;
-      target[v] = (i32)q_best;
-      if ((i32)g > 0 && atomicExch(&inP[v], 1) == 0) Pout[atomicAdd(pcount, 1)] = v;
-    }
-    __syncwarp();
-    for (i32 e = beg + lane; e < end; e += 32) acc[part[adjncy[e]]] = 0;
-    __syncwarp();
+std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots) {
+  GKW_REQUIRE(nslots >= 0 && nslots <= kStatSlots, GKW_E_INTERNAL, "stats slot out of range");
+  std::vector<LevelStatsDev> d((size_t)std::max(nslots, 1));
+  if (nslots) {
+    GKW_CUDA(cudaMemcpyAsync(d.data(), c->stats, sizeof(LevelStatsDev) * nslots, cudaMemcpyDeviceToHost,
+                             h.stream));
   }
-}
-
-// ---------------------------------------------------------------------------
-// Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
-// boundary, gain > 0, a valid destination by weight, and no neighbour with a
-// smaller id that is itself positive and valid.  P is compacted on the way
-// (entries whose gain is no longer positive leave it).
-// ---------------------------------------------------------------------------
-__global__ void k_candidates(const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
-                             const i32* __restrict__ vwgt, const i32* __restrict__ part,
-                             const i32* __restrict__ bnd, const i32* __restrict__ gain,
-                             const i32* __restrict__ target, const u32* __restrict__ pw, float maxw,
-                             i32* __restrict__ inP, i32* __restrict__ P0, i32* __restrict__ P1,
-                             u64* __restrict__ cands, RoundState* __restrict__ st) {
-  if (st->done) return;
-  const i32 pc = st->pcur;
-  const i32 nP = st->pcount[pc];
-  const i32* Pin = pc ? P1 : P0;
-  i32* Pout = pc ? P0 : P1;
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < nP; i += (i64)gridDim.x * blockDim.x) {
-    const i32 v = Pin[i];
-    const i32 g = gain[v];
-    if (g <= 0) {
-      inP[v] = 0;
-      continue;
-    }
-    Pout[atomicAdd(&st->pcount[pc ^ 1], 1)] = v;
-    if (!bnd[v]) continue;
-    const i32 t = target[v];
-    if (!valid_move(pw[t], (u32)vwgt[v], maxw)) continue;
-    bool yield = false;
-    for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
-      const i32 u = adjncy[e];
-      if (u < v && gain[u] > 0 && valid_move(pw[target[u]], (u32)vwgt[u], maxw)) {
-        yield = true;
-        break;
-      }
-    }
-    if (!yield) cands[atomicAdd(&st->ccount, 1)] = move_key(g, v);
+  GKW_CUDA(cudaMemcpyAsync(h.h_pinned, c->err, sizeof(i32), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  const i32 err = *(i32*)h.h_pinned;
+  if (err == 1) throw Error{GKW_E_INTERNAL, "level kernel: grid barrier timed out"};
+  if (err == 2) throw Error{GKW_E_INTERNAL, "balancing did not terminate"};
+  if (err == 3) throw Error{GKW_E_INTERNAL, "refinement did not terminate"};
+  std::vector<RefineLevelStats> out((size_t)nslots);
+  for (i32 i = 0; i < nslots; ++i) {
+    out[i].rounds = d[i].rounds;
+    out[i].moves = d[i].moves;
+    out[i].gain_sum = d[i].gain_sum;
+    out[i].brounds = d[i].brounds;
+    out[i].bmoves = d[i].bmoves;
   }
-}
-
-// ---------------------------------------------------------------------------
-// Sort the candidates by (gain desc, id asc) and keep the first min(cnt, cap)
-// (uncoarsen.hpp:471-476 with move_request.hpp:36-41).  One CTA; more than
-// kSortMax candidates are streamed through a shared buffer that keeps the
-// running top `cap`.  Also resets the per-round counters.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_select(const u64* __restrict__ cands, u64* __restrict__ top,
-                                                 i32 cap, RoundState* __restrict__ st, i32 balance_mode) {
-  __shared__ u64 s[kSortMax];
-  if (balance_mode ? st->bdone : st->done) return;
-  const i32 cnt = st->ccount;
-  __syncthreads();
-  if (cnt == 0) {
-    if (threadIdx.x == 0) {
-      if (balance_mode) st->bdone = 1;
-      else st->done = 1;
-    }
-    return;
-  }
-  const i32 B = cnt < cap ? cnt : cap;
-  if (cnt <= kSortMax) {
-    i32 P = 32;
-    while (P < cnt) P <<= 1;
-    for (i32 i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cnt ? cands[i] : ~0ull;
-    __syncthreads();
-    for (i32 kk = 2; kk <= P; kk <<= 1)
-      for (i32 j = kk >> 1; j > 0; j >>= 1) {
-        for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
-          const i32 l = i ^ j;
-          if (l > i) {
-            const u64 x = s[i], y = s[l];
-            const bool up = (i & kk) == 0;
-            if (up ? (x > y) : (x < y)) { s[i] = y; s[l] = x; }
-          }
-        }
-        __syncthreads();
-      }
-  } else {
-    // running top-cap: s[0..cap) holds the best so far (sorted), the rest is refilled
-    i32 next = 0;
-    bool first = true;
-    while (next < cnt) {
-      const i32 lo = first ? 0 : cap;
-      for (i32 i = lo + threadIdx.x; i < kSortMax; i += blockDim.x) {
-        const i32 src = next + (i - lo);
-        s[i] = src < cnt ? cands[src] : ~0ull;
-      }
-      next += kSortMax - lo;
-      first = false;
-      __syncthreads();
-      for (i32 kk = 2; kk <= kSortMax; kk <<= 1)
-        for (i32 j = kk >> 1; j > 0; j >>= 1) {
-          for (i32 i = threadIdx.x; i < kSortMax; i += blockDim.x) {
-            const i32 l = i ^ j;
-            if (l > i) {
-              const u64 x = s[i], y = s[l];
-              const bool up = (i & kk) == 0;
-              if (up ? (x > y) : (x < y)) { s[i] = y; s[l] = x; }
-            }
-          }
-          __syncthreads();
-        }
-    }
-  }
-  for (i32 i = threadIdx.x; i < B; i += blockDim.x) top[i] = s[i];
-  for (i32 i = threadIdx.x; i < (B + 31) / 32; i += blockDim.x) st->bad[i] = 0;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    st->B = B;
-    st->ccount = 0;
-    st->ucount = 0;
-    if (balance_mode) {
-      st->firstbad = B;
-    } else {
-      st->pcount[st->pcur] = 0;
-      st->pcur ^= 1;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Balance check (uncoarsen.hpp:239-288).  CTA p computes the prefix sums of
-// part p's weight change over the sorted moves and flags every prefix index j
-// whose change is positive and pushes part p over MAXW.  A prefix j is
-// balanced when no part flags it.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_balance(const u64* __restrict__ top, const i32* __restrict__ part,
-                                                  const i32* __restrict__ target, const i32* __restrict__ vwgt,
-                                                  const u32* __restrict__ pw, float maxw,
-                                                  RoundState* __restrict__ st) {
-  __shared__ i32 s_warp[33];
-  if (st->done) return;
-  const i32 B = st->B;
-  const i32 p = blockIdx.x;
-  constexpr int IT = kMaxMoveCap / 1024;
-  i32 e[IT];
-  i32 sum = 0;
-#pragma unroll
-  for (int i = 0; i < IT; ++i) {
-    const i32 j = threadIdx.x * IT + i;
-    i32 d = 0;
-    if (j < B) {
-      const i32 v = (i32)(u32)top[j];
-      const i32 w = vwgt[v];
-      if (target[v] == p) d += w;
-      if (part[v] == p) d -= w;
-    }
-    e[i] = d;
-    sum += d;
-  }
-  // block exclusive scan of the per-thread sums
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  i32 inc = sum;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const i32 y = __shfl_up_sync(kFullMask, inc, o);
-    if (lane >= o) inc += y;
-  }
-  if (lane == 31) s_warp[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    const i32 x = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
-    i32 xi = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const i32 y = __shfl_up_sync(kFullMask, xi, o);
-      if (lane >= o) xi += y;
-    }
-    s_warp[lane] = xi - x;
-  }
-  __syncthreads();
-  i32 run = inc - sum + s_warp[wid];
-  const u32 base = pw[p];
-#pragma unroll
-  for (int i = 0; i < IT; ++i) {
-    const i32 j = threadIdx.x * IT + i;
-    run += e[i];
-    if (j < B && run > 0 && __uint2float_rn((u32)run + base) > maxw)
-      atomicOr(&st->bad[j >> 5], 1u << (j & 31));
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Apply the moves 0..pos, pos = the largest balanced prefix index
-// (uncoarsen.hpp:284-286 take the max balanced index; prefix 0 is always
-// balanced).  Part weights change by the same sums as pw[p] += D[p][pos];
-// moved vertices and their neighbours are flagged and appended to U
-// (uncoarsen.hpp:290-323).
-// ---------------------------------------------------------------------------
-__global__ void k_apply(const u64* __restrict__ top, const i32* __restrict__ xadj,
-                        const i32* __restrict__ adjncy, const i32* __restrict__ vwgt, i32* __restrict__ part,
-                        const i32* __restrict__ target, u32* __restrict__ pw, i32* __restrict__ updflag,
-                        i32* __restrict__ U, RoundState* __restrict__ st) {
-  if (st->done) return;
-  const i32 B = st->B;
-  i32 pos = 0;
-  const i32 nwords = (B + 31) >> 5;
-  for (i32 w = nwords - 1; w >= 0; --w) {
-    u32 valid = kFullMask;
-    if (w == nwords - 1 && (B & 31)) valid = (1u << (B & 31)) - 1;
-    const u32 zeros = ~st->bad[w] & valid;
-    if (zeros) {
-      pos = w * 32 + 31 - __clz(zeros);
-      break;
-    }
-  }
-  const i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j == 0) {
-    st->rounds += 1;
-    st->moves += pos + 1;
-  }
-  if (j > pos) return;
-  const u64 key = top[j];
-  const i32 v = (i32)(u32)key;
-  const i32 g = key_gain(key);
-  const i32 s = part[v], d = target[v];
-  const u32 w = (u32)vwgt[v];
-  atomicAdd(&pw[d], w);
-  atomicSub(&pw[s], w);
-  part[v] = d;
-  atomicAdd((unsigned long long*)&st->gain_sum, (unsigned long long)(i64)g);
-  if (atomicExch(&updflag[v], 1) == 0) U[atomicAdd(&st->ucount, 1)] = v;
-  for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
-    const i32 u = adjncy[e];
-    if (atomicExch(&updflag[u], 1) == 0) U[atomicAdd(&st->ucount, 1)] = u;
-  }
-}
-
-
-// ---------------------------------------------------------------------------
-// Balance rounds (default mode; the reference has none -- an overweight part
-// is only reported, cuda_check.hpp:105-113).  One round:
-//   k_bal_prep    lightest part (ties: smaller id), new round epoch
-//   k_bal_filter  boundary vertices of overweight parts -> list
-//   k_bal_eval    per listed vertex (one warp): best neighbouring part with
-//                 room by signed gain ed_q - id (ties: smaller q), else the
-//                 lightest part if it has room; marks candidates
-//   k_bal_emit    candidates without a smaller-id candidate neighbour -> keys
-//   k_select      sort by (gain desc, id asc), cap
-//   k_bal_check   per part: first move index whose source is no longer
-//                 overweight before it or whose destination overflows
-//   k_bal_apply   apply the prefix before that index, flag U
-//   k_update      refresh gains of U
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool over_cap(u32 w, float cap) { return __uint2float_rn(w) > cap; }
-
-__global__ void k_bal_prep(const u32* __restrict__ pw, i32 k, u32* __restrict__ epoch, RoundState* __restrict__ st) {
-  __shared__ u64 s_best[32];
-  if (st->bdone) return;
-  u64 best = ~0ull;
-  for (i32 p = threadIdx.x; p < k; p += blockDim.x) {
-    const u64 key = ((u64)pw[p] << 32) | (u32)p;
-    best = key < best ? key : best;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    const u64 y = __shfl_xor_sync(kFullMask, best, o);
-    best = y < best ? y : best;
-  }
-  if ((threadIdx.x & 31) == 0) s_best[threadIdx.x >> 5] = best;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = s_best[w] < best ? s_best[w] : best;
-    best = s_best[0] < best ? s_best[0] : best;
-    st->light = (i32)(u32)best;
-    st->epoch = ++(*epoch);
-    st->lcount = 0;
-  }
-}
-
-__global__ void k_bal_filter(i32 n, const i32* __restrict__ part, const i32* __restrict__ bnd,
-                             const u32* __restrict__ pw, float cap, i32* __restrict__ list,
-                             RoundState* __restrict__ st) {
-  if (st->bdone) return;
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  if (bnd[v] && over_cap(pw[part[v]], cap)) list[atomicAdd(&st->lcount, 1)] = (i32)v;
-}
-
-__global__ void k_bal_eval(const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
-                           const i32* __restrict__ adjwgt, const i32* __restrict__ vwgt, i32 k,
-                           const i32* __restrict__ part, const u32* __restrict__ pw, float cap,
-                           const i32* __restrict__ list, u32* __restrict__ bmark, i32* __restrict__ btarget,
-                           i32* __restrict__ bgain, RoundState* __restrict__ st) {
-  extern __shared__ u32 acc_all[];
-  if (st->bdone) return;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int wpb = blockDim.x >> 5;
-  u32* acc = acc_all + (size_t)wid * k;
-  for (i32 q = lane; q < k; q += 32) acc[q] = 0;
-  __syncwarp();
-  const i32 nl = st->lcount;
-  const u32 ep = st->epoch;
-  const i32 light = st->light;
-  const i64 nw = (i64)gridDim.x * wpb;
-  for (i64 i = (i64)blockIdx.x * wpb + wid; i < nl; i += nw) {
-    const i32 v = list[i];
-    const i32 p = part[v];
-    const u32 w = (u32)vwgt[v];
-    const i32 beg = xadj[v], end = xadj[v + 1];
-    for (i32 e = beg + lane; e < end; e += 32) atomicAdd(&acc[part[adjncy[e]]], (u32)adjwgt[e]);
-    __syncwarp();
-    const u32 id = acc[p];
-    // best neighbouring part with room: max signed gain, then smaller part id
-    u64 best = 0;
-    for (i32 e = beg + lane; e < end; e += 32) {
-      const i32 q = part[adjncy[e]];
-      if (q == p || over_cap(pw[q] + w, cap)) continue;
-      const i32 g = (i32)(acc[q] - id);
-      const u64 key = (1ull << 63) | ((u64)((u32)g ^ 0x80000000u) << 31) | (u64)(0x7fffffffu - (u32)q);
-      best = best > key ? best : key;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const u64 y = __shfl_xor_sync(kFullMask, best, o);
-      best = best > y ? best : y;
-    }
-    i32 q_best = -1, g_best = 0;
-    if (best) {
-      q_best = (i32)(0x7fffffffu - (u32)(best & 0x7fffffffu));
-      g_best = (i32)((u32)(best >> 31) ^ 0x80000000u);
-    } else if (light != p && !over_cap(pw[light] + w, cap)) {
-      q_best = light;
-      g_best = (i32)(acc[light] - id);
-    }
-    if (lane == 0 && q_best >= 0) {
-      bmark[v] = ep;
-      btarget[v] = q_best;
-      bgain[v] = g_best;
-    }
-    __syncwarp();
-    for (i32 e = beg + lane; e < end; e += 32) acc[part[adjncy[e]]] = 0;
-    __syncwarp();
-  }
-}
-
-__global__ void k_bal_emit(const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
-                           const i32* __restrict__ list, const u32* __restrict__ bmark,
-                           const i32* __restrict__ bgain, u64* __restrict__ cands, RoundState* __restrict__ st) {
-  if (st->bdone) return;
-  const i32 nl = st->lcount;
-  const u32 ep = st->epoch;
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += (i64)gridDim.x * blockDim.x) {
-    const i32 v = list[i];
-    if (bmark[v] != ep) continue;
-    bool yield = false;
-    for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
-      const i32 u = adjncy[e];
-      if (u < v && bmark[u] == ep) { yield = true; break; }
-    }
-    if (!yield) cands[atomicAdd(&st->ccount, 1)] = move_key(bgain[v], v);
-  }
-}
-
-// CTA p: exclusive prefix of weight leaving p, inclusive prefix of weight
-// entering p, over the sorted moves; the first move that leaves p while p is
-// no longer overweight, or enters p beyond cap, bounds the applied prefix.
-__global__ void __launch_bounds__(1024) k_bal_check(const u64* __restrict__ top, const i32* __restrict__ part,
-                                                    const i32* __restrict__ btarget, const i32* __restrict__ vwgt,
-                                                    const u32* __restrict__ pw, float cap,
-                                                    RoundState* __restrict__ st) {
-  __shared__ i32 s_w[2][33];
-  if (st->bdone) return;
-  const i32 B = st->B;
-  const i32 p = blockIdx.x;
-  constexpr int IT = kMaxMoveCap / 1024;
-  u32 o_e[IT], i_e[IT];
-  bool is_src[IT], is_des[IT];
-  u32 so = 0, si = 0;
-#pragma unroll
-  for (int i = 0; i < IT; ++i) {
-    const i32 j = threadIdx.x * IT + i;
-    o_e[i] = 0; i_e[i] = 0; is_src[i] = false; is_des[i] = false;
-    if (j < B) {
-      const i32 v = (i32)(u32)top[j];
-      const u32 w = (u32)vwgt[v];
-      if (part[v] == p) { o_e[i] = w; is_src[i] = true; }
-      if (btarget[v] == p) { i_e[i] = w; is_des[i] = true; }
-    }
-    so += o_e[i];
-    si += i_e[i];
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  u32 io = so, ii = si;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const u32 a = __shfl_up_sync(kFullMask, io, o);
-    const u32 b = __shfl_up_sync(kFullMask, ii, o);
-    if (lane >= o) { io += a; ii += b; }
-  }
-  if (lane == 31) { s_w[0][wid] = (i32)io; s_w[1][wid] = (i32)ii; }
-  __syncthreads();
-  if (wid == 0) {
-    const bool in = lane < (int)(blockDim.x >> 5);
-    u32 a = in ? (u32)s_w[0][lane] : 0, b = in ? (u32)s_w[1][lane] : 0;
-    u32 ai = a, bi = b;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const u32 x = __shfl_up_sync(kFullMask, ai, o);
-      const u32 y = __shfl_up_sync(kFullMask, bi, o);
-      if (lane >= o) { ai += x; bi += y; }
-    }
-    s_w[0][lane] = (i32)(ai - a);
-    s_w[1][lane] = (i32)(bi - b);
-  }
-  __syncthreads();
-  u32 out_ex = io - so + (u32)s_w[0][wid];   // weight leaving p before this thread's first move
-  u32 in_in = ii - si + (u32)s_w[1][wid];
-  const u32 base = pw[p];
-  i32 first = INT_MAX;
-#pragma unroll
-  for (int i = 0; i < IT; ++i) {
-    const i32 j = threadIdx.x * IT + i;
-    in_in += i_e[i];
-    if (j < B) {
-      if (is_src[i] && !over_cap(base - out_ex, cap)) first = j < first ? j : first;
-      if (is_des[i] && over_cap(base + in_in, cap)) first = j < first ? j : first;
-    }
-    out_ex += o_e[i];
-  }
-  if (first != INT_MAX) atomicMin(&st->firstbad, first);
-}
-
-__global__ void k_bal_apply(const u64* __restrict__ top, const i32* __restrict__ xadj,
-                            const i32* __restrict__ adjncy, const i32* __restrict__ vwgt, i32* __restrict__ part,
-                            const i32* __restrict__ btarget, u32* __restrict__ pw, i32* __restrict__ updflag,
-                            i32* __restrict__ U, RoundState* __restrict__ st) {
-  if (st->bdone) return;
-  const i32 pos = st->firstbad - 1;
-  const i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j == 0) {
-    st->brounds += 1;
-    st->bmoves += pos + 1;
-  }
-  if (j > pos) return;
-  const i32 v = (i32)(u32)top[j];
-  const i32 s = part[v], d = btarget[v];
-  const u32 w = (u32)vwgt[v];
-  atomicAdd(&pw[d], w);
-  atomicSub(&pw[s], w);
-  part[v] = d;
-  if (atomicExch(&updflag[v], 1) == 0) U[atomicAdd(&st->ucount, 1)] = v;
-  for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
-    const i32 u = adjncy[e];
-    if (atomicExch(&updflag[u], 1) == 0) U[atomicAdd(&st->ucount, 1)] = u;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Host drivers
-// ---------------------------------------------------------------------------
-static void launch_update(Handle& h, RefineCtx* c, const DevGraph& g, i32 grid_cap) {
-  const i32 wpb = c->upd_warps;
-  const size_t sm = (size_t)wpb * c->k * sizeof(u32);
-  const u32 grid = std::max<u32>(1, std::min<u32>((u32)grid_cap, (u32)h.sm_count * 8));
-  launch(k_update, grid, wpb * 32, sm, h.stream, g.xadj, g.adjncy, g.adjwgt, c->k, c->part[c->cur],
-                                              c->bnd[c->cur], c->gain, c->target, c->updflag, c->inP,
-                                              c->U, c->P[0], c->P[1], c->st);
-  GKW_CHECK_LAUNCH();
-}
-
-void refine_project(Handle& h, RefineCtx* c, const DevGraph& fine, const i32* cmap, i32 nc) {
-  (void)nc;
-  reset_state(h, c);
-  const i32 nxt = c->cur ^ 1;
-  if (fine.n > 0) {
-    launch(k_project, ceil_div(fine.n, 256), 256, 0, h.stream, fine.n, cmap, c->part[c->cur], c->bnd[c->cur],
-                                                          c->part[nxt], c->bnd[nxt], c->gain, c->target,
-                                                          c->updflag, c->inP, c->U, c->st);
-    GKW_CHECK_LAUNCH();
-  }
-  c->cur = nxt;
-  launch_update(h, c, fine, (i32)ceil_div(std::max(fine.n, 1), 8));
-}
-
-__global__ void k_build_lists(i32 n, const i32* __restrict__ updated, const i32* __restrict__ gain,
-                              i32* __restrict__ updflag, i32* __restrict__ inP, i32* __restrict__ U,
-                              i32* __restrict__ P0, RoundState* __restrict__ st) {
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  const i32 u = updated ? (updated[v] != 0) : 0;
-  updflag[v] = u;
-  if (u) U[atomicAdd(&st->ucount, 1)] = (i32)v;
-  const i32 pos = gain[v] > 0;
-  inP[v] = pos;
-  if (pos) P0[atomicAdd(&st->pcount[0], 1)] = (i32)v;
-}
-
-void refine_update_flagged(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_updated) {
-  reset_state(h, c);
-  if (g.n > 0) {
-    launch(k_build_lists, ceil_div(g.n, 256), 256, 0, h.stream, g.n, d_updated, c->gain, c->updflag, c->inP,
-                                                           c->U, c->P[0], c->st);
-    GKW_CHECK_LAUNCH();
-  }
-  launch_update(h, c, g, (i32)ceil_div(std::max(g.n, 1), 8));
-}
-
-RefineLevelStats refine_level(Handle& h, RefineCtx* c, const DevGraph& g, const RefineParams& p) {
-  GKW_REQUIRE(p.move_cap >= 1 && p.move_cap <= c->cap, GKW_E_INVALID, "move_cap out of range");
-  constexpr i32 kBatch = 8;
-  const u32 cgrid = std::max<u32>(1, std::min<u32>(ceil_div(std::max(g.n, 1), 256), (u32)h.sm_count * 4));
-  const u32 agrid = ceil_div(p.move_cap, 256);
-  RoundState* hst = reinterpret_cast<RoundState*>(h.h_pinned);
-  static_assert(sizeof(RoundState) <= 64 * sizeof(i64), "pinned staging too small");
-  // every round applies >= 1 move of positive gain; 4n+64 rounds is far above
-  // anything the cut allows in practice and bounds the host loop
-  const i64 max_batches = (4 * (i64)g.n + 64) / kBatch + 1;
-  for (i64 b = 0;; ++b) {
-    GKW_REQUIRE(b < max_batches, GKW_E_INTERNAL, "refinement did not terminate");
-    for (i32 r = 0; r < kBatch; ++r) {
-      launch(k_candidates, cgrid, 256, 0, h.stream, g.xadj, g.adjncy, g.vwgt, c->part[c->cur], c->bnd[c->cur],
-                                                c->gain, c->target, c->pw, p.maxw, c->inP, c->P[0], c->P[1],
-                                                c->cands, c->st);
-      launch(k_select, 1, 1024, 0, h.stream, c->cands, c->top, p.move_cap, c->st, 0);
-      launch(k_balance, c->k, 1024, 0, h.stream, c->top, c->part[c->cur], c->target, g.vwgt, c->pw, p.maxw, c->st);
-      launch(k_apply, agrid, 256, 0, h.stream, c->top, g.xadj, g.adjncy, g.vwgt, c->part[c->cur], c->target,
-                                           c->pw, c->updflag, c->U, c->st);
-      launch_update(h, c, g, (i32)ceil_div(std::max(g.n, 1), 8));
-    }
-    GKW_CHECK_LAUNCH();
-    GKW_CUDA(cudaMemcpyAsync(hst, c->st, sizeof(RoundState), cudaMemcpyDeviceToHost, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-    if (hst->done) break;
-  }
-  RefineLevelStats s;
-  s.rounds = hst->rounds;
-  s.moves = hst->moves;
-  s.gain_sum = hst->gain_sum;
-  return s;
-}
-
-
-RefineLevelStats balance_level(Handle& h, RefineCtx* c, const DevGraph& g, float cap, i32 move_cap) {
-  GKW_REQUIRE(move_cap >= 1 && move_cap <= c->cap, GKW_E_INVALID, "move_cap out of range");
-  RefineLevelStats s;
-  if (g.n == 0) return s;
-  constexpr i32 kBatch = 8;
-  const i32 wpb = c->upd_warps;
-  const size_t sm = (size_t)wpb * c->k * sizeof(u32);
-  const u32 nb = ceil_div(g.n, 256);
-  const u32 egrid = std::max<u32>(1, std::min<u32>(ceil_div(g.n, wpb), (u32)h.sm_count * 8));
-  const u32 tgrid = std::max<u32>(1, std::min<u32>(nb, (u32)h.sm_count * 4));
-  const u32 agrid = ceil_div(move_cap, 256);
-  // the balance loop shares the round state with refinement: clear its part
-  GKW_CUDA(cudaMemsetAsync(&c->st->bdone, 0, sizeof(i32), h.stream));
-  GKW_CUDA(cudaMemsetAsync(&c->st->brounds, 0, sizeof(i32), h.stream));
-  GKW_CUDA(cudaMemsetAsync(&c->st->bmoves, 0, sizeof(i64), h.stream));
-  GKW_CUDA(cudaMemsetAsync(&c->st->ccount, 0, sizeof(i32), h.stream));
-  RoundState* hst = reinterpret_cast<RoundState*>(h.h_pinned);
-  const i64 max_batches = (4 * (i64)g.n + 64) / kBatch + 1;
-  for (i64 b = 0;; ++b) {
-    GKW_REQUIRE(b < max_batches, GKW_E_INTERNAL, "balancing did not terminate");
-    for (i32 r = 0; r < kBatch; ++r) {
-      launch(k_bal_prep, 1, 256, 0, h.stream, c->pw, c->k, c->epoch, c->st);
-      launch(k_bal_filter, nb, 256, 0, h.stream, g.n, c->part[c->cur], c->bnd[c->cur], c->pw, cap, c->blist, c->st);
-      launch(k_bal_eval, egrid, wpb * 32, sm, h.stream, g.xadj, g.adjncy, g.adjwgt, g.vwgt, c->k, c->part[c->cur],
-             c->pw, cap, c->blist, c->bmark, c->btarget, c->bgain, c->st);
-      launch(k_bal_emit, tgrid, 256, 0, h.stream, g.xadj, g.adjncy, c->blist, c->bmark, c->bgain, c->cands, c->st);
-      launch(k_select, 1, 1024, 0, h.stream, c->cands, c->top, move_cap, c->st, 1);
-      launch(k_bal_check, c->k, 1024, 0, h.stream, c->top, c->part[c->cur], c->btarget, g.vwgt, c->pw, cap, c->st);
-      launch(k_bal_apply, agrid, 256, 0, h.stream, c->top, g.xadj, g.adjncy, g.vwgt, c->part[c->cur], c->btarget,
-             c->pw, c->updflag, c->U, c->st);
-      launch_update(h, c, g, (i32)ceil_div(std::max(g.n, 1), 8));
-    }
-    GKW_CHECK_LAUNCH();
-    GKW_CUDA(cudaMemcpyAsync(hst, c->st, sizeof(RoundState), cudaMemcpyDeviceToHost, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-    if (hst->bdone) break;
-  }
-  s.rounds = hst->brounds;
-  s.moves = hst->bmoves;
-  // clear the flag so that the refinement rounds' gain updates run again
-  GKW_CUDA(cudaMemsetAsync(&c->st->bdone, 0, sizeof(i32), h.stream));
-  return s;
+  return out;
 }
 
 // ---------------------------------------------------------------------------
 // Metrics: exact weighted cut over u < v (uncoarsen.hpp:398-424) and part
-// weights (cuda_check.hpp:61-73).
+// weights (cuda_check.hpp:61-73); part weights are summed per CTA in shared
+// memory first.
 // ---------------------------------------------------------------------------
 __global__ void k_cut_pw(i32 n, const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
                          const i32* __restrict__ adjwgt, const i32* __restrict__ vwgt,
                          const i32* __restrict__ part, i32 k, unsigned long long* __restrict__ cut,
                          unsigned long long* __restrict__ pw, i32* __restrict__ bad) {
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ unsigned long long s_pw[];
+  const bool local = k <= 4096;
+  if (local) {
+    for (i32 p = threadIdx.x; p < k; p += blockDim.x) s_pw[p] = 0;
+    __syncthreads();
+  }
   u64 c = 0;
-  if (v < n) {
+  for (i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (i64)gridDim.x * blockDim.x) {
     const i32 p = part[v];
     if ((u32)p >= (u32)k) {
       atomicOr(bad, 1);
-    } else {
-      for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
-        const i32 u = adjncy[e];
-        if (v < u && part[u] != p) c += (u32)adjwgt[e];
-      }
-      atomicAdd(&pw[p], (unsigned long long)(u32)vwgt[v]);
+      continue;
     }
+    for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
+      const i32 u = adjncy[e];
+      if (v < u && part[u] != p) c += (u32)adjwgt[e];
+    }
+    if (local) atomicAdd(&s_pw[p], (unsigned long long)(u32)vwgt[v]);
+    else atomicAdd(&pw[p], (unsigned long long)(u32)vwgt[v]);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFullMask, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(cut, (unsigned long long)c);
+  if (local) {
+    __syncthreads();
+    for (i32 p = threadIdx.x; p < k; p += blockDim.x)
+      if (s_pw[p]) atomicAdd(&pw[p], s_pw[p]);
+  }
 }
 
 __global__ void k_check_parts(i32 n, const i32* __restrict__ part, i32 k, i32* __restrict__ bad) {
@@ -920,7 +1086,9 @@ void compute_cut_pw(Handle& h, const DevGraph& g, const i32* part, i32 k, i64* d
   GKW_CUDA(cudaMemsetAsync(d_cut, 0, sizeof(i64) * 2, h.stream));   // [0] cut, [1] bad-part flag
   GKW_CUDA(cudaMemsetAsync(d_pw, 0, sizeof(i64) * k, h.stream));
   if (g.n == 0) return;
-  launch(k_cut_pw, ceil_div(g.n, 256), 256, 0, h.stream, g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
+  const size_t sm = k <= 4096 ? sizeof(unsigned long long) * k : 0;
+  const u32 grid = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)h.sm_count * 8));
+  launch(k_cut_pw, grid, 256, sm, h.stream, g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
          (unsigned long long*)d_cut, (unsigned long long*)d_pw, (i32*)(d_cut + 1));
   GKW_CHECK_LAUNCH();
 }
