@@ -173,12 +173,14 @@ __global__ void k_group_chunks(i32 n, const i32* __restrict__ gsize, i32 cap, i3
   }
 }
 
-// big[] layout: [0] = number of big groups, [1] = number with > kGroupSmem members
+// counts[]: [0] groups of 7..32 members (warp sort), [1] groups above kGroupSmem
+// (global sort), [2] n_c, [3] members of big groups, [4] groups of
+// 33..kGroupSmem members (CTA sort)
 __global__ void k_group_scatter(i32 n, const u64* __restrict__ keys, const i32* __restrict__ gsize,
                                 const i32* __restrict__ cbase, const i32* __restrict__ goff,
                                 i32* __restrict__ gcur, i32 cap, i32* __restrict__ cmap,
                                 i32* __restrict__ members, i32* __restrict__ biglist,
-                                i32* __restrict__ giantlist, i32* __restrict__ counts) {
+                                i32* __restrict__ ctalist, i32* __restrict__ giantlist, i32* __restrict__ counts) {
   const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   const i32 r = (i32)(u32)(keys[v] >> 32);
@@ -189,7 +191,8 @@ __global__ void k_group_scatter(i32 n, const u64* __restrict__ keys, const i32* 
     const i32 slot = atomicAdd(&gcur[r], 1);
     members[goff[r] + slot] = (i32)v;
     if (r == (i32)v) {
-      if (s <= kGroupSmem) biglist[atomicAdd(&counts[0], 1)] = r;
+      if (s <= 32) biglist[atomicAdd(&counts[0], 1)] = r;
+      else if (s <= kGroupSmem) ctalist[atomicAdd(&counts[4], 1)] = r;
       else giantlist[atomicAdd(&counts[1], 1)] = r;
     }
   }
@@ -253,11 +256,10 @@ __global__ void k_group_sort_cta(const i32* __restrict__ biglist, const i32* __r
                                  const i32* __restrict__ goff, const i32* __restrict__ cbase,
                                  const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap) {
   __shared__ u64 sk[kGroupSmem];
-  const i32 nbig = counts[0];
+  const i32 nbig = counts[4];
   for (i32 b = blockIdx.x; b < nbig; b += gridDim.x) {
     const i32 r = biglist[b];
     const i32 s = gsize[r];
-    if (s <= 32) continue;   // block-uniform
     i32 P = 64;
     while (P < s) P <<= 1;
     for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
@@ -317,10 +319,11 @@ i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap) {
   i32* members = h.scratch.alloc_n<i32>(n);
   i32* biglist = h.scratch.alloc_n<i32>(n);
   i32* giantlist = h.scratch.alloc_n<i32>(n);
-  i32* counts = h.scratch.alloc_n<i32>(4);   // [0] big, [1] giant, [2] nc, [3] nbig members
+  i32* ctalist = h.scratch.alloc_n<i32>(n);
+  i32* counts = h.scratch.alloc_n<i32>(8);
   GKW_CUDA(cudaMemsetAsync(gsize, 0, sizeof(i32) * n, h.stream));
   GKW_CUDA(cudaMemsetAsync(gcur, 0, sizeof(i32) * n, h.stream));
-  GKW_CUDA(cudaMemsetAsync(counts, 0, sizeof(i32) * 4, h.stream));
+  GKW_CUDA(cudaMemsetAsync(counts, 0, sizeof(i32) * 8, h.stream));
   launch(k_group_count, nb, 256, 0, h.stream, n, keys, gsize);
   GKW_CHECK_LAUNCH();
   launch(k_group_chunks, nb, 256, 0, h.stream, n, gsize, cap, chunks, bigsz);
@@ -328,13 +331,13 @@ i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap) {
   exclusive_scan_i32(h, chunks, chunks, n, counts + 2);   // chunks -> chunk base, total = nc
   exclusive_scan_i32(h, bigsz, bigsz, n, counts + 3);     // member offsets of big groups
   launch(k_group_scatter, nb, 256, 0, h.stream, n, keys, gsize, chunks, bigsz, gcur, cap, cmap, members,
-                                            biglist, giantlist, counts);
+         biglist, ctalist, giantlist, counts);
   GKW_CHECK_LAUNCH();
   const u32 ng = std::max<u32>(1, std::min<u32>(ceil_div(n, 8 * 32), (u32)h.sm_count * 16));
   launch(k_group_sort_warp, ng, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz, chunks, members,
                                               cap, cmap);
   GKW_CHECK_LAUNCH();
-  launch(k_group_sort_cta, (u32)h.sm_count * 2, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz,
+  launch(k_group_sort_cta, (u32)h.sm_count * 2, 256, 0, h.stream, ctalist, counts, keys, gsize, bigsz,
                                                               chunks, members, cap, cmap);
   GKW_CHECK_LAUNCH();
   i32* hp = (i32*)h.h_pinned;
@@ -454,47 +457,120 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
   const i64 nw = (i64)gridDim.x * WARPS;
   for (i64 c = (i64)blockIdx.x * WARPS + wid; c < nc; c += nw) {
     const i32 L = rowlen[c];
-    if (L > WCAP) {
+    const i32 nm = mcnt[c];
+    if (L > WCAP || nm > 32) {
       if (lane == 0) heavy[atomicAdd(nheavy, 1)] = (i32)c;
       continue;
     }
-    u32 hsz = 32;
+    // lane j < nm: member j's row; exclusive prefix of the row lengths
+    i32 mbeg = 0, mlen = 0;
+    if (lane < nm) {
+      const i32 v = memtab[c * (i64)cap + lane];
+      mbeg = xadj[v];
+      mlen = xadj[v + 1] - mbeg;
+    }
+    i32 moff = mlen;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const i32 y = __shfl_up_sync(kFull, moff, o);
+      if (lane >= o) moff += y;
+    }
+    moff -= mlen;
+    // entry i of the concatenated rows -> its CSR position
+    auto entry_pos = [&](i32 i) {
+      i32 pos = -1;
+      for (i32 jm = 0; jm < nm; ++jm) {
+        const i32 oj = __shfl_sync(kFull, moff, jm);
+        const i32 lj = __shfl_sync(kFull, mlen, jm);
+        const i32 bj = __shfl_sync(kFull, mbeg, jm);
+        if (i >= oj && i < oj + lj) pos = bj + (i - oj);
+      }
+      return pos;
+    };
+    const i32 o = ub[c];
+    if (L <= 32) {
+      // all entries in registers: sort (key, w), merge equal keys, drop self
+      u64 kv = ~0ull;
+      const i32 pos = entry_pos(lane);
+      if (lane < L) {
+        const u32 key = (u32)cmap[adjncy[pos]];
+        if (key != (u32)c) kv = ((u64)key << 32) | (u32)adjwgt[pos];
+      }
+#pragma unroll
+      for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+          const u64 ot = __shfl_xor_sync(kFull, kv, jj);
+          const bool up = (lane & kk) == 0;
+          const bool lower = (lane & jj) == 0;
+          kv = (lower == up) ? umin64(kv, ot) : umax64(kv, ot);
+        }
+      }
+      const u32 key = (u32)(kv >> 32);
+      const u32 w = (u32)kv;
+      const u32 kprev = __shfl_up_sync(kFull, key, 1);
+      const u32 knext = __shfl_down_sync(kFull, key, 1);
+      const bool head = lane == 0 || kprev != key;
+      const bool last = lane == 31 || knext != key;
+      // inclusive prefix sum of w (mod 2^32) and the start lane of each run
+      u32 S = w;
+      i32 start = head ? lane : 0;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const u32 y = __shfl_up_sync(kFull, S, d);
+        const i32 z = __shfl_up_sync(kFull, start, d);
+        if (lane >= d) {
+          S += y;
+          start = start > z ? start : z;
+        }
+      }
+      const u32 before = __shfl_sync(kFull, S, start > 0 ? start - 1 : 0);
+      const u32 total = S - (start > 0 ? before : 0u);
+      const bool valid = last && key != 0xffffffffu;
+      const u32 bal = __ballot_sync(kFull, valid);
+      if (valid) {
+        const i32 at = o + __popc(bal & ((1u << lane) - 1));
+        sadj[at] = (i32)key;
+        swgt[at] = (i32)total;
+      }
+      if (lane == 0) cnt[c] = __popc(bal);
+      continue;
+    }
+    u32 hsz = 64;
     while (hsz < 2u * (u32)L) hsz <<= 1;
     for (u32 i = lane; i < hsz; i += 32) { T.keys[i] = kEmpty; T.vals[i] = 0; }
     __syncwarp();
-    const i32 nm = mcnt[c];
-    for (i32 j = 0; j < nm; ++j) {
-      const i32 v = memtab[c * (i64)cap + j];
-      const i32 beg = xadj[v], end = xadj[v + 1];
-      for (i32 e = beg + lane; e < end; e += 32) {
-        const u32 key = (u32)cmap[adjncy[e]];
-        if (key != (u32)c) table_add(T.keys, T.vals, hsz, key, (u32)adjwgt[e]);
+    for (i32 b = 0; b < L; b += 32) {
+      const i32 i = b + lane;
+      const i32 pos = entry_pos(i);
+      if (i < L) {
+        const u32 key = (u32)cmap[adjncy[pos]];
+        if (key != (u32)c) table_add(T.keys, T.vals, hsz, key, (u32)adjwgt[pos]);
       }
     }
     __syncwarp();
     // compact occupied slots
     i32 U = 0;
     for (u32 base = 0; base < hsz; base += 32) {
-      const u32 s = base + lane;
-      const bool occ = T.keys[s] != kEmpty;
+      const u32 sl = base + lane;
+      const bool occ = T.keys[sl] != kEmpty;
       const u32 bal = __ballot_sync(kFull, occ);
       if (occ) {
-        const i32 pos = U + __popc(bal & ((1u << lane) - 1));
-        T.out[pos] = ((u64)T.keys[s] << 32) | T.vals[s];
+        const i32 at = U + __popc(bal & ((1u << lane) - 1));
+        T.out[at] = ((u64)T.keys[sl] << 32) | T.vals[sl];
       }
       U += __popc(bal);
     }
     __syncwarp();
-    const i32 o = ub[c];
     if (U <= 32) {
       u64 key = lane < U ? T.out[lane] : ~0ull;
 #pragma unroll
       for (int kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
-        for (int j = kk >> 1; j > 0; j >>= 1) {
-          const u64 ot = __shfl_xor_sync(kFull, key, j);
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+          const u64 ot = __shfl_xor_sync(kFull, key, jj);
           const bool up = (lane & kk) == 0;
-          const bool lower = (lane & j) == 0;
+          const bool lower = (lane & jj) == 0;
           key = (lower == up) ? umin64(key, ot) : umax64(key, ot);
         }
       }
@@ -595,15 +671,14 @@ __global__ void k_max_heavy(const i32* __restrict__ heavy, const i32* __restrict
     atomicMax(maxlen, rowlen[heavy[i]]);
 }
 
+// one thread per coarse row (rows are short; consecutive threads touch
+// consecutive rows)
 __global__ void k_copy_rows(i32 nc, const i32* __restrict__ ub, const i32* __restrict__ cnt,
                             const i32* __restrict__ cx, const i32* __restrict__ sadj,
                             const i32* __restrict__ swgt, i32* __restrict__ cadj, i32* __restrict__ cwgt) {
-  const int lane = threadIdx.x & 31;
-  const i64 w0 = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
-  for (i64 c = w0; c < nc; c += nw) {
+  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
     const i32 src = ub[c], dst = cx[c], len = cnt[c];
-    for (i32 i = lane; i < len; i += 32) {
+    for (i32 i = 0; i < len; ++i) {
       cadj[dst + i] = sadj[src + i];
       cwgt[dst + i] = swgt[src + i];
     }
@@ -695,7 +770,8 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, i32 nc, i32 cap
     *cadjwgt = out_pool.alloc_n<i32>(std::max<i64>(*mc, 1));
   }
   if (nc > 0) {
-    launch(k_copy_rows, std::max<u32>(1, std::min<u32>(ceil_div(nc, 8), (u32)h.sm_count * 16)), 256, 0, h.stream, nc, ub, cnt, cxadj, sadj, swgt, *cadjncy, *cadjwgt);
+    launch(k_copy_rows, ceil_div(nc, 256), 256, 0, h.stream, nc, ub, cnt, cxadj, sadj, swgt, *cadjncy,
+           *cadjwgt);
     GKW_CHECK_LAUNCH();
   }
   h.scratch.release(mk);

@@ -75,7 +75,8 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     const i32* __restrict__ vwgt, const i32* __restrict__ lo, const i32* __restrict__ hi,
     const i32* __restrict__ cnt, const i32* __restrict__ off, i32* __restrict__ mlist,
     i32* __restrict__ degS, i32* __restrict__ inR, i32* __restrict__ conn, i32* __restrict__ lo_out,
-    i32* __restrict__ hi_out, u64 seed, double eps, i32 trials) {
+    i32* __restrict__ hi_out, u64 seed, double eps, i32 trials, i32* __restrict__ loc, i32* __restrict__ frontier,
+    i32* __restrict__ fpos) {
   __shared__ i32 s_cnt;
   __shared__ i64 s_wsum[kInitTrials];
   __shared__ i64 s_cut[kInitTrials];
@@ -101,7 +102,11 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
       if (w < wid) woff += s_wc[w];
       tot += s_wc[w];
     }
-    if (mine) M[s_cnt + woff + __popc(bal & ((1u << lane) - 1))] = v;
+    if (mine) {
+      const i32 idx = s_cnt + woff + __popc(bal & ((1u << lane) - 1));
+      M[idx] = v;
+      loc[v] = idx;
+    }
     __syncthreads();
     if (threadIdx.x == 0) s_cnt += tot;
     __syncthreads();
@@ -145,16 +150,34 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     __syncwarp();
     i64 wR = 0;
     // ---- growth ----
+    // F = the members outside R with conn > 0 (the frontier).  A frontier
+    // vertex always outranks a non-frontier one, so while F is not empty the
+    // argmax over F equals the argmax over all unassigned members; the full
+    // scan is only needed when F is empty.
+    // F holds at most s entries: this sub-problem's slice [off, off + s) of
+    // the trial's list (sub-problems of one depth run concurrently)
+    i32* F = frontier + (i64)t * n + off[p0];
+    i32* posF = fpos + (i64)t * n;
+    i32 nF = 0;
     i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0 * 1315423911ull + (u64)t) % (u32)s);
     for (i32 step = 0; step < s; ++step) {
       if (step > 0) {
         u64 best = 0;
-        for (i32 i = lane; i < s; i += 32) {
-          const i32 v = M[i];
-          if (!R[v]) {
+        if (nF > 0) {
+          for (i32 f = lane; f < nF; f += 32) {
+            const i32 v = F[f];
             const i32 c = C[v];
-            const u64 key = grow_key(c > 0, 2 * c - degS[v], i);
+            const u64 key = grow_key(true, 2 * c - degS[v], loc[v]);
             best = best > key ? best : key;
+          }
+        } else {
+          for (i32 i = lane; i < s; i += 32) {
+            const i32 v = M[i];
+            if (!R[v]) {
+              const i32 c = C[v];
+              const u64 key = grow_key(c > 0, 2 * c - degS[v], i);
+              best = best > key ? best : key;
+            }
           }
         }
         best = warp_max_u64(best);
@@ -164,11 +187,39 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
         if (wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
       }
       const i32 v = M[pick];
-      if (lane == 0) R[v] = 1;
+      // leave the frontier (swap-remove), enter R
+      if (lane == 0) {
+        R[v] = 1;
+        if (C[v] > 0) {
+          const i32 at = posF[v];
+          const i32 last = F[nF - 1];
+          F[at] = last;
+          posF[last] = at;
+        }
+      }
+      if (C[v] > 0) --nF;
       wR += (u32)vwgt[v];
-      for (i32 e = xadj[v] + lane; e < xadj[v + 1]; e += 32) {
-        const i32 u = adjncy[e];
-        if (lo[u] == p0) C[u] += adjwgt[e];
+      __syncwarp();
+      // neighbours gain connection; those reaching conn > 0 join the frontier
+      for (i32 e0 = xadj[v]; e0 < xadj[v + 1]; e0 += 32) {
+        const i32 e = e0 + lane;
+        bool join = false;
+        i32 u = 0;
+        if (e < xadj[v + 1]) {
+          u = adjncy[e];
+          if (lo[u] == p0) {
+            const i32 old = C[u];
+            C[u] = old + adjwgt[e];
+            join = !R[u] && old <= 0 && old + adjwgt[e] > 0;
+          }
+        }
+        const u32 m = __ballot_sync(kFull32, join);
+        if (join) {
+          const i32 at = nF + __popc(m & ((1u << lane) - 1));
+          F[at] = u;
+          posF[u] = at;
+        }
+        nF += __popc(m);
       }
       __syncwarp();
       if (wR >= TL) break;
@@ -250,6 +301,9 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   i32* degS = h.scratch.alloc_n<i32>(n);
   i32* inR = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
   i32* conn = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
+  i32* loc = h.scratch.alloc_n<i32>(n);
+  i32* frontier = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
+  i32* fpos = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
   const u32 nb = ceil_div(n, 256);
   launch(k_init_fill, nb, 256, 0, h.stream, n, lo[0], hi[0], k);
   GKW_CHECK_LAUNCH();
@@ -263,7 +317,7 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     exclusive_scan_i32(h, cnt, off, k, nullptr);
     launch(k_gggp_depth, k, kInitTrials * 32, 0, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a], hi[a],
                                                         cnt, off, mlist, degS, inR, conn, lo[b], hi[b], seed,
-                                                        eps, trials);
+                                                        eps, trials, loc, frontier, fpos);
     GKW_CHECK_LAUNCH();
   }
   GKW_CUDA(cudaMemcpyAsync(d_part, lo[depth & 1], sizeof(i32) * n, cudaMemcpyDeviceToDevice, h.stream));

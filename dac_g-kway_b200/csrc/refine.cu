@@ -16,6 +16,8 @@
 // ld.global.cg (L2, coherent) after the barrier.
 #include <algorithm>
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "gkw_internal.cuh"
@@ -29,6 +31,7 @@ constexpr i32 kBadWords = kMaxMoveCap / 32;
 constexpr int kLevelThreads = 512;
 constexpr long long kBarrierCycles = 4000000000ll;   // ~2 s at 2 GHz
 constexpr i32 kStatSlots = GKW_MAX_LEVELS + 2;
+constexpr i32 kTraceCap = 4096;   // phase marks per level (diagnostic timeline)
 
 struct RoundState {
   i32 pcount[2];
@@ -85,6 +88,8 @@ struct RefineCtx {
   GridBarrier* bar = nullptr;
   i32* err = nullptr;
   LevelStatsDev* stats = nullptr;
+  u64* trace = nullptr;     // GKW_TRACE=1: per-level phase timelines
+  i32* trace_n = nullptr;
   i32 acc_warps = 16;
   size_t smem = 0;
   i32 grid = 0;
@@ -115,6 +120,9 @@ struct LevelArgs {
   i32* err;
   LevelStatsDev* stat_slot;
   i32 acc_warps;
+  u64* trace;        // optional phase timeline: (phase id << 56) | globaltimer ns
+  i32 trace_cap;
+  i32* trace_n;
 };
 
 enum : i32 { LF_PROJECT = 1, LF_LISTS = 2, LF_UPDATE = 4, LF_BALANCE = 8, LF_REFINE = 16 };
@@ -162,6 +170,37 @@ __device__ __forceinline__ void warp_append64(bool pred, u64 val, u64* list, i32
   if (lane == leader) base = atomicAdd(counter, __popc(mask));
   base = __shfl_sync(kFullMask, base, leader);
   if (pred) list[base + __popc(mask & ((1u << lane) - 1))] = val;
+}
+
+__device__ __forceinline__ u64 globaltimer_ns() {
+  u64 t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Phase timeline (diagnostic): block 0, thread 0 records each barrier exit.
+__device__ __forceinline__ void trace_mark(const LevelArgs& a, u32 phase) {
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    const i32 i = *a.trace_n;
+    if (i < a.trace_cap) {
+      a.trace[i] = ((u64)phase << 56) | (globaltimer_ns() & 0x00ffffffffffffffull);
+      *a.trace_n = i + 1;
+    }
+  }
+}
+
+// Block-aggregated append of one u64 per flagged thread: one global atomic
+// per CTA.  Every thread of the block calls it (block-uniform control flow).
+__device__ __forceinline__ void block_append64(bool pred, u64 val, u64* list, i32* counter, i32* s_cnt,
+                                               i32* s_base) {
+  if (threadIdx.x == 0) *s_cnt = 0;
+  __syncthreads();
+  const i32 local = pred ? atomicAdd(s_cnt, 1) : -1;
+  __syncthreads();
+  if (threadIdx.x == 0 && *s_cnt) *s_base = atomicAdd(counter, *s_cnt);
+  __syncthreads();
+  if (pred) list[*s_base + local] = val;
+  __syncthreads();
 }
 
 // Grid barrier (all CTAs of a cooperative launch).  Returns false when any
@@ -255,9 +294,8 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all) {
   u32* acc = acc_all + (size_t)wid * a.k;
   RoundState* st = a.st;
   const i32 nU = ldc(&st->ucount);
-  const i32 pc = ldc(&st->pcur);
-  i32* Pout = pc ? a.P1 : a.P0;
-  i32* pcount = &st->pcount[pc];
+  i32* Pout = a.P0;          // P is never compacted within a level: entries whose
+  i32* pcount = &st->pcount[0];   // gain dropped stay and are skipped by gain
   const i64 nw = (i64)gridDim.x * a.acc_warps;
   for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nU; i += nw) {
     const i32 v = ldc(a.U + i);
@@ -306,43 +344,42 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all) {
 // Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
 // boundary, gain > 0, a valid destination by weight, and no neighbour with a
 // smaller id that is itself positive and valid.  P is compacted on the way.
-__device__ void ph_candidates(const LevelArgs& a) {
+__device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
   RoundState* st = a.st;
   const int lane = threadIdx.x & 31;
-  const i32 pc = ldc(&st->pcur);
-  const i32 nP = ldc(&st->pcount[pc]);
-  const i32* Pin = pc ? a.P1 : a.P0;
-  i32* Pout = pc ? a.P0 : a.P1;
-  const i64 stride = (i64)gridDim.x * blockDim.x;
-  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nP; base += stride) {
-    const i64 i = base + lane;
-    bool keep = false, cand = false;
+  const i32 nP = ldc(&st->pcount[0]);
+  // entry r*32*W + lane*W + w goes to warp w, lane `lane`: the entries of a
+  // round spread over all warps, so each warp checks at most a few of them
+  const i64 W = (i64)gridDim.x * (blockDim.x >> 5);
+  const i64 gw = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (i64 r0 = 0; r0 < nP; r0 += 32 * W) {
+    const i64 i = r0 + lane * W + gw;
+    bool check = false;
     i32 v = 0, g = 0;
     if (i < nP) {
-      v = ldc(Pin + i);
+      v = ldc(a.P0 + i);
       g = ldc(a.gain + v);
-      if (g <= 0) {
-        a.inP[v] = 0;
-      } else {
-        keep = true;
-        if (ldc(a.bnd + v)) {
-          const i32 t = ldc(a.target + v);
-          if (valid_move(ldc(a.pw + t), (u32)a.vwgt[v], a.maxw)) {
-            cand = true;
-            for (i32 e = a.xadj[v]; e < a.xadj[v + 1]; ++e) {
-              const i32 u = a.adjncy[e];
-              if (u < v && ldc(a.gain + u) > 0 &&
-                  valid_move(ldc(a.pw + ldc(a.target + u)), (u32)a.vwgt[u], a.maxw)) {
-                cand = false;
-                break;
-              }
-            }
-          }
-        }
-      }
+      if (g > 0 && ldc(a.bnd + v))
+        check = valid_move(ldc(a.pw + ldc(a.target + v)), (u32)a.vwgt[v], a.maxw);
     }
-    warp_append(keep, v, Pout, &st->pcount[pc ^ 1]);
-    warp_append64(cand, move_key(g, v), a.cands, &st->ccount);
+    // independent-set test, one candidate at a time, neighbours across lanes
+    u32 pend = __ballot_sync(kFullMask, check);
+    bool cand = false;
+    while (pend) {
+      const int src = __ffs(pend) - 1;
+      pend &= pend - 1;
+      const i32 cv = __shfl_sync(kFullMask, v, src);
+      const i32 beg = a.xadj[cv], end = a.xadj[cv + 1];
+      bool blocked = false;
+      for (i32 e = beg + lane; e < end && !blocked; e += 32) {
+        const i32 u = a.adjncy[e];
+        blocked = u < cv && ldc(a.gain + u) > 0 &&
+                  valid_move(ldc(a.pw + ldc(a.target + u)), (u32)a.vwgt[u], a.maxw);
+      }
+      const bool any_blocked = __any_sync(kFullMask, blocked);
+      if (lane == src) cand = !any_blocked;
+    }
+    block_append64(cand, move_key(g, v), a.cands, &st->ccount, s_cnt, s_base);
   }
 }
 
@@ -363,6 +400,8 @@ __device__ void ph_select(const LevelArgs& a, u64* s, bool balance_mode) {
   }
   const i32 cap = a.move_cap;
   const i32 B = cnt < cap ? cnt : cap;
+  // Element i is owned by thread i mod blockDim; for strides j < 32 both
+  // elements of a pair belong to one warp.
   auto bitonic = [&](i32 P) {
     for (i32 kk = 2; kk <= P; kk <<= 1)
       for (i32 j = kk >> 1; j > 0; j >>= 1) {
@@ -374,7 +413,11 @@ __device__ void ph_select(const LevelArgs& a, u64* s, bool balance_mode) {
             if (up ? (x > y) : (x < y)) { s[i] = y; s[l] = x; }
           }
         }
-        __syncthreads();
+        // a block barrier is needed when this stage or the next one pairs
+        // elements of different warps: j >= 32 now, or the next stage is
+        // (2kk, kk) with kk >= 32
+        if (j >= 32 || (j == 1 && kk >= 32)) __syncthreads();
+        else __syncwarp();
       }
   };
   if (cnt <= kSortMax) {
@@ -406,12 +449,7 @@ __device__ void ph_select(const LevelArgs& a, u64* s, bool balance_mode) {
     st->B = B;
     st->ccount = 0;
     st->ucount = 0;
-    if (balance_mode) {
-      st->firstbad = B;
-    } else {
-      st->pcount[st->pcur] = 0;
-      st->pcur ^= 1;
-    }
+    if (balance_mode) st->firstbad = B;
   }
 }
 
@@ -481,12 +519,33 @@ __device__ void ph_check_refine(const LevelArgs& a, u32* s_warp) {
   }
 }
 
+// U appends of one apply phase, staged per CTA in shared memory (one global
+// atomic per CTA); entries beyond the stage go to U directly.
+constexpr i32 kUStage = 1024;
+struct UStage {
+  i32 buf[kUStage];
+  i32 cnt;
+  i32 base;
+};
+__device__ __forceinline__ void ustage_push(UStage& S, i32 x, i32* U, i32* ucount) {
+  const i32 idx = atomicAdd(&S.cnt, 1);
+  if (idx < kUStage) S.buf[idx] = x;
+  else U[atomicAdd(ucount, 1)] = x;
+}
+__device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
+  __syncthreads();
+  const i32 c = S.cnt < kUStage ? S.cnt : kUStage;
+  if (threadIdx.x == 0 && c) S.base = atomicAdd(ucount, c);
+  __syncthreads();
+  for (i32 t = threadIdx.x; t < c; t += blockDim.x) U[S.base + t] = S.buf[t];
+}
+
 // Apply the moves 0..pos, pos = the largest balanced prefix index
 // (uncoarsen.hpp:284-286 keep the max balanced index; prefix 0 is always
 // balanced).  Part weights change by the same sums as pw[p] += D[p][pos]; moved
 // vertices and their neighbours are flagged and appended to U
 // (uncoarsen.hpp:290-323).  One warp per move.
-__device__ void ph_apply_refine(const LevelArgs& a) {
+__device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
   const i32 B = ldc(&st->B);
   i32 pos = 0;
@@ -503,6 +562,12 @@ __device__ void ph_apply_refine(const LevelArgs& a) {
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  __shared__ unsigned long long s_gsum;
+  if (threadIdx.x == 0) {
+    s_gsum = 0;
+    S.cnt = 0;
+  }
+  __syncthreads();
   if (warp == 0 && lane == 0) {
     st->rounds += 1;
     st->moves += pos + 1;
@@ -516,22 +581,17 @@ __device__ void ph_apply_refine(const LevelArgs& a) {
       atomicAdd(&a.pw[d], w);
       atomicSub(&a.pw[s], w);
       a.part[v] = d;
-      atomicAdd((unsigned long long*)&st->gain_sum, (unsigned long long)(i64)key_gain(key));
+      atomicAdd(&s_gsum, (unsigned long long)(i64)key_gain(key));
+      if (atomicExch(&a.updflag[v], 1) == 0) ustage_push(S, v, a.U, &st->ucount);
     }
-    const bool first = lane == 0 && atomicExch(&a.updflag[v], 1) == 0;
-    warp_append(first, v, a.U, &st->ucount);
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
-    for (i32 e0 = beg; e0 < end; e0 += 32) {
-      const i32 e = e0 + lane;
-      bool add = false;
-      i32 u = 0;
-      if (e < end) {
-        u = a.adjncy[e];
-        add = atomicExch(&a.updflag[u], 1) == 0;
-      }
-      warp_append(add, u, a.U, &st->ucount);
+    for (i32 e = beg + lane; e < end; e += 32) {
+      const i32 u = a.adjncy[e];
+      if (atomicExch(&a.updflag[u], 1) == 0) ustage_push(S, u, a.U, &st->ucount);
     }
   }
+  ustage_flush(S, a.U, &st->ucount);
+  if (threadIdx.x == 0 && s_gsum) atomicAdd((unsigned long long*)&st->gain_sum, s_gsum);
 }
 
 // ---------------------------------------------------------------------------
@@ -550,24 +610,47 @@ __device__ void ph_apply_refine(const LevelArgs& a) {
 __device__ void ph_bal_prep(const LevelArgs& a, u64* s_tmp) {
   if (blockIdx.x != 0) return;
   u64 best = ~0ull;
+  u32 heavy = 0;
   for (i32 p = threadIdx.x; p < a.k; p += blockDim.x) {
-    const u64 key = ((u64)ldc(a.pw + p) << 32) | (u32)p;
+    const u32 w = ldc(a.pw + p);
+    const u64 key = ((u64)w << 32) | (u32)p;
     best = key < best ? key : best;
+    heavy = w > heavy ? w : heavy;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const u64 y = __shfl_xor_sync(kFullMask, best, o);
     best = y < best ? y : best;
+    const u32 z = __shfl_xor_sync(kFullMask, heavy, o);
+    heavy = z > heavy ? z : heavy;
   }
   if ((threadIdx.x & 31) == 0) s_tmp[threadIdx.x >> 5] = best;
+  __shared__ u32 s_heavy[32];
+  if ((threadIdx.x & 31) == 0) s_heavy[threadIdx.x >> 5] = heavy;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) best = s_tmp[w] < best ? s_tmp[w] : best;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      best = s_tmp[w] < best ? s_tmp[w] : best;
+      heavy = s_heavy[w] > heavy ? s_heavy[w] : heavy;
+    }
     a.st->light = (i32)(u32)best;
     a.st->epoch = ++(*a.epoch);
     a.st->lcount = 0;
+    if (!over_cap(heavy, a.bcap)) a.st->bdone = 1;   // no part is overweight
   }
   __syncthreads();
+}
+
+// Boundary vertices of overweight parts -> blist.
+__device__ void ph_bal_filter(const LevelArgs& a) {
+  const int lane = threadIdx.x & 31;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += stride) {
+    const i64 v = base + lane;
+    bool want = false;
+    if (v < a.n) want = ldc(a.bnd + v) && over_cap(ldc(a.pw + ldc(a.part + v)), a.bcap);
+    warp_append(want, (i32)v, a.blist, &a.st->lcount);
+  }
 }
 
 __device__ void ph_bal_eval(const LevelArgs& a, u32* acc_all) {
@@ -577,54 +660,46 @@ __device__ void ph_bal_eval(const LevelArgs& a, u32* acc_all) {
   RoundState* st = a.st;
   const u32 ep = ldc(&st->epoch);
   const i32 light = ldc(&st->light);
+  const i32 nl = ldc(&st->lcount);
   const float cap = a.bcap;
   const i64 nw = (i64)gridDim.x * a.acc_warps;
-  for (i64 chunk = (i64)blockIdx.x * a.acc_warps + wid; chunk * 32 < a.n; chunk += nw) {
-    const i64 v0 = chunk * 32 + lane;
-    bool want = false;
-    if (v0 < a.n) want = ldc(a.bnd + v0) && over_cap(ldc(a.pw + ldc(a.part + v0)), cap);
-    u32 mask = __ballot_sync(kFullMask, want);
-    while (mask) {
-      const int bit = __ffs(mask) - 1;
-      mask &= mask - 1;
-      const i32 v = (i32)(chunk * 32 + bit);
-      const i32 p = ldc(a.part + v);
-      const u32 w = (u32)a.vwgt[v];
-      const i32 beg = a.xadj[v], end = a.xadj[v + 1];
-      for (i32 e = beg + lane; e < end; e += 32) atomicAdd(&acc[ldc(a.part + a.adjncy[e])], (u32)a.adjwgt[e]);
-      __syncwarp();
-      const u32 id = acc[p];
-      u64 best = 0;
-      for (i32 e = beg + lane; e < end; e += 32) {
-        const i32 q = ldc(a.part + a.adjncy[e]);
-        if (q == p || over_cap(ldc(a.pw + q) + w, cap)) continue;
-        const i32 g = (i32)(acc[q] - id);
-        const u64 key = (1ull << 63) | ((u64)((u32)g ^ 0x80000000u) << 31) | (u64)(0x7fffffffu - (u32)q);
-        best = best > key ? best : key;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const u64 y = __shfl_xor_sync(kFullMask, best, o);
-        best = best > y ? best : y;
-      }
-      i32 q_best = -1, g_best = 0;
-      if (best) {
-        q_best = (i32)(0x7fffffffu - (u32)(best & 0x7fffffffu));
-        g_best = (i32)((u32)(best >> 31) ^ 0x80000000u);
-      } else if (light != p && !over_cap(ldc(a.pw + light) + w, cap)) {
-        q_best = light;
-        g_best = (i32)(acc[light] - id);
-      }
-      if (lane == 0 && q_best >= 0) {
-        a.bmark[v] = ep;
-        a.btarget[v] = q_best;
-        a.bgain[v] = g_best;
-        a.blist[atomicAdd(&st->lcount, 1)] = v;
-      }
-      __syncwarp();
-      for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
-      __syncwarp();
+  for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nl; i += nw) {
+    const i32 v = ldc(a.blist + i);
+    const i32 p = ldc(a.part + v);
+    const u32 w = (u32)a.vwgt[v];
+    const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+    for (i32 e = beg + lane; e < end; e += 32) atomicAdd(&acc[ldc(a.part + a.adjncy[e])], (u32)a.adjwgt[e]);
+    __syncwarp();
+    const u32 id = acc[p];
+    u64 best = 0;
+    for (i32 e = beg + lane; e < end; e += 32) {
+      const i32 q = ldc(a.part + a.adjncy[e]);
+      if (q == p || over_cap(ldc(a.pw + q) + w, cap)) continue;
+      const i32 g = (i32)(acc[q] - id);
+      const u64 key = (1ull << 63) | ((u64)((u32)g ^ 0x80000000u) << 31) | (u64)(0x7fffffffu - (u32)q);
+      best = best > key ? best : key;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const u64 y = __shfl_xor_sync(kFullMask, best, o);
+      best = best > y ? best : y;
+    }
+    i32 q_best = -1, g_best = 0;
+    if (best) {
+      q_best = (i32)(0x7fffffffu - (u32)(best & 0x7fffffffu));
+      g_best = (i32)((u32)(best >> 31) ^ 0x80000000u);
+    } else if (light != p && !over_cap(ldc(a.pw + light) + w, cap)) {
+      q_best = light;
+      g_best = (i32)(acc[light] - id);
+    }
+    if (lane == 0 && q_best >= 0) {
+      a.bmark[v] = ep;
+      a.btarget[v] = q_best;
+      a.bgain[v] = g_best;
+    }
+    __syncwarp();
+    for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
+    __syncwarp();
   }
 }
 
@@ -640,9 +715,9 @@ __device__ void ph_bal_emit(const LevelArgs& a) {
     i32 v = 0, g = 0;
     if (i < nl) {
       v = ldc(a.blist + i);
-      g = ldc(a.bgain + v);
-      emit = true;
-      for (i32 e = a.xadj[v]; e < a.xadj[v + 1]; ++e) {
+      emit = ldc(a.bmark + v) == ep;
+      g = emit ? ldc(a.bgain + v) : 0;
+      for (i32 e = a.xadj[v]; emit && e < a.xadj[v + 1]; ++e) {
         const i32 u = a.adjncy[e];
         if (u < v && ldc(a.bmark + u) == ep) { emit = false; break; }
       }
@@ -697,12 +772,14 @@ __device__ void ph_check_balance(const LevelArgs& a, u32* s_warp) {
   }
 }
 
-__device__ void ph_apply_balance(const LevelArgs& a) {
+__device__ void ph_apply_balance(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
   const i32 pos = ldc(&st->firstbad) - 1;
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  if (threadIdx.x == 0) S.cnt = 0;
+  __syncthreads();
   if (warp == 0 && lane == 0) {
     st->brounds += 1;
     st->bmoves += pos + 1;
@@ -715,21 +792,15 @@ __device__ void ph_apply_balance(const LevelArgs& a) {
       atomicAdd(&a.pw[d], w);
       atomicSub(&a.pw[s], w);
       a.part[v] = d;
+      if (atomicExch(&a.updflag[v], 1) == 0) ustage_push(S, v, a.U, &st->ucount);
     }
-    const bool first = lane == 0 && atomicExch(&a.updflag[v], 1) == 0;
-    warp_append(first, v, a.U, &st->ucount);
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
-    for (i32 e0 = beg; e0 < end; e0 += 32) {
-      const i32 e = e0 + lane;
-      bool add = false;
-      i32 u = 0;
-      if (e < end) {
-        u = a.adjncy[e];
-        add = atomicExch(&a.updflag[u], 1) == 0;
-      }
-      warp_append(add, u, a.U, &st->ucount);
+    for (i32 e = beg + lane; e < end; e += 32) {
+      const i32 u = a.adjncy[e];
+      if (atomicExch(&a.updflag[u], 1) == 0) ustage_push(S, u, a.U, &st->ucount);
     }
   }
+  ustage_flush(S, a.U, &st->ucount);
 }
 
 // ---------------------------------------------------------------------------
@@ -742,6 +813,8 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
   __shared__ u32 s_warp[33];
   __shared__ u64 s_tmp[32];
   __shared__ i32 s_flag;
+  __shared__ i32 s_cnt, s_base;
+  __shared__ UStage s_ustage;
   {
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (wid < a.acc_warps)
@@ -749,18 +822,22 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
   }
   __syncthreads();
   RoundState* st = a.st;
+  trace_mark(a, 0);
   if (a.flags & LF_PROJECT) {
     ph_project(a);
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    trace_mark(a, 1);
   }
   if (a.flags & LF_LISTS) {
     ph_lists(a);
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    trace_mark(a, 2);
   }
   if (a.flags & LF_UPDATE) ph_update(a, acc_all);
   if (a.flags & LF_BALANCE) ph_bal_prep(a, s_tmp);
   if (a.flags & (LF_UPDATE | LF_BALANCE)) {
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    trace_mark(a, 3);
   }
   if (a.flags & LF_BALANCE) {
     for (i64 r = 0;; ++r) {
@@ -768,20 +845,30 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 2);
         return;
       }
+      if (ldc(&st->bdone)) break;   // nothing overweight (prep) or no candidate (select)
+      ph_bal_filter(a);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 9);
       ph_bal_eval(a, acc_all);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 10);
       ph_bal_emit(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 11);
       ph_select(a, s_sort, true);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 12);
       if (ldc(&st->bdone)) break;
       ph_check_balance(a, s_warp);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
-      ph_apply_balance(a);
+      trace_mark(a, 13);
+      ph_apply_balance(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 14);
       ph_update(a, acc_all);
       ph_bal_prep(a, s_tmp);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 15);
     }
   }
   if (a.flags & LF_REFINE) {
@@ -790,17 +877,22 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 3);
         return;
       }
-      ph_candidates(a);
+      ph_candidates(a, &s_cnt, &s_base);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 20);
       ph_select(a, s_sort, false);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 21);
       if (ldc(&st->done)) break;
       ph_check_refine(a, s_warp);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
-      ph_apply_refine(a);
+      trace_mark(a, 22);
+      ph_apply_refine(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 23);
       ph_update(a, acc_all);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      trace_mark(a, 24);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -857,6 +949,11 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->bar = P.alloc_n<GridBarrier>(1);
   c->err = P.alloc_n<i32>(1);
   c->stats = P.alloc_n<LevelStatsDev>(kStatSlots);
+  if (const char* t = getenv("GKW_TRACE"); t && *t == '1') {
+    c->trace = P.alloc_n<u64>((size_t)kStatSlots * kTraceCap);
+    c->trace_n = P.alloc_n<i32>(kStatSlots);
+    GKW_CUDA(cudaMemsetAsync(c->trace_n, 0, sizeof(i32) * kStatSlots, h.stream));
+  }
   GKW_CUDA(cudaMemsetAsync(c->bmark, 0, sizeof(u32) * n, h.stream));
   GKW_CUDA(cudaMemsetAsync(c->epoch, 0, sizeof(u32), h.stream));
   GKW_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(GridBarrier), h.stream));
@@ -991,8 +1088,18 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.err = c->err;
   a.stat_slot = c->stats + slot;
   a.acc_warps = c->acc_warps;
+  if (c->trace) {
+    a.trace = c->trace + (size_t)slot * kTraceCap;
+    a.trace_cap = kTraceCap;
+    a.trace_n = c->trace_n + slot;
+  }
+  // small levels use fewer CTAs: the barrier gets cheaper and the work fits;
+  // at least enough CTAs for the per-part checks to run in few passes
+  i32 grid = (i32)ceil_div(std::max(g.n, 1), 2048);
+  grid = std::max(grid, std::max(32, c->k / 4));
+  grid = std::min(grid, c->grid);
   void* args[] = {&a};
-  GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_level, dim3(c->grid), dim3(kLevelThreads), args, c->smem,
+  GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_level, dim3(grid), dim3(kLevelThreads), args, c->smem,
                                        h.stream));
   count_launch();
   c->cur = dst;
@@ -1011,6 +1118,29 @@ std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots) {
   if (err == 1) throw Error{GKW_E_INTERNAL, "level kernel: grid barrier timed out"};
   if (err == 2) throw Error{GKW_E_INTERNAL, "balancing did not terminate"};
   if (err == 3) throw Error{GKW_E_INTERNAL, "refinement did not terminate"};
+  if (c->trace && nslots) {
+    std::vector<i32> tn(nslots);
+    std::vector<u64> tr((size_t)nslots * kTraceCap);
+    GKW_CUDA(cudaMemcpy(tn.data(), c->trace_n, sizeof(i32) * nslots, cudaMemcpyDeviceToHost));
+    GKW_CUDA(cudaMemcpy(tr.data(), c->trace, sizeof(u64) * tr.size(), cudaMemcpyDeviceToHost));
+    for (i32 s = 0; s < nslots; ++s) {
+      if (tn[s] < 2) continue;
+      double acc[32] = {0};
+      i32 cnt[32] = {0};
+      const u64* t = tr.data() + (size_t)s * kTraceCap;
+      for (i32 i = 1; i < tn[s]; ++i) {
+        const u32 ph = (u32)(t[i] >> 56);
+        const double dt = (double)((t[i] & 0x00ffffffffffffffull) - (t[i - 1] & 0x00ffffffffffffffull));
+        if (ph < 32) { acc[ph] += dt; cnt[ph] += 1; }
+      }
+      const double tot = (double)((t[tn[s] - 1] & 0x00ffffffffffffffull) - (t[0] & 0x00ffffffffffffffull));
+      fprintf(stderr, "[gkw trace] level slot %d: %.1f us total;", s, tot / 1e3);
+      for (i32 p = 0; p < 32; ++p)
+        if (cnt[p]) fprintf(stderr, " ph%d x%d %.2fus", p, cnt[p], acc[p] / cnt[p] / 1e3);
+      fprintf(stderr, "\n");
+    }
+    GKW_CUDA(cudaMemset(c->trace_n, 0, sizeof(i32) * kStatSlots));
+  }
   std::vector<RefineLevelStats> out((size_t)nslots);
   for (i32 i = 0; i < nslots; ++i) {
     out[i].rounds = d[i].rounds;
