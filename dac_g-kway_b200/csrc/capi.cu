@@ -136,6 +136,14 @@ gkw_status gkw_create(gkw_handle** out, int32_t device) {
     int sms = 0;
     GKW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     h->h.sm_count = sms;
+    e = cudaMalloc(&h->h.coop, sizeof(CoopState));
+    if (e == cudaSuccess) e = cudaMemset(h->h.coop, 0, sizeof(CoopState));
+    if (e != cudaSuccess) {
+      cudaFreeHost(h->h.h_pinned);
+      cudaStreamDestroy(h->h.stream);
+      delete h;
+      GKW_CUDA(e);
+    }
     *out = h;
   });
 }
@@ -147,6 +155,9 @@ gkw_status gkw_destroy(gkw_handle* h) {
     cudaStreamSynchronize(h->h.stream);
     if (h->h.own_stream) cudaStreamDestroy(h->h.stream);
     cudaFreeHost(h->h.h_pinned);
+    if (h->h.scan) cudaFree(h->h.scan);
+    if (h->h.coop) cudaFree(h->h.coop);
+    if (h->h.arena) cudaFree(h->h.arena);
     delete h;
   });
 }
@@ -236,13 +247,11 @@ gkw_status gkw_union_find(gkw_handle* h, int32_t n, const int32_t* d_cand, int32
     GKW_REQUIRE(n >= 0, GKW_E_INVALID, "negative n");
     hh.scratch.reset();
     u64* keys = hh.scratch.alloc_n<u64>(std::max(n, 1));
-    const i32 r = run_union_find(hh, n, d_cand, keys);
-    if (n) {
-      launch(k_unpack_keys, ceil_div(n, 256), 256, 0, hh.stream, n, keys, d_root, d_dist);
-      GKW_CHECK_LAUNCH();
-    }
-    sync(hh);
-    if (rounds_out) *rounds_out = r;
+    run_union_find(hh, n, d_cand, keys, &hh.coop->uf_rounds);
+    if (n) launch(k_unpack_keys, ceil_div(n, 256), 256, 0, hh.stream, n, keys, d_root, d_dist);
+    GKW_CHECK_LAUNCH();
+    const CoopState c = read_coop(hh);
+    if (rounds_out) *rounds_out = c.uf_rounds;
   });
 }
 
@@ -253,13 +262,11 @@ gkw_status gkw_group_map(gkw_handle* h, int32_t n, const int32_t* d_root, const 
     GKW_REQUIRE(n >= 0, GKW_E_INVALID, "negative n");
     hh.scratch.reset();
     u64* keys = hh.scratch.alloc_n<u64>(std::max(n, 1));
-    if (n) {
-      launch(k_pack_keys, ceil_div(n, 256), 256, 0, hh.stream, n, d_root, d_dist, keys);
-      GKW_CHECK_LAUNCH();
-    }
-    const i32 nc = run_group_map(hh, n, keys, group_cap, d_cmap);
-    sync(hh);
-    if (nc_out) *nc_out = nc;
+    if (n) launch(k_pack_keys, ceil_div(n, 256), 256, 0, hh.stream, n, d_root, d_dist, keys);
+    GKW_CHECK_LAUNCH();
+    run_group_map(hh, n, keys, group_cap, d_cmap, &hh.coop->nc);
+    const CoopState c = read_coop(hh);
+    if (nc_out) *nc_out = c.nc;
   });
 }
 
@@ -272,9 +279,7 @@ gkw_status gkw_contract(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_
     GKW_REQUIRE(nc >= 0 && nc <= std::max(g.n, 0), GKW_E_INVALID, "nc out of range");
     GKW_REQUIRE(d_cadjncy && d_cadjwgt, GKW_E_INVALID, "output arrays are NULL");
     hh.scratch.reset();
-    // group cap: the largest coarse vertex may hold any number of members here
-    // (the per-phase entry point accepts any cmap), so size the member table
-    // by the largest member count.
+    // the member table is sized by the largest member count (any cmap is accepted here)
     i32 cap = 1;
     {
       std::vector<i32> hc(g.n);
@@ -285,12 +290,16 @@ gkw_status gkw_contract(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_
         cap = std::max(cap, ++cnt[hc[v]]);
       }
     }
-    i32* cadj = d_cadjncy;
-    i32* cwgt = d_cadjwgt;
-    i64 mc = 0;
-    run_contract(hh, g, d_cmap, nc, cap, d_cxadj, &cadj, &cwgt, d_cvwgt, &mc, hh.scratch);
-    sync(hh);
-    if (mc_out) *mc_out = mc;
+    GKW_CUDA(cudaMemcpy(&hh.coop->nc, &nc, sizeof(i32), cudaMemcpyHostToDevice));
+    run_contract(hh, g, d_cmap, &hh.coop->nc, nc, cap, d_cxadj, d_cadjncy, d_cadjwgt, d_cvwgt, &hh.coop->mc);
+    CoopState c = read_coop(hh);
+    if (c.arena_overflow) {
+      ensure_arena(hh, (u64)((double)(hh.arena_words + (u64)c.arena_need) * 1.25) + 1024);
+      run_contract(hh, g, d_cmap, &hh.coop->nc, nc, cap, d_cxadj, d_cadjncy, d_cadjwgt, d_cvwgt, &hh.coop->mc);
+      c = read_coop(hh);
+      GKW_REQUIRE(!c.arena_overflow, GKW_E_INTERNAL, "long-row arena overflow after growth");
+    }
+    if (mc_out) *mc_out = c.mc;
   });
 }
 

@@ -5,7 +5,7 @@
 #include <algorithm>
 #include <climits>
 
-#include "gkw_internal.cuh"
+#include "device_util.cuh"
 
 namespace gkw {
 
@@ -68,82 +68,96 @@ void run_match(Handle& h, const DevGraph& g, i32* cand) {
 
 // ===========================================================================
 // Union-find label propagation (coarsen.hpp:80-118, loop :461-469), Jacobi
-// schedule.  Keys are (label << 32 | round of last raise).  Round r reads
-// buffer (r-1)&1 and raises buffer r&1 with atomicMax; that buffer still holds
-// round r-2's keys, which never exceed round r-1's, so max(own key, pushes)
-// is exactly the synchronous update.  A round whose predecessor saw no change
-// returns at once, so rounds are launched in batches without a host round trip
-// per round; the host reads the per-round change flags once per batch.
+// schedule, as one persistent cooperative kernel.  Keys are
+// (label << 32 | round of last raise).  Round r reads buffer (r-1)&1 and
+// raises buffer r&1 with atomicMax; that buffer still holds round r-2's keys,
+// which never exceed round r-1's, so max(own key, pushes) is exactly the
+// synchronous update.  chg[r&1] records whether round r raised anything; the
+// grid barrier separates rounds and the loop ends after the first quiet
+// round -- no host round trip per round.
 // ===========================================================================
-__global__ void k_uf_init(i32 n, u64* __restrict__ k0, u64* __restrict__ k1) {
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < n) {
+constexpr int kUfThreads = 512;
+
+__global__ void __launch_bounds__(kUfThreads) k_uf_persist(i32 n, const i32* __restrict__ cand, u64* k0, u64* k1,
+                                                          i32* chg, GridBarrier* bar, i32* err, i32* rounds_out,
+                                                          i32 max_rounds) {
+  __shared__ i32 s_flag, s_any;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  for (i64 v = t0; v < n; v += stride) {
     const u64 key = (u64)(u32)v << 32;
     k0[v] = key;
     k1[v] = key;
   }
-}
-
-__global__ void __launch_bounds__(256) k_uf_round(i32 n, const i32* __restrict__ cand,
-                                                  const u64* __restrict__ src, u64* __restrict__ dst,
-                                                  u32 it, i32* __restrict__ changed, i32 ring) {
-  // round `it` records its change flag in slot (it-1) % ring; a round whose
-  // predecessor saw no change returns at once (the test is grid-uniform)
-  if (it >= 2 && changed[(it - 2) % ring] == 0) return;
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  bool diff = false;
-  if (v < n) {
-    const i32 c = cand[v];
-    const u64 kv = src[v];
-    const u64 kc = src[c];
-    const u32 a = (u32)(kv >> 32), b = (u32)(kc >> 32);
-    atomicMax((unsigned long long*)&dst[v], (unsigned long long)kv);
-    if (a > b) {
-      atomicMax((unsigned long long*)&dst[c], (unsigned long long)(((u64)a << 32) | it));
-      diff = true;
-    } else if (a < b) {
-      atomicMax((unsigned long long*)&dst[v], (unsigned long long)(((u64)b << 32) | it));
-      diff = true;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    chg[0] = 0;
+    chg[1] = 0;
+  }
+  if (!grid_barrier(bar, err, &s_flag)) return;
+  u64* buf[2] = {k0, k1};
+  i32 rounds = -1;
+  for (i32 it = 1;; ++it) {
+    if (it > max_rounds) {   // uniform across CTAs
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(err, 2);
+      return;
+    }
+    const u64* src = buf[(it - 1) & 1];
+    u64* dst = buf[it & 1];
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    bool diff = false;
+    for (i64 v = t0; v < n; v += stride) {
+      const i32 c = cand[v];
+      const u64 kv = ldcg(src + v);
+      const u64 kc = ldcg(src + c);
+      const u32 a = (u32)(kv >> 32), b = (u32)(kc >> 32);
+      atomicMax((unsigned long long*)&dst[v], (unsigned long long)kv);
+      if (a > b) {
+        atomicMax((unsigned long long*)&dst[c], (unsigned long long)(((u64)a << 32) | (u32)it));
+        diff = true;
+      } else if (a < b) {
+        atomicMax((unsigned long long*)&dst[v], (unsigned long long)(((u64)b << 32) | (u32)it));
+        diff = true;
+      }
+    }
+    if (diff) s_any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0 && s_any) atomicOr(&chg[it & 1], 1);
+    // chg[(it+1)&1] was read by every CTA after the previous barrier
+    if (blockIdx.x == 0 && threadIdx.x == 0) chg[(it + 1) & 1] = 0;
+    if (!grid_barrier(bar, err, &s_flag)) return;
+    if (ldcg(&chg[it & 1]) == 0) {
+      rounds = it;
+      break;
     }
   }
-  const u32 any = __ballot_sync(kFull, diff);
-  if (any && (threadIdx.x & 31) == 0) atomicOr(&changed[(it - 1) % ring], 1);
+  // after the first quiet round both buffers hold the fixed point
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rounds_out = rounds;
 }
 
-i32 run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out) {
-  if (n == 0) return 1;
-  constexpr i32 kBatch = 16, kRing = 2 * kBatch;
+// Writes the final keys to keys_out and the reference's round-launch count
+// to *d_rounds (device).  No host synchronisation.
+void run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out, i32* d_rounds) {
+  if (n == 0) {
+    const i32 one = 1;
+    GKW_CUDA(cudaMemcpyAsync(d_rounds, &one, sizeof(i32), cudaMemcpyHostToDevice, h.stream));
+    return;
+  }
   Pool::Mark mk = h.scratch.mark();
   u64* kb = h.scratch.alloc_n<u64>(n);
-  i32* changed = h.scratch.alloc_n<i32>(kRing);
-  const u32 nb = ceil_div(n, 256);
-  launch(k_uf_init, nb, 256, 0, h.stream, n, keys_out, kb);
-  GKW_CHECK_LAUNCH();
-  u64* buf[2] = {keys_out, kb};
-  i32* hp = (i32*)h.h_pinned;
-  i32 rounds = -1;
-  for (i32 batch = 0; rounds < 0; ++batch) {
-    // rounds 16b+1 .. 16b+16 use slots [16(b%2), 16(b%2)+16); the previous
-    // batch's slots (read by this batch's first round) stay intact
-    i32* slots = changed + (batch & 1) * kBatch;
-    GKW_CUDA(cudaMemsetAsync(slots, 0, sizeof(i32) * kBatch, h.stream));
-    for (i32 j = 0; j < kBatch; ++j) {
-      const i32 it = batch * kBatch + j + 1;
-      launch(k_uf_round, nb, 256, 0, h.stream, n, cand, buf[(it - 1) & 1], buf[it & 1], (u32)it, changed,
-             kRing);
-    }
-    GKW_CHECK_LAUNCH();
-    GKW_CUDA(cudaMemcpyAsync(hp, slots, sizeof(i32) * kBatch, cudaMemcpyDeviceToHost, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-    for (i32 j = 0; j < kBatch; ++j)
-      if (hp[j] == 0) { rounds = batch * kBatch + j + 1; break; }
-    // Jacobi rounds raise a label at most once per hop of the longest path
-    GKW_REQUIRE((i64)batch * kBatch <= (i64)n + 2 * kBatch, GKW_E_INTERNAL, "union-find did not converge");
-  }
-  // After the first no-change round both buffers hold the fixed point, and
-  // rounds after it return at once, so keys_out (buffer 0) is final.
+  i32* chg = h.scratch.alloc_n<i32>(2);
+  int bps = 0;
+  GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_uf_persist, kUfThreads, 0));
+  GKW_REQUIRE(bps >= 1, GKW_E_INTERNAL, "union-find kernel does not fit on an SM");
+  i32 grid = std::min<i32>(h.sm_count * std::min(bps, 2), (i32)ceil_div(n, kUfThreads));
+  grid = std::max(grid, 1);
+  i32 max_rounds = n + 2;
+  GridBarrier* barp = &h.coop->bar;
+  i32* errp = &h.coop->err;
+  void* args[] = {&n, &cand, &keys_out, &kb, &chg, &barp, &errp, &d_rounds, &max_rounds};
+  GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_uf_persist, dim3(grid), dim3(kUfThreads), args, 0, h.stream));
+  count_launch();
   h.scratch.release(mk);
-  return rounds;
 }
 
 // ===========================================================================
@@ -277,39 +291,60 @@ __global__ void k_group_sort_cta(const i32* __restrict__ biglist, const i32* __r
   }
 }
 
-// global bitonic network for one giant group (rare)
-__global__ void k_giant_load(i32 s, i32 P, const i32* __restrict__ mem, const u64* __restrict__ keys,
-                             u64* __restrict__ out) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P) return;
-  u64 key = ~0ull;
-  if (i < s) {
-    const i32 m = mem[i];
-    key = ((keys[m] & 0xffffffffull) << 32) | (u32)m;
+// Giant groups (more than kGroupSmem members, rare): every CTA of one
+// cooperative launch sorts each giant group in turn with a bitonic network in
+// global scratch, grid barriers between the stages.
+__global__ void __launch_bounds__(512) k_giant_sort(const i32* __restrict__ giantlist, const i32* __restrict__ counts,
+                                                    const u64* __restrict__ keys, const i32* __restrict__ gsize,
+                                                    const i32* __restrict__ goff, const i32* __restrict__ cbase,
+                                                    const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap,
+                                                    u64* a, GridBarrier* bar, i32* err) {
+  __shared__ i32 s_flag;
+  const i32 ng = counts[1];
+  if (ng == 0) return;   // uniform: no barrier is entered
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  for (i32 gi = 0; gi < ng; ++gi) {
+    const i32 r = giantlist[gi];
+    const i32 s = gsize[r];
+    i64 P = 1;
+    while (P < s) P <<= 1;
+    const i32* mem = members + goff[r];
+    for (i64 i = t0; i < P; i += stride) {
+      u64 key = ~0ull;
+      if (i < s) {
+        const i32 m = mem[i];
+        key = ((keys[m] & 0xffffffffull) << 32) | (u32)m;
+      }
+      a[i] = key;
+    }
+    if (!grid_barrier(bar, err, &s_flag)) return;
+    for (i64 kk = 2; kk <= P; kk <<= 1) {
+      for (i64 j = kk >> 1; j > 0; j >>= 1) {
+        for (i64 i = t0; i < P; i += stride) {
+          const i64 l = i ^ j;
+          if (l > i) {
+            const u64 x = ldcg(a + i), y = ldcg(a + l);
+            const bool up = (i & kk) == 0;
+            if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
+          }
+        }
+        if (!grid_barrier(bar, err, &s_flag)) return;
+      }
+    }
+    const i32 base = cbase[r];
+    for (i64 i = t0; i < s; i += stride) cmap[(u32)ldcg(a + i)] = base + (i32)(i / cap);
+    if (!grid_barrier(bar, err, &s_flag)) return;
   }
-  out[i] = key;
 }
 
-__global__ void k_bitonic_step(u64* __restrict__ a, i32 P, i32 j, i32 kk) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P) return;
-  const i64 l = i ^ j;
-  if (l > i) {
-    const u64 x = a[i], y = a[l];
-    const bool up = (i & kk) == 0;
-    if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
-  }
-}
-
-__global__ void k_giant_assign(i32 s, const u64* __restrict__ a, i32 base, i32 cap,
-                               i32* __restrict__ cmap) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < s) cmap[(u32)a[i]] = base + (i32)(i / cap);
-}
-
-i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap) {
+// cmap for every vertex and *d_nc = n_c (device).  No host synchronisation.
+void run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap, i32* d_nc) {
   GKW_REQUIRE(cap >= 1, GKW_E_INVALID, "group_cap must be >= 1");
-  if (n == 0) return 0;
+  if (n == 0) {
+    GKW_CUDA(cudaMemsetAsync(d_nc, 0, sizeof(i32), h.stream));
+    return;
+  }
   Pool::Mark mk = h.scratch.mark();
   const u32 nb = ceil_div(n, 256);
   i32* gsize = h.scratch.alloc_n<i32>(n);
@@ -321,55 +356,37 @@ i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap) {
   i32* giantlist = h.scratch.alloc_n<i32>(n);
   i32* ctalist = h.scratch.alloc_n<i32>(n);
   i32* counts = h.scratch.alloc_n<i32>(8);
+  u64* gscratch = h.scratch.alloc_n<u64>(2 * (size_t)n);
   GKW_CUDA(cudaMemsetAsync(gsize, 0, sizeof(i32) * n, h.stream));
   GKW_CUDA(cudaMemsetAsync(gcur, 0, sizeof(i32) * n, h.stream));
   GKW_CUDA(cudaMemsetAsync(counts, 0, sizeof(i32) * 8, h.stream));
   launch(k_group_count, nb, 256, 0, h.stream, n, keys, gsize);
-  GKW_CHECK_LAUNCH();
   launch(k_group_chunks, nb, 256, 0, h.stream, n, gsize, cap, chunks, bigsz);
   GKW_CHECK_LAUNCH();
-  exclusive_scan_i32(h, chunks, chunks, n, counts + 2);   // chunks -> chunk base, total = nc
-  exclusive_scan_i32(h, bigsz, bigsz, n, counts + 3);     // member offsets of big groups
+  exclusive_scan_i32(h, chunks, chunks, n, d_nc);   // chunks -> chunk base, total = n_c
+  exclusive_scan_i32(h, bigsz, bigsz, n, counts + 3);   // member offsets of big groups
   launch(k_group_scatter, nb, 256, 0, h.stream, n, keys, gsize, chunks, bigsz, gcur, cap, cmap, members,
          biglist, ctalist, giantlist, counts);
-  GKW_CHECK_LAUNCH();
   const u32 ng = std::max<u32>(1, std::min<u32>(ceil_div(n, 8 * 32), (u32)h.sm_count * 16));
-  launch(k_group_sort_warp, ng, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz, chunks, members,
-                                              cap, cmap);
+  launch(k_group_sort_warp, ng, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz, chunks, members, cap, cmap);
+  launch(k_group_sort_cta, (u32)h.sm_count * 2, 256, 0, h.stream, ctalist, counts, keys, gsize, bigsz, chunks,
+         members, cap, cmap);
   GKW_CHECK_LAUNCH();
-  launch(k_group_sort_cta, (u32)h.sm_count * 2, 256, 0, h.stream, ctalist, counts, keys, gsize, bigsz,
-                                                              chunks, members, cap, cmap);
-  GKW_CHECK_LAUNCH();
-  i32* hp = (i32*)h.h_pinned;
-  GKW_CUDA(cudaMemcpyAsync(hp, counts, sizeof(i32) * 4, cudaMemcpyDeviceToHost, h.stream));
-  GKW_CUDA(cudaStreamSynchronize(h.stream));
-  const i32 n_giant = hp[1];
-  const i32 nc = hp[2];
-  if (n_giant > 0) {
-    std::vector<i32> giants(n_giant);
-    GKW_CUDA(cudaMemcpy(giants.data(), giantlist, sizeof(i32) * n_giant, cudaMemcpyDeviceToHost));
-    std::vector<i32> gs(n), go(n), cb(n);
-    for (i32 r : giants) {
-      i32 s, off, base;
-      GKW_CUDA(cudaMemcpy(&s, gsize + r, sizeof(i32), cudaMemcpyDeviceToHost));
-      GKW_CUDA(cudaMemcpy(&off, bigsz + r, sizeof(i32), cudaMemcpyDeviceToHost));
-      GKW_CUDA(cudaMemcpy(&base, chunks + r, sizeof(i32), cudaMemcpyDeviceToHost));
-      i32 P = 1;
-      while (P < s) P <<= 1;
-      Pool::Mark m2 = h.scratch.mark();
-      u64* a = h.scratch.alloc_n<u64>(P);
-      const u32 pb = ceil_div(P, 256);
-      launch(k_giant_load, pb, 256, 0, h.stream, s, P, members + off, keys, a);
-      for (i32 kk = 2; kk <= P; kk <<= 1)
-        for (i32 j = kk >> 1; j > 0; j >>= 1) launch(k_bitonic_step, pb, 256, 0, h.stream, a, P, j, kk);
-      launch(k_giant_assign, ceil_div(s, 256), 256, 0, h.stream, s, a, base, cap, cmap);
-      GKW_CHECK_LAUNCH();
-      GKW_CUDA(cudaStreamSynchronize(h.stream));
-      h.scratch.release(m2);
-    }
+  {
+    const i32* gl = giantlist;
+    const i32* cn = counts;
+    const i32* gs = gsize;
+    const i32* go = bigsz;
+    const i32* cb = chunks;
+    const i32* mb = members;
+    i32 capv = cap;
+    GridBarrier* barp = &h.coop->bar;
+    i32* errp = &h.coop->err;
+    void* args[] = {&gl, &cn, (void*)&keys, &gs, &go, &cb, &mb, &capv, &cmap, &gscratch, &barp, &errp};
+    GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_giant_sort, dim3(h.sm_count), dim3(512), args, 0, h.stream));
+    count_launch();
   }
   h.scratch.release(mk);
-  return nc;
 }
 
 // ===========================================================================
@@ -384,8 +401,14 @@ i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap) {
 // ===========================================================================
 __global__ void k_coarse_accum(i32 n, const i32* __restrict__ xadj, const i32* __restrict__ vwgt,
                                const i32* __restrict__ cmap, i32 cap, i32* __restrict__ cvwgt,
-                               i32* __restrict__ rowlen, i32* __restrict__ mcnt, i32* __restrict__ memtab) {
+                               i32* __restrict__ rowlen, i32* __restrict__ mcnt, i32* __restrict__ memtab,
+                               ArenaHdr* arena) {
   const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v == 0 && arena) {
+    arena->used = 0;
+    arena->need = 0;
+    arena->overflow = 0;
+  }
   if (v >= n) return;
   const i32 c = cmap[v];
   atomicAdd((u32*)&cvwgt[c], (u32)vwgt[v]);
@@ -446,7 +469,7 @@ __device__ void warp_bitonic_u64(u64* a, i32 P, int lane) {
 
 template <int WCAP, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
-    i32 nc, const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
+    const i32* __restrict__ ncp, const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
     const i32* __restrict__ cmap, const i32* __restrict__ memtab, const i32* __restrict__ mcnt, i32 cap,
     const i32* __restrict__ rowlen, const i32* __restrict__ ub, i32* __restrict__ sadj,
     i32* __restrict__ swgt, i32* __restrict__ cnt, i32* __restrict__ heavy, i32* __restrict__ nheavy) {
@@ -454,6 +477,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
   WarpTable<WCAP>* tabs = reinterpret_cast<WarpTable<WCAP>*>(smem_raw);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   WarpTable<WCAP>& T = tabs[wid];
+  const i32 nc = *ncp;
   const i64 nw = (i64)gridDim.x * WARPS;
   for (i64 c = (i64)blockIdx.x * WARPS + wid; c < nc; c += nw) {
     const i32 L = rowlen[c];
@@ -595,19 +619,22 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
   }
 }
 
-// One CTA per heavy coarse row.  Table in dynamic shared memory when it fits,
-// otherwise in a global scratch slice (tab_keys/tab_vals/tab_out sized for the
-// largest heavy row).
+// One CTA per heavy coarse row.  Table in dynamic shared memory when the row
+// fits (L <= cta_cap); longer rows take their table from the handle's arena
+// (bump allocation: keys and values of hsz words each, then hsz/2 sorted
+// outputs as u64).  A row that does not fit in the arena records the words it
+// needs and sets the overflow flag; the host grows the arena and runs the
+// contraction again.
 template <bool GLOBAL_TABLE>
 __global__ void __launch_bounds__(512) k_contract_cta(
     const i32* __restrict__ heavy, const i32* __restrict__ nheavy, i32 cta_cap,
     const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
     const i32* __restrict__ cmap, const i32* __restrict__ memtab, const i32* __restrict__ mcnt, i32 cap,
     const i32* __restrict__ rowlen, const i32* __restrict__ ub, i32* __restrict__ sadj,
-    i32* __restrict__ swgt, i32* __restrict__ cnt, u32* __restrict__ gkeys, u32* __restrict__ gvals,
-    u64* __restrict__ gout, i64 gstride) {
+    i32* __restrict__ swgt, i32* __restrict__ cnt, ArenaHdr* arena, u32* arena_words, u64 arena_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_count;
+  __shared__ u64 s_off;
   const i32 nh = *nheavy;
   for (i32 b = blockIdx.x; b < nh; b += gridDim.x) {
     const i32 c = heavy[b];
@@ -619,9 +646,22 @@ __global__ void __launch_bounds__(512) k_contract_cta(
     u32 *keys, *vals;
     u64* out;
     if (GLOBAL_TABLE) {
-      keys = gkeys + (i64)blockIdx.x * gstride * 2;
-      vals = gvals + (i64)blockIdx.x * gstride * 2;
-      out = gout + (i64)blockIdx.x * gstride;
+      const u64 words = 3ull * hsz;   // keys + vals + hsz/2 u64 outputs
+      if (threadIdx.x == 0) {
+        const u64 off = atomicAdd((unsigned long long*)&arena->used, (unsigned long long)words);
+        if (off + words > arena_cap) {
+          atomicAdd((unsigned long long*)&arena->need, (unsigned long long)words);
+          atomicExch(&arena->overflow, 1);
+          s_off = ~0ull;
+        } else {
+          s_off = off;
+        }
+      }
+      __syncthreads();
+      if (s_off == ~0ull) continue;   // block-uniform; redone after the arena grows
+      keys = arena_words + s_off;
+      vals = keys + hsz;
+      out = reinterpret_cast<u64*>(vals + hsz);
     } else {
       keys = reinterpret_cast<u32*>(smem_raw);
       vals = keys + 2 * cta_cap;
@@ -640,10 +680,10 @@ __global__ void __launch_bounds__(512) k_contract_cta(
       }
     }
     __syncthreads();
-    for (u32 s = threadIdx.x; s < hsz; s += blockDim.x) {
-      if (keys[s] != kEmpty) {
+    for (u32 sl = threadIdx.x; sl < hsz; sl += blockDim.x) {
+      if (keys[sl] != kEmpty) {
         const i32 pos = atomicAdd(&s_count, 1);
-        out[pos] = ((u64)keys[s] << 32) | vals[s];
+        out[pos] = ((u64)keys[sl] << 32) | vals[sl];
       }
     }
     __syncthreads();
@@ -664,18 +704,12 @@ __global__ void __launch_bounds__(512) k_contract_cta(
   }
 }
 
-__global__ void k_max_heavy(const i32* __restrict__ heavy, const i32* __restrict__ nheavy,
-                            const i32* __restrict__ rowlen, i32* __restrict__ maxlen) {
-  const i32 nh = *nheavy;
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += (i64)gridDim.x * blockDim.x)
-    atomicMax(maxlen, rowlen[heavy[i]]);
-}
-
 // one thread per coarse row (rows are short; consecutive threads touch
 // consecutive rows)
-__global__ void k_copy_rows(i32 nc, const i32* __restrict__ ub, const i32* __restrict__ cnt,
+__global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__ ub, const i32* __restrict__ cnt,
                             const i32* __restrict__ cx, const i32* __restrict__ sadj,
                             const i32* __restrict__ swgt, i32* __restrict__ cadj, i32* __restrict__ cwgt) {
+  const i32 nc = *ncp;
   for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
     const i32 src = ub[c], dst = cx[c], len = cnt[c];
     for (i32 i = 0; i < len; ++i) {
@@ -685,96 +719,99 @@ __global__ void k_copy_rows(i32 nc, const i32* __restrict__ ub, const i32* __res
   }
 }
 
-__global__ void k_set_last(i32* cx, i32 nc, const i32* total) { cx[nc] = *total; }
+void ensure_arena(Handle& h, u64 words) {
+  if (h.arena && h.arena_words >= words) return;
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  if (h.arena) GKW_CUDA(cudaFree(h.arena));
+  h.arena = nullptr;
+  h.arena_words = 0;
+  GKW_CUDA(cudaMalloc(&h.arena, sizeof(ArenaHdr) + sizeof(u32) * words));
+  GKW_CUDA(cudaMemset(h.arena, 0, sizeof(ArenaHdr)));
+  h.arena_words = words;
+}
 
-void run_contract(Handle& h, const DevGraph& g, const i32* cmap, i32 nc, i32 cap, i32* cxadj,
-                  i32** cadjncy, i32** cadjwgt, i32* cvwgt, i64* mc, Pool& out_pool) {
+void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc, i32 nc_ub, i32 cap, i32* cxadj,
+                  i32* cadjncy, i32* cadjwgt, i32* cvwgt, i32* d_mc) {
   Pool::Mark mk = h.scratch.mark();
   const i32 n = g.n;
+  const i64 nu = (i64)nc_ub + 1;
   const u32 nb = ceil_div(std::max(n, 1), 256);
-  i32* rowlen = h.scratch.alloc_n<i32>(nc + 1);
-  i32* ub = h.scratch.alloc_n<i32>(nc + 1);
-  i32* mcnt = h.scratch.alloc_n<i32>(nc + 1);
-  i32* memtab = h.scratch.alloc_n<i32>((i64)nc * cap + 1);
-  i32* cnt = h.scratch.alloc_n<i32>(nc + 1);
-  i32* heavy = h.scratch.alloc_n<i32>(nc + 1);
-  i32* misc = h.scratch.alloc_n<i32>(8);   // [0] nheavy, [1] ub total, [2] mc, [3] max heavy len
+  i32* rowlen = h.scratch.alloc_n<i32>(nu);
+  i32* ub = h.scratch.alloc_n<i32>(nu);
+  i32* mcnt = h.scratch.alloc_n<i32>(nu);
+  i32* memtab = h.scratch.alloc_n<i32>((i64)nc_ub * cap + 1);
+  i32* cnt = h.scratch.alloc_n<i32>(nu);
+  i32* heavy = h.scratch.alloc_n<i32>(nu);
+  i32* misc = h.scratch.alloc_n<i32>(8);   // [0] heavy rows, [1] ub total
   i32* sadj = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
   i32* swgt = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
-  GKW_CUDA(cudaMemsetAsync(cvwgt, 0, sizeof(i32) * std::max(nc, 1), h.stream));
-  GKW_CUDA(cudaMemsetAsync(rowlen, 0, sizeof(i32) * (nc + 1), h.stream));
-  GKW_CUDA(cudaMemsetAsync(mcnt, 0, sizeof(i32) * (nc + 1), h.stream));
+  ensure_arena(h, u64(4) << 20);   // 16 MB of long-row tables to start with
+  GKW_CUDA(cudaMemsetAsync(cvwgt, 0, sizeof(i32) * std::max(nc_ub, 1), h.stream));
+  GKW_CUDA(cudaMemsetAsync(rowlen, 0, sizeof(i32) * nu, h.stream));
+  GKW_CUDA(cudaMemsetAsync(mcnt, 0, sizeof(i32) * nu, h.stream));
+  GKW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(i32) * nu, h.stream));
   GKW_CUDA(cudaMemsetAsync(misc, 0, sizeof(i32) * 8, h.stream));
-  if (n > 0) {
-    launch(k_coarse_accum, nb, 256, 0, h.stream, n, g.xadj, g.vwgt, cmap, cap, cvwgt, rowlen, mcnt, memtab);
-    GKW_CHECK_LAUNCH();
-  }
-  exclusive_scan_i32(h, rowlen, ub, nc, misc + 1);
-  // warp kernel: table capacity from the average row length
-  const double avgL = nc ? (double)g.m / nc : 0.0;
-  const u32 gridw = std::max<u32>(1, std::min<u32>(ceil_div(nc, 8), (u32)h.sm_count * 32));
-  if (nc > 0) {
-    if (avgL <= 48) {
-      constexpr int W = 128, WARPS = 8;
-      const size_t sm = sizeof(WarpTable<W>) * WARPS;
-      GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, 
-          nc, g.xadj, g.adjncy, g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
-    } else {
-      constexpr int W = 512, WARPS = 8;
-      const size_t sm = sizeof(WarpTable<W>) * WARPS;
-      GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, 
-          nc, g.xadj, g.adjncy, g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
-    }
-    GKW_CHECK_LAUNCH();
-    // heavy rows: shared-memory CTA table up to kCtaCap entries
-    // table of 2*kCtaCap slots (a power of two, so any L <= kCtaCap hashes
-    // into <= 2*kCtaCap slots) + kCtaCap sorted outputs: 96 KB
-    constexpr i32 kCtaCap = 4096;
-    const size_t csm = (size_t)kCtaCap * 2 * 4 * 2 + (size_t)kCtaCap * 8;
-    GKW_CUDA(cudaFuncSetAttribute(k_contract_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-    launch(k_contract_cta<false>, (u32)h.sm_count * 2, 512, csm, h.stream, 
-        heavy, misc, kCtaCap, g.xadj, g.adjncy, g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt,
-        cnt, nullptr, nullptr, nullptr, 0);
-    GKW_CHECK_LAUNCH();
-    // rows beyond the CTA table: global tables sized by the longest such row
-    launch(k_max_heavy, 64, 256, 0, h.stream, heavy, misc, rowlen, misc + 3);
-    GKW_CHECK_LAUNCH();
-    i32* hp = (i32*)h.h_pinned;
-    GKW_CUDA(cudaMemcpyAsync(hp, misc, sizeof(i32) * 4, cudaMemcpyDeviceToHost, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-    const i32 maxL = hp[3];
-    if (maxL > kCtaCap) {
-      i64 stride = 64;
-      while (stride < 2 * (i64)maxL) stride <<= 1;   // table size; out needs <= stride/2
-      const u32 nblk = (u32)h.sm_count;
-      u32* gk = h.scratch.alloc_n<u32>(nblk * stride * 2);
-      u32* gv = h.scratch.alloc_n<u32>(nblk * stride * 2);
-      u64* go = h.scratch.alloc_n<u64>(nblk * stride);
-      launch(k_contract_cta<true>, nblk, 512, 0, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy, g.adjwgt,
-                                                       cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt,
-                                                       cnt, gk, gv, go, stride);
-      GKW_CHECK_LAUNCH();
-    }
-  }
-  exclusive_scan_i32(h, cnt, cxadj, nc, misc + 2);
-  launch(k_set_last, 1, 1, 0, h.stream, cxadj, nc, misc + 2);
+  if (n > 0)
+    launch(k_coarse_accum, nb, 256, 0, h.stream, n, g.xadj, g.vwgt, cmap, cap, cvwgt, rowlen, mcnt, memtab, h.arena);
   GKW_CHECK_LAUNCH();
-  i32* hp = (i32*)h.h_pinned;
-  GKW_CUDA(cudaMemcpyAsync(hp, misc + 2, sizeof(i32), cudaMemcpyDeviceToHost, h.stream));
-  GKW_CUDA(cudaStreamSynchronize(h.stream));
-  *mc = hp[0];
-  if (*cadjncy == nullptr) {
-    *cadjncy = out_pool.alloc_n<i32>(std::max<i64>(*mc, 1));
-    *cadjwgt = out_pool.alloc_n<i32>(std::max<i64>(*mc, 1));
+  exclusive_scan_i32(h, rowlen, ub, nu, misc + 1);   // rows beyond n_c have length 0
+  const double avgL = nc_ub ? (double)g.m / nc_ub : 0.0;
+  const u32 gridw = std::max<u32>(1, std::min<u32>(ceil_div(std::max(nc_ub, 1), 8), (u32)h.sm_count * 32));
+  u32* words = reinterpret_cast<u32*>(h.arena + 1);
+  if (avgL <= 48) {
+    constexpr int W = 128, WARPS = 8;
+    const size_t sm = sizeof(WarpTable<W>) * WARPS;
+    GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, d_nc, g.xadj, g.adjncy, g.adjwgt, cmap,
+           memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
+  } else {
+    constexpr int W = 512, WARPS = 8;
+    const size_t sm = sizeof(WarpTable<W>) * WARPS;
+    GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, d_nc, g.xadj, g.adjncy, g.adjwgt, cmap,
+           memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
   }
-  if (nc > 0) {
-    launch(k_copy_rows, ceil_div(nc, 256), 256, 0, h.stream, nc, ub, cnt, cxadj, sadj, swgt, *cadjncy,
-           *cadjwgt);
-    GKW_CHECK_LAUNCH();
-  }
+  GKW_CHECK_LAUNCH();
+  // heavy rows: a shared-memory table up to kCtaCap entries, the arena beyond
+  // (2*kCtaCap table slots, a power of two, + kCtaCap sorted outputs: 96 KB)
+  constexpr i32 kCtaCap = 4096;
+  const size_t csm = (size_t)kCtaCap * 2 * 4 * 2 + (size_t)kCtaCap * 8;
+  GKW_CUDA(cudaFuncSetAttribute(k_contract_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  launch(k_contract_cta<false>, (u32)h.sm_count * 2, 512, csm, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
+         g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, h.arena, words, h.arena_words);
+  launch(k_contract_cta<true>, (u32)h.sm_count, 512, 0, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
+         g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, h.arena, words, h.arena_words);
+  GKW_CHECK_LAUNCH();
+  exclusive_scan_i32(h, cnt, cxadj, nu, d_mc);   // cxadj[n_c] = m_c (rows beyond n_c are empty)
+  if (nc_ub > 0)
+    launch(k_copy_rows, ceil_div(nc_ub, 256), 256, 0, h.stream, d_nc, ub, cnt, cxadj, sadj, swgt, cadjncy,
+           cadjwgt);
+  GKW_CHECK_LAUNCH();
   h.scratch.release(mk);
+}
+
+CoopState read_coop(Handle& h) {
+  CoopState* hc = reinterpret_cast<CoopState*>(h.h_pinned);
+  static_assert(sizeof(CoopState) + sizeof(ArenaHdr) + 8 <= 64 * sizeof(i64), "pinned staging too small");
+  GKW_CUDA(cudaMemcpyAsync(hc, h.coop, sizeof(CoopState), cudaMemcpyDeviceToHost, h.stream));
+  ArenaHdr* ha = reinterpret_cast<ArenaHdr*>(hc + 1);
+  if (h.arena) GKW_CUDA(cudaMemcpyAsync(ha, h.arena, sizeof(ArenaHdr), cudaMemcpyDeviceToHost, h.stream));
+  i32* hs = reinterpret_cast<i32*>(ha + 1);
+  if (h.scan) GKW_CUDA(cudaMemcpyAsync(hs, &h.scan->err, sizeof(i32), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  CoopState c = *hc;
+  c.arena_overflow = h.arena ? ha->overflow : 0;
+  c.arena_need = h.arena ? (i64)ha->need : 0;
+  c.scan_err = h.scan ? *hs : 0;
+  if (c.err || c.scan_err) {   // report once, leave the handle usable
+    GKW_CUDA(cudaMemsetAsync(h.coop, 0, sizeof(CoopState), h.stream));
+    if (h.scan) GKW_CUDA(cudaMemsetAsync(&h.scan->err, 0, sizeof(i32), h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+  }
+  if (c.err == 1) throw Error{GKW_E_INTERNAL, "cooperative kernel: grid barrier timed out"};
+  if (c.err == 2) throw Error{GKW_E_INTERNAL, "union-find did not converge"};
+  if (c.scan_err) throw Error{GKW_E_INTERNAL, "scan: look-back wait timed out"};
+  return c;
 }
 
 void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
@@ -782,17 +819,28 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
   u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
   run_match(h, g, cand);
-  out.uf_rounds = run_union_find(h, g.n, cand, keys);
+  run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
   out.cmap = h.hier.alloc_n<i32>(std::max(g.n, 1));
-  out.nc = run_group_map(h, g.n, keys, cap, out.cmap);
+  run_group_map(h, g.n, keys, cap, out.cmap, &h.coop->nc);
   h.scratch.release(mk);
-  if (out.nc == g.n) return;   // caller discards the level
-  out.cxadj = h.hier.alloc_n<i32>(out.nc + 1);
-  out.cvwgt = h.hier.alloc_n<i32>(std::max(out.nc, 1));
-  out.cadjncy = nullptr;
-  out.cadjwgt = nullptr;
-  run_contract(h, g, out.cmap, out.nc, cap, out.cxadj, &out.cadjncy, &out.cadjwgt, out.cvwgt, &out.mc,
-               h.hier);
+  // coarse arrays at upper bounds (n_c <= n, m_c <= m); one host sync per level
+  out.cxadj = h.hier.alloc_n<i32>((i64)g.n + 1);
+  out.cvwgt = h.hier.alloc_n<i32>(std::max(g.n, 1));
+  out.cadjncy = h.hier.alloc_n<i32>(std::max<i64>(g.m, 1));
+  out.cadjwgt = h.hier.alloc_n<i32>(std::max<i64>(g.m, 1));
+  run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
+               &h.coop->mc);
+  CoopState c = read_coop(h);
+  if (c.arena_overflow) {   // very long coarse rows: grow the arena and redo the step
+    ensure_arena(h, (u64)((double)(h.arena_words + (u64)c.arena_need) * 1.25) + 1024);
+    run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
+                 &h.coop->mc);
+    c = read_coop(h);
+    GKW_REQUIRE(!c.arena_overflow, GKW_E_INTERNAL, "long-row arena overflow after growth");
+  }
+  out.nc = c.nc;
+  out.mc = c.mc;
+  out.uf_rounds = c.uf_rounds;
 }
 
 }  // namespace gkw

@@ -132,59 +132,69 @@ __device__ __forceinline__ i32 block_exclusive_scan(i32 x, i32* s_warp, i32& tot
   return r;
 }
 
-__global__ void k_scan_reduce(const i32* __restrict__ in, i64 n, i32* __restrict__ partial) {
-  __shared__ i32 s_warp[33];
-  const i64 base = (i64)blockIdx.x * kScanTile + (i64)threadIdx.x * kScanItems;
-  i32 s = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i)
-    if (base + i < n) s += in[base + i];
-  i32 total;
-  block_exclusive_scan(s, s_warp, total);
-  if (threadIdx.x == 0) partial[blockIdx.x] = total;
-}
+// Single-pass scan with decoupled look-back.  Tile t publishes its aggregate
+// (status 1) and then its inclusive prefix (status 2) in a status word
+// (epoch << 34 | status << 32 | value); a word of an older epoch reads as
+// "not published".  Tiles take tickets from a persistent 64-bit counter in
+// launch order (tile = ticket - base, base = tickets handed out by earlier
+// calls), so a tile only waits on tiles that already hold an SM.  A wait
+// longer than kScanSpinCycles sets the error word and the tile continues
+// (the result is then reported as an error, never a hang).
+constexpr long long kScanSpinCycles = 2000000000ll;
 
-// single block: exclusive scan of the nb tile sums in place, grand total out
-__global__ void k_scan_partials(i32* __restrict__ partial, i32 nb, i32* __restrict__ total_out) {
+__global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const i32* in, i32* out, i64 n, i32* total,
+                                                             ScanState* ss, u64 base, u64 epoch, i32 ntiles) {
   __shared__ i32 s_warp[33];
-  i32 carry = 0;
-  for (i32 base = 0; base < nb; base += kScanTile) {
-    i32 v[kScanItems];
-    i32 s = 0;
-    const i32 b0 = base + threadIdx.x * kScanItems;
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-      v[i] = (b0 + i < nb) ? partial[b0 + i] : 0;
-      s += v[i];
-    }
-    i32 tot;
-    i32 off = block_exclusive_scan(s, s_warp, tot) + carry;
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-      if (b0 + i < nb) partial[b0 + i] = off;
-      off += v[i];
-    }
-    carry += tot;
-  }
-  if (threadIdx.x == 0 && total_out) *total_out = carry;
-}
-
-__global__ void k_scan_down(const i32* in, i32* out, i64 n, const i32* __restrict__ partial) {
-  __shared__ i32 s_warp[33];
-  const i64 base = (i64)blockIdx.x * kScanTile + (i64)threadIdx.x * kScanItems;
+  __shared__ i32 s_tile;
+  __shared__ i32 s_excl;
+  if (threadIdx.x == 0) s_tile = (i32)(atomicAdd((unsigned long long*)&ss->ticket, 1ull) - base);
+  __syncthreads();
+  const i32 tile = s_tile;
+  const i64 b0 = (i64)tile * kScanTile + (i64)threadIdx.x * kScanItems;
   i32 v[kScanItems];
-  i32 s = 0;
+  i32 sum = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    v[i] = (base + i < n) ? in[base + i] : 0;
-    s += v[i];
+    v[i] = (b0 + i < n) ? in[b0 + i] : 0;
+    sum += v[i];
   }
-  i32 tot;
-  i32 off = block_exclusive_scan(s, s_warp, tot) + partial[blockIdx.x];
+  i32 agg;
+  const i32 off = block_exclusive_scan(sum, s_warp, agg);
+  if (threadIdx.x == 0) {
+    unsigned long long* st = (unsigned long long*)ss->tiles;
+    const u64 tag = epoch << 34;
+    i32 excl = 0;
+    if (tile == 0) {
+      atomicExch(&st[0], (unsigned long long)(tag | (2ull << 32) | (u32)agg));
+    } else {
+      atomicExch(&st[tile], (unsigned long long)(tag | (1ull << 32) | (u32)agg));
+      i32 j = tile - 1;
+      const long long t0 = clock64();
+      while (j >= 0) {
+        const u64 w = (u64)atomicAdd(&st[j], 0ull);
+        const u32 status = (w >> 34) == epoch ? (u32)((w >> 32) & 3u) : 0u;
+        if (status == 0) {
+          if (clock64() - t0 > kScanSpinCycles) {
+            atomicExch(&ss->err, 1);
+            break;
+          }
+          continue;
+        }
+        excl += (i32)(u32)w;
+        if (status == 2) break;
+        --j;
+      }
+      atomicExch(&st[tile], (unsigned long long)(tag | (2ull << 32) | (u32)(excl + agg)));
+    }
+    s_excl = excl;
+    if (tile == ntiles - 1 && total) *total = excl + agg;
+  }
+  __syncthreads();
+  i32 run = off + s_excl;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    if (base + i < n) out[base + i] = off;
-    off += v[i];
+    if (b0 + i < n) out[b0 + i] = run;
+    run += v[i];
   }
 }
 
@@ -192,24 +202,29 @@ __global__ void k_set_i32(i32* p, i32 v) { *p = v; }
 
 void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total) {
   if (n <= 0) {
-    if (total) {
-      launch(k_set_i32, 1, 1, 0, h.stream, total, 0);
-      GKW_CHECK_LAUNCH();
-    }
+    if (total) launch(k_set_i32, 1, 1, 0, h.stream, total, 0);
+    GKW_CHECK_LAUNCH();
     return;
   }
-  const i64 nb64 = (n + kScanTile - 1) / kScanTile;
-  GKW_REQUIRE(nb64 < (i64)1 << 30, GKW_E_UNSUPPORTED, "scan too large");
-  const i32 nb = (i32)nb64;
-  Pool::Mark mk = h.scratch.mark();
-  i32* partial = h.scratch.alloc_n<i32>(nb);
-  launch(k_scan_reduce, nb, kScanThreads, 0, h.stream, in, n, partial);
+  const i64 nt64 = (n + kScanTile - 1) / kScanTile;
+  GKW_REQUIRE(nt64 < (i64)1 << 30, GKW_E_UNSUPPORTED, "scan too large");
+  const i32 nt = (i32)nt64;
+  if (h.scan_tiles_cap < nt) {
+    if (h.scan) GKW_CUDA(cudaFree(h.scan));
+    h.scan = nullptr;
+    const i32 cap = std::max(nt, 1024);
+    GKW_CUDA(cudaMalloc(&h.scan, sizeof(ScanState) + sizeof(u64) * (size_t)cap));
+    GKW_CUDA(cudaMemset(h.scan, 0, sizeof(ScanState) + sizeof(u64) * (size_t)cap));
+    h.scan_tiles_cap = cap;
+    h.scan_tickets = 0;
+    h.scan_epoch = 0;
+  }
+  h.scan_epoch += 1;
+  GKW_REQUIRE(h.scan_epoch < ((u64)1 << 29), GKW_E_INTERNAL, "scan epoch overflow");
+  launch(k_scan_1pass, nt, kScanThreads, 0, h.stream, in, out, n, total, h.scan, h.scan_tickets, h.scan_epoch,
+         nt);
   GKW_CHECK_LAUNCH();
-  launch(k_scan_partials, 1, kScanThreads, 0, h.stream, partial, nb, total);
-  GKW_CHECK_LAUNCH();
-  launch(k_scan_down, nb, kScanThreads, 0, h.stream, in, out, n, partial);
-  GKW_CHECK_LAUNCH();
-  h.scratch.release(mk);   // stream-ordered reuse is safe: later kernels run after these
+  h.scan_tickets += (u64)nt;
 }
 
 float balance_cap(i64 total_vwgt, i32 k, double eps) {

@@ -97,6 +97,43 @@ struct CoarsenOut {
   i32 uf_rounds = 0;
 };
 
+// Grid barrier words of a cooperative launch (see device_util.cuh).
+struct GridBarrier {
+  u32 count;
+  u32 gen;
+};
+
+// Device-side state of one handle shared by the cooperative kernels and the
+// per-level scalars read back once per level.
+struct CoopState {
+  GridBarrier bar;
+  i32 err;        // nonzero: a cooperative kernel timed out or ran away
+  i32 nc;         // coarse vertex count of the last coarsening step
+  i32 mc;         // coarse CSR entries of the last coarsening step
+  i32 uf_rounds;  // union-find round launches of the last coarsening step
+  i32 scan_err;
+  i32 arena_overflow;
+  i64 arena_need;
+};
+
+// Bump arena for the hash tables of very long coarse rows (handle-owned,
+// grown when a level reports overflow).
+struct ArenaHdr {
+  u64 used;
+  u64 need;
+  i32 overflow;
+  i32 pad;
+};
+
+// Single-pass scan state (one per handle): ticket counter, error word, tile
+// status words follow the header.
+struct ScanState {
+  u64 ticket;
+  i32 err;
+  i32 pad;
+  u64 tiles[1];
+};
+
 // The library handle: one stream, two pools (level hierarchy and scratch),
 // small pinned host staging, the device id.
 struct Handle {
@@ -107,6 +144,13 @@ struct Handle {
   Pool scratch;
   i64* h_pinned = nullptr;      // 64 pinned i64 slots for scalar readbacks
   i32 sm_count = 148;
+  ScanState* scan = nullptr;    // single-pass scan state
+  CoopState* coop = nullptr;    // cooperative-kernel state and per-level scalars
+  ArenaHdr* arena = nullptr;    // long-row hash tables: header + words
+  u64 arena_words = 0;
+  i32 scan_tiles_cap = 0;
+  u64 scan_tickets = 0;         // tickets handed out so far
+  u64 scan_epoch = 0;
   Handle() : hier(size_t(256) << 20), scratch(size_t(256) << 20) {}
 };
 
@@ -130,10 +174,19 @@ void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total);
 // ---- coarsening (coarsen.cu) ----
 void run_match(Handle& h, const DevGraph& g, i32* cand);
 // returns the number of round launches the reference's loop would make
-i32 run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out);
-i32 run_group_map(Handle& h, i32 n, const u64* keys, i32 group_cap, i32* cmap);
-void run_contract(Handle& h, const DevGraph& g, const i32* cmap, i32 nc, i32 group_cap,
-                  i32* cxadj, i32** cadjncy, i32** cadjwgt, i32* cvwgt, i64* mc, Pool& out_pool);
+// These run without host synchronisation; results that the host needs are
+// left in device memory (see CoopState) and read once per level.
+void run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out, i32* d_rounds);
+void run_group_map(Handle& h, i32 n, const u64* keys, i32 group_cap, i32* cmap, i32* d_nc);
+// Contraction with the coarse vertex count on the device (d_nc) and an upper
+// bound nc_ub on the host; cxadj needs nc_ub+1 entries, cadjncy/cadjwgt room
+// for g.m, cvwgt nc_ub.  *d_mc receives m_c.  Returns false if the long-row
+// arena overflowed (the caller grows it and runs the step again).
+void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc, i32 nc_ub, i32 group_cap,
+                  i32* cxadj, i32* cadjncy, i32* cadjwgt, i32* cvwgt, i32* d_mc);
+void ensure_arena(Handle& h, u64 words);
+// Reads the CoopState (one host sync) and throws on a recorded error.
+CoopState read_coop(Handle& h);
 void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out);
 
 // ---- refinement (refine.cu) ----

@@ -10,7 +10,7 @@
 // gain must be recomputed (moved vertices and their neighbours).
 //
 // The grid barrier is a counter + generation word; a CTA that waits longer
-// than kBarrierCycles sets the error word and every CTA leaves the kernel, so
+// than kGridBarrierCycles sets the error word and every CTA leaves the kernel, so
 // a fault in the round logic ends the launch with an error status instead of
 // a hang.  Data written by other CTAs within the launch is read with
 // ld.global.cg (L2, coherent) after the barrier.
@@ -20,7 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 
-#include "gkw_internal.cuh"
+#include "device_util.cuh"
 
 namespace gkw {
 
@@ -29,7 +29,6 @@ constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pa
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
 constexpr i32 kBadWords = kMaxMoveCap / 32;
 constexpr int kLevelThreads = 512;
-constexpr long long kBarrierCycles = 4000000000ll;   // ~2 s at 2 GHz
 constexpr i32 kStatSlots = GKW_MAX_LEVELS + 2;
 constexpr i32 kTraceCap = 4096;   // phase marks per level (diagnostic timeline)
 
@@ -53,10 +52,6 @@ struct RoundState {
   u32 epoch;
 };
 
-struct GridBarrier {
-  u32 count;
-  u32 gen;
-};
 
 struct LevelStatsDev {
   i32 rounds, brounds;
@@ -201,36 +196,6 @@ __device__ __forceinline__ void block_append64(bool pred, u64 val, u64* list, i3
   __syncthreads();
   if (pred) list[*s_base + local] = val;
   __syncthreads();
-}
-
-// Grid barrier (all CTAs of a cooperative launch).  Returns false when any
-// CTA has timed out; the caller then leaves the kernel.
-__device__ bool grid_barrier(GridBarrier* b, i32* err, i32* s_flag) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile u32* vgen = &b->gen;
-    const u32 g = *vgen;
-    __threadfence();
-    const u32 arrived = atomicAdd(&b->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      b->count = 0;
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    } else {
-      const long long t0 = clock64();
-      while (*vgen == g) {
-        if (clock64() - t0 > kBarrierCycles) {
-          atomicExch(err, 1);
-          break;
-        }
-        __nanosleep(20);
-      }
-    }
-    __threadfence();
-    *s_flag = *(volatile i32*)err;
-  }
-  __syncthreads();
-  return *s_flag == 0;
 }
 
 // ---------------------------------------------------------------------------
