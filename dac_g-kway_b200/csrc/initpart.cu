@@ -20,6 +20,9 @@
 // trial index) wins.  Seeds: trial t of sub-problem p0 starts at member
 // index mix(seed, p0, t) mod s.  Deterministic for a given seed.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
 
 #include "gkw_internal.cuh"
 
@@ -309,6 +312,13 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   GKW_CHECK_LAUNCH();
   i32 depth = 0;
   while ((1 << depth) < k) ++depth;
+  const bool trace = getenv("GKW_TRACE") && *getenv("GKW_TRACE") == '1';
+  std::vector<cudaEvent_t> ev;
+  if (trace) {
+    ev.resize(depth + 1);
+    for (auto& e : ev) GKW_CUDA(cudaEventCreate(&e));
+    GKW_CUDA(cudaEventRecord(ev[0], h.stream));
+  }
   for (i32 d = 0; d < depth; ++d) {
     const i32 a = d & 1, b = a ^ 1;
     GKW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(i32) * k, h.stream));
@@ -319,6 +329,18 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
                                                         cnt, off, mlist, degS, inR, conn, lo[b], hi[b], seed,
                                                         eps, trials, loc, frontier, fpos);
     GKW_CHECK_LAUNCH();
+    if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));
+  }
+  if (trace) {
+    GKW_CUDA(cudaEventSynchronize(ev[depth]));
+    fprintf(stderr, "[gkw trace] init n=%d k=%d:", n, k);
+    for (i32 d = 0; d < depth; ++d) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[d], ev[d + 1]);
+      fprintf(stderr, " d%d %.1fus", d, ms * 1e3);
+    }
+    fprintf(stderr, "\n");
+    for (auto& e : ev) cudaEventDestroy(e);
   }
   GKW_CUDA(cudaMemcpyAsync(d_part, lo[depth & 1], sizeof(i32) * n, cudaMemcpyDeviceToDevice, h.stream));
   GKW_CUDA(cudaStreamSynchronize(h.stream));

@@ -29,6 +29,8 @@ constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pa
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
 constexpr i32 kBadWords = kMaxMoveCap / 32;
 constexpr int kLevelThreads = 512;
+constexpr i32 kGreedySmemParts = 4096;   // balance greedy pass: part weights in smem up to this k
+constexpr i32 kGreedyWords = 3 * kMaxMoveCap + kGreedySmemParts;
 constexpr i32 kStatSlots = GKW_MAX_LEVELS + 2;
 constexpr i32 kTraceCap = 4096;   // phase marks per level (diagnostic timeline)
 
@@ -79,6 +81,7 @@ struct RefineCtx {
   i32* btarget = nullptr;
   i32* bgain = nullptr;
   i32* blist = nullptr;
+  u32* brem = nullptr;
   u32* epoch = nullptr;   // never reset: marks of earlier rounds stay stale
   GridBarrier* bar = nullptr;
   i32* err = nullptr;
@@ -110,6 +113,7 @@ struct LevelArgs {
   RoundState* st;
   u32* bmark;
   i32 *btarget, *bgain, *blist;
+  u32* brem;          // part weights of the balance greedy pass when k > kGreedySmemParts
   u32* epoch;
   GridBarrier* bar;
   i32* err;
@@ -352,7 +356,7 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
 // (uncoarsen.hpp:471-476 with move_request.hpp:36-41).  Block 0 only; more than
 // kSortMax candidates are streamed through shared memory keeping the running
 // top `cap`.  Resets the per-round counters.
-__device__ void ph_select(const LevelArgs& a, u64* s, bool balance_mode) {
+__device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, bool balance_mode) {
   if (blockIdx.x != 0) return;
   RoundState* st = a.st;
   const i32 cnt = ldc(&st->ccount);
@@ -406,15 +410,46 @@ __device__ void ph_select(const LevelArgs& a, u64* s, bool balance_mode) {
       bitonic(kSortMax);
     }
   }
-  for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
-  if (!balance_mode)
+  if (!balance_mode) {
+    for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
     for (i32 i = threadIdx.x; i < (B + 31) / 32; i += blockDim.x) st->bad[i] = 0;
+  } else {
+    // greedy pass in sorted order: take a move while its source is still
+    // overweight and its destination stays within the cap, skip the others.
+    // Sources and destinations of one round are disjoint (a destination had
+    // room, a source did not), so one running weight per part suffices.
+    i32* mv_src = greedy;
+    i32* mv_des = mv_src + kMaxMoveCap;
+    u32* mv_w = reinterpret_cast<u32*>(mv_des + kMaxMoveCap);
+    u32* rem = a.k <= kGreedySmemParts ? mv_w + kMaxMoveCap : a.brem;
+    for (i32 t = threadIdx.x; t < B; t += blockDim.x) {
+      const i32 v = (i32)(u32)s[t];
+      mv_src[t] = ldc(a.part + v);
+      mv_des[t] = ldc(a.btarget + v);
+      mv_w[t] = (u32)a.vwgt[v];
+    }
+    for (i32 q = threadIdx.x; q < a.k; q += blockDim.x) rem[q] = ldc(a.pw + q);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      i32 nsel = 0;
+      const float cap_f = a.bcap;
+      for (i32 t = 0; t < B; ++t) {
+        const u32 w = mv_w[t];
+        const i32 sp = mv_src[t], dp = mv_des[t];
+        if (over_cap(rem[sp], cap_f) && !over_cap(rem[dp] + w, cap_f)) {
+          rem[sp] -= w;
+          rem[dp] += w;
+          a.top[nsel++] = s[t];
+        }
+      }
+      st->firstbad = nsel;   // moves 0..nsel-1 of top are applied
+    }
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     st->B = B;
     st->ccount = 0;
     st->ucount = 0;
-    if (balance_mode) st->firstbad = B;
   }
 }
 
@@ -562,15 +597,17 @@ __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
 // ---------------------------------------------------------------------------
 // Balance rounds (default mode; the reference has none -- an overweight part
 // is only reported, cuda_check.hpp:105-113).
-//   prep      lightest part (ties: smaller id), new round epoch   (block 0)
-//   eval      boundary vertices of overweight parts: best neighbouring part
-//             with room by signed gain ed_q - id (ties: smaller q), else the
-//             lightest part if it has room; marks candidates
+//   prep      lightest part (ties: smaller id), new round epoch, stop when no
+//             part is overweight                                  (block 0)
+//   filter    boundary vertices of overweight parts -> list
+//   eval      per listed vertex (one warp): best neighbouring part with room
+//             by signed gain ed_q - id (ties: smaller q), else the lightest
+//             part if it has room; marks candidates
 //   emit      candidates without a smaller-id candidate neighbour -> keys
-//   select    sort by (gain desc, id asc), cap
-//   check     per part: first move index whose source is no longer
-//             overweight before it or whose destination overflows
-//   apply     the prefix before that index, flag U; then the gain update
+//   select    sort by (gain desc, id asc), cap, then a greedy pass in that
+//             order keeps each move whose source is still overweight and
+//             whose destination stays within the cap          (block 0)
+//   apply     the kept moves, flag U; then the gain update
 // ---------------------------------------------------------------------------
 __device__ void ph_bal_prep(const LevelArgs& a, u64* s_tmp) {
   if (blockIdx.x != 0) return;
@@ -691,52 +728,6 @@ __device__ void ph_bal_emit(const LevelArgs& a) {
   }
 }
 
-// Part p: exclusive prefix of weight leaving p, inclusive prefix of weight
-// entering p, over the sorted moves; the first move that leaves p while p is
-// no longer overweight, or enters p beyond the cap, bounds the applied prefix.
-__device__ void ph_check_balance(const LevelArgs& a, u32* s_warp) {
-  RoundState* st = a.st;
-  const i32 B = ldc(&st->B);
-  const float cap = a.bcap;
-  for (i32 p = blockIdx.x; p < a.k; p += gridDim.x) {
-    u32 o_e[kIT], i_e[kIT];
-    bool o_f[kIT], i_f[kIT];
-    u32 so = 0, si = 0;
-#pragma unroll
-    for (int i = 0; i < kIT; ++i) {
-      const i32 j = threadIdx.x * kIT + i;
-      o_e[i] = 0;
-      i_e[i] = 0;
-      o_f[i] = false;
-      i_f[i] = false;
-      if (j < B) {
-        const i32 v = (i32)(u32)ldc(a.top + j);
-        const u32 w = (u32)a.vwgt[v];
-        if (ldc(a.part + v) == p) { o_e[i] = w; o_f[i] = true; }
-        if (ldc(a.btarget + v) == p) { i_e[i] = w; i_f[i] = true; }
-      }
-      so += o_e[i];
-      si += i_e[i];
-    }
-    u32 t1, t2;
-    u32 out_ex = block_exscan_u32(so, s_warp, t1);
-    u32 in_in = block_exscan_u32(si, s_warp, t2);
-    const u32 base = ldc(a.pw + p);
-    i32 first = INT_MAX;
-#pragma unroll
-    for (int i = 0; i < kIT; ++i) {
-      const i32 j = threadIdx.x * kIT + i;
-      in_in += i_e[i];
-      if (j < B) {
-        if (o_f[i] && !over_cap(base - out_ex, cap)) first = j < first ? j : first;
-        if (i_f[i] && over_cap(base + in_in, cap)) first = j < first ? j : first;
-      }
-      out_ex += o_e[i];
-    }
-    if (first != INT_MAX) atomicMin(&st->firstbad, first);
-  }
-}
-
 __device__ void ph_apply_balance(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
   const i32 pos = ldc(&st->firstbad) - 1;
@@ -774,7 +765,8 @@ __device__ void ph_apply_balance(const LevelArgs& a, UStage& S) {
 __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   u64* s_sort = reinterpret_cast<u64*>(smem_raw);                  // kSortMax u64
-  u32* acc_all = reinterpret_cast<u32*>(smem_raw + kSortMax * 8);  // acc_warps * k u32
+  i32* greedy = reinterpret_cast<i32*>(smem_raw + kSortMax * 8);   // kGreedyWords
+  u32* acc_all = reinterpret_cast<u32*>(greedy + kGreedyWords);    // acc_warps * k u32
   __shared__ u32 s_warp[33];
   __shared__ u64 s_tmp[32];
   __shared__ i32 s_flag;
@@ -820,13 +812,10 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       ph_bal_emit(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 11);
-      ph_select(a, s_sort, true);
+      ph_select(a, s_sort, greedy, true);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 12);
       if (ldc(&st->bdone)) break;
-      ph_check_balance(a, s_warp);
-      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
-      trace_mark(a, 13);
       ph_apply_balance(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 14);
@@ -845,7 +834,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       ph_candidates(a, &s_cnt, &s_base);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 20);
-      ph_select(a, s_sort, false);
+      ph_select(a, s_sort, greedy, false);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 21);
       if (ldc(&st->done)) break;
@@ -910,6 +899,7 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->btarget = P.alloc_n<i32>(n);
   c->bgain = P.alloc_n<i32>(n);
   c->blist = P.alloc_n<i32>(n);
+  c->brem = P.alloc_n<u32>(c->k);
   c->epoch = P.alloc_n<u32>(1);
   c->bar = P.alloc_n<GridBarrier>(1);
   c->err = P.alloc_n<i32>(1);
@@ -925,10 +915,10 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   GKW_CUDA(cudaMemsetAsync(c->err, 0, sizeof(i32), h.stream));
   GKW_CUDA(cudaMemsetAsync(c->stats, 0, sizeof(LevelStatsDev) * kStatSlots, h.stream));
   // per-warp part-connection rows: as many warps as fit beside the sort buffer
-  const size_t budget = 160 * 1024;
+  const size_t budget = 120 * 1024;
   const i32 w = (i32)std::min<size_t>(kLevelThreads / 32, budget / (4 * (size_t)c->k));
   c->acc_warps = std::max(1, w);
-  c->smem = (size_t)kSortMax * 8 + (size_t)c->acc_warps * c->k * 4;
+  c->smem = (size_t)kSortMax * 8 + (size_t)kGreedyWords * 4 + (size_t)c->acc_warps * c->k * 4;
   GKW_CUDA(cudaFuncSetAttribute(k_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
   int bps = 0;
   GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_level, kLevelThreads, c->smem));
@@ -1048,6 +1038,7 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.btarget = c->btarget;
   a.bgain = c->bgain;
   a.blist = c->blist;
+  a.brem = c->brem;
   a.epoch = c->epoch;
   a.bar = c->bar;
   a.err = c->err;

@@ -469,16 +469,21 @@ static i32 balance_level(RefineState& s, float cap, i32 move_cap, i64* moves_out
       return a.v < b.v;
     });
     const i32 B = (i32)std::min<size_t>(buf.size(), (size_t)move_cap);
+    // greedy pass in sorted order: a move is taken while its source is still
+    // overweight and its destination stays within the cap; others are skipped
     std::vector<u32> outw(s.k, 0), inw(s.k, 0);
-    i32 pos = B - 1;
+    std::vector<BalMove> take;
     for (i32 t = 0; t < B; ++t) {
       const u32 w = (u32)s.vwgt[buf[t].v];
       const bool src_over = (float)(u32)(s.pw[buf[t].src] - outw[buf[t].src]) > cap;
       const bool des_ok = !((float)(u32)(s.pw[buf[t].des] + inw[buf[t].des] + w) > cap);
-      if (!src_over || !des_ok) { pos = t - 1; break; }
+      if (!src_over || !des_ok) continue;
       outw[buf[t].src] += w;
       inw[buf[t].des] += w;
+      take.push_back(buf[t]);
     }
+    buf.swap(take);
+    const i32 pos = (i32)buf.size() - 1;
     for (i32 t = 0; t <= pos; ++t) {
       const u32 v = buf[t].v, w = (u32)s.vwgt[v];
       s.pw[buf[t].src] -= w;
