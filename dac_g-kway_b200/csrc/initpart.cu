@@ -73,14 +73,186 @@ __device__ __forceinline__ u64 move_key2(i32 g, i32 idx) {
 
 __device__ __forceinline__ i32 key_idx(u64 key) { return (i32)(0x3fffffffu - (u32)(key & 0x3fffffffu)); }
 
+// Topology of one sub-problem in local (member) indices: row i holds the
+// member's neighbours inside the sub-problem.
+struct LocalTopo {
+  const i32* rb;     // row start in nb/nw
+  const i32* rn;     // neighbours inside the sub-problem
+  const i32* nb;     // local neighbour index
+  const i32* nw;     // edge weight
+  const i32* degS;   // weight to other members
+  const i32* vw;     // vertex weight
+};
+
+struct TrialState {
+  i32* C;      // connection weight to the region R
+  i32* R;      // in R
+  i32* F;      // frontier list
+  i32* posF;   // position in F
+};
+
+// One GGGP trial by one warp (growth then positive-gain refinement); see the
+// file comment for the rules.  Returns the trial's cut and |W(R) - TL|.
+__device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL, i64 WS, i64 capL,
+                           i64 capR, i64& cut_out, i64& dev_out) {
+  const int lane = threadIdx.x & 31;
+  i32* C = S.C;
+  i32* R = S.R;
+  i32* F = S.F;
+  i32* posF = S.posF;
+  for (i32 i = lane; i < s; i += 32) {
+    R[i] = 0;
+    C[i] = 0;
+  }
+  __syncwarp();
+  i64 wR = 0;
+  i32 nF = 0;
+  // ---- growth: F = members outside R with conn > 0; a frontier member
+  // always outranks a non-frontier one, so the argmax over F equals the argmax
+  // over all unassigned members, and the full scan is only needed when F is
+  // empty
+  for (i32 step = 0; step < s; ++step) {
+    if (step > 0) {
+      u64 best = 0;
+      if (nF > 0) {
+        for (i32 f = lane; f < nF; f += 32) {
+          const i32 i = F[f];
+          const i32 c = C[i];
+          const u64 key = grow_key(true, 2 * c - T.degS[i], i);
+          best = best > key ? best : key;
+        }
+      } else {
+        for (i32 i = lane; i < s; i += 32) {
+          if (!R[i]) {
+            const i32 c = C[i];
+            const u64 key = grow_key(c > 0, 2 * c - T.degS[i], i);
+            best = best > key ? best : key;
+          }
+        }
+      }
+      best = warp_max_u64(best);
+      if (best == 0) break;
+      pick = key_idx(best);
+      const i64 vw = (u32)T.vw[pick];
+      if (wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
+    }
+    const i32 cp = C[pick];
+    if (lane == 0) {
+      R[pick] = 1;
+      if (cp > 0) {   // leave the frontier (swap-remove)
+        const i32 at = posF[pick];
+        const i32 last = F[nF - 1];
+        F[at] = last;
+        posF[last] = at;
+      }
+    }
+    if (cp > 0) --nF;
+    wR += (u32)T.vw[pick];
+    __syncwarp();
+    const i32 rb = T.rb[pick], rn = T.rn[pick];
+    for (i32 j0 = 0; j0 < rn; j0 += 32) {
+      const i32 j = j0 + lane;
+      bool join = false;
+      i32 u = 0;
+      if (j < rn) {
+        u = T.nb[rb + j];
+        const i32 w = T.nw[rb + j];
+        const i32 old = C[u];
+        C[u] = old + w;
+        join = !R[u] && old <= 0 && old + w > 0;
+      }
+      const u32 m = __ballot_sync(kFull32, join);
+      if (join) {
+        const i32 at = nF + __popc(m & ((1u << lane) - 1));
+        F[at] = u;
+        posF[u] = at;
+      }
+      nF += __popc(m);
+    }
+    __syncwarp();
+    if (wR >= TL) break;
+  }
+  // ---- refinement: positive-gain moves within the side caps ----
+  const i32 max_moves = s / 4 + 32;
+  for (i32 mv = 0; mv < max_moves; ++mv) {
+    u64 best = 0;
+    for (i32 i = lane; i < s; i += 32) {
+      const i32 r = R[i];
+      const i32 c = C[i], d = T.degS[i];
+      const i32 g = r ? (d - 2 * c) : (2 * c - d);
+      if (g <= 0) continue;
+      const i64 vw = (u32)T.vw[i];
+      const bool ok = r ? ((WS - wR) + vw <= capR) : (wR + vw <= capL);
+      if (!ok) continue;
+      const u64 key = move_key2(g, i);
+      best = best > key ? best : key;
+    }
+    best = warp_max_u64(best);
+    if (best == 0) break;
+    const i32 i = key_idx(best);
+    const i32 r = R[i];
+    __syncwarp();
+    if (lane == 0) R[i] = r ^ 1;
+    wR += r ? -(i64)(u32)T.vw[i] : (i64)(u32)T.vw[i];
+    const i32 sign = r ? -1 : 1;
+    const i32 rb = T.rb[i], rn = T.rn[i];
+    for (i32 j = lane; j < rn; j += 32) C[T.nb[rb + j]] += sign * T.nw[rb + j];
+    __syncwarp();
+  }
+  i64 cut = 0;
+  for (i32 i = lane; i < s; i += 32)
+    if (R[i]) cut += T.degS[i] - C[i];
+  cut = warp_sum_i64(cut);
+  cut_out = cut;
+  dev_out = wR > TL ? wR - TL : TL - wR;
+}
+
+// Exclusive scan of a[0..s) in shared memory by the whole block (total out).
+__device__ i32 block_exscan_smem(i32* a, i32 s, i32* s_warp) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  i32 carry = 0;
+  for (i32 base = 0; base < s; base += blockDim.x) {
+    const i32 i = base + threadIdx.x;
+    const i32 x = i < s ? a[i] : 0;
+    i32 inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const i32 y = __shfl_up_sync(kFull32, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      const i32 w = lane < nw ? s_warp[lane] : 0;
+      i32 wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const i32 y = __shfl_up_sync(kFull32, wi, o);
+        if (lane >= o) wi += y;
+      }
+      if (lane < nw) s_warp[lane] = wi - w;
+      if (lane == nw - 1) s_warp[32] = wi;
+    }
+    __syncthreads();
+    if (i < s) a[i] = carry + inc - x + s_warp[wid];
+    carry += s_warp[32];
+    __syncthreads();
+  }
+  return carry;
+}
+
+constexpr size_t kGggpSmem = 200 * 1024;   // dynamic shared memory of the depth kernel
+
 __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     i32 n, const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
     const i32* __restrict__ vwgt, const i32* __restrict__ lo, const i32* __restrict__ hi,
-    const i32* __restrict__ cnt, const i32* __restrict__ off, i32* __restrict__ mlist,
-    i32* __restrict__ degS, i32* __restrict__ inR, i32* __restrict__ conn, i32* __restrict__ lo_out,
-    i32* __restrict__ hi_out, u64 seed, double eps, i32 trials, i32* __restrict__ loc, i32* __restrict__ frontier,
-    i32* __restrict__ fpos) {
+    const i32* __restrict__ cnt, const i32* __restrict__ off, i32* __restrict__ mlist, i32* __restrict__ loc,
+    i32* __restrict__ lo_out, i32* __restrict__ hi_out, u64 seed, double eps, i32 trials,
+    i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_cnt;
+  __shared__ i32 s_warp[33];
   __shared__ i64 s_wsum[kInitTrials];
   __shared__ i64 s_cut[kInitTrials];
   __shared__ i64 s_dev[kInitTrials];
@@ -89,21 +261,21 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   const i32 s = cnt[p0];
   if (s == 0) return;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  i32* M = mlist + off[p0];
+  const i32 base_off = off[p0];
+  i32* M = mlist + base_off;
   // deterministic member list: all vertices with lo == p0, in id order
-  __shared__ i32 s_wc[kInitTrials];
   if (threadIdx.x == 0) s_cnt = 0;
   __syncthreads();
   for (i32 base = 0; base < n; base += blockDim.x) {
     const i32 v = base + threadIdx.x;
     const bool mine = v < n && lo[v] == p0;
     const u32 bal = __ballot_sync(kFull32, mine);
-    if (lane == 0) s_wc[wid] = __popc(bal);
+    if (lane == 0) s_warp[wid] = __popc(bal);
     __syncthreads();
     i32 woff = 0, tot = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      if (w < wid) woff += s_wc[w];
-      tot += s_wc[w];
+      if (w < wid) woff += s_warp[w];
+      tot += s_warp[w];
     }
     if (mine) {
       const i32 idx = s_cnt + woff + __popc(bal & ((1u << lane) - 1));
@@ -123,150 +295,113 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     return;
   }
   const i32 pm = p0 + (p1 - p0) / 2;
-  // deg_S and W(S)
-  i64 wpart = 0;
+  // per member: neighbours inside the sub-problem, weight to them, W(S)
+  i64 wpart = 0, epart = 0;
   for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
     const i32 v = M[i];
-    i32 d = 0;
+    i32 d = 0, c = 0;
     for (i32 e = xadj[v]; e < xadj[v + 1]; ++e)
-      if (lo[adjncy[e]] == p0) d += adjwgt[e];
-    degS[v] = d;
+      if (lo[adjncy[e]] == p0) {
+        d += adjwgt[e];
+        ++c;
+      }
+    g_rn[base_off + i] = c;
+    g_deg[base_off + i] = d;
+    g_vw[base_off + i] = vwgt[v];
     wpart += (u32)vwgt[v];
+    epart += c;
   }
   wpart = warp_sum_i64(wpart);
-  if (lane == 0) s_wsum[wid] = wpart;
+  epart = warp_sum_i64(epart);
+  if (lane == 0) {
+    s_wsum[wid] = wpart;
+    s_cut[wid] = epart;
+  }
   __syncthreads();
-  i64 WS = 0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) WS += s_wsum[w];
+  i64 WS = 0, ES = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    WS += s_wsum[w];
+    ES += s_cut[w];
+  }
+  __syncthreads();
   const i64 TL = WS * (pm - p0) / (p1 - p0);
   const i64 capL = (i64)((double)TL * (1.0 + eps * 0.5));
   const i64 capR = (i64)((double)(WS - TL) * (1.0 + eps * 0.5));
-
+  // shared memory when the local CSR and the trials' state fit
+  const size_t need = sizeof(i32) * ((size_t)4 * s + 2 * (size_t)ES + (size_t)4 * s * trials);
+  const bool in_smem = need <= kGggpSmem;   // block-uniform
+  LocalTopo T;
+  i32 *rb, *rn, *deg, *vw, *nb, *nw, *state;
+  if (in_smem) {
+    i32* p = reinterpret_cast<i32*>(smem_raw);
+    rb = p; p += s;
+    rn = p; p += s;
+    deg = p; p += s;
+    vw = p; p += s;
+    nb = p; p += ES;
+    nw = p; p += ES;
+    state = p;
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
+      rn[i] = g_rn[base_off + i];
+      rb[i] = rn[i];
+      deg[i] = g_deg[base_off + i];
+      vw[i] = g_vw[base_off + i];
+    }
+    __syncthreads();
+    block_exscan_smem(rb, s, s_warp);
+  } else {
+    // rows in the global arrays at the members' own CSR positions
+    rb = g_rb + base_off;
+    rn = g_rn + base_off;
+    deg = g_deg + base_off;
+    vw = g_vw + base_off;
+    nb = g_nb;
+    nw = g_nw;
+    state = nullptr;
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) rb[i] = xadj[M[i]];
+    __syncthreads();
+  }
+  for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
+    const i32 v = M[i];
+    i32 j = rb[i];
+    for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
+      const i32 u = adjncy[e];
+      if (lo[u] == p0) {
+        nb[j] = loc[u];
+        nw[j] = adjwgt[e];
+        ++j;
+      }
+    }
+  }
+  __syncthreads();
+  T.rb = rb;
+  T.rn = rn;
+  T.nb = nb;
+  T.nw = nw;
+  T.degS = deg;
+  T.vw = vw;
   const i32 t = wid;
   if (t < trials) {
-    i32* R = inR + (i64)t * n;
-    i32* C = conn + (i64)t * n;
-    for (i32 i = lane; i < s; i += 32) {
-      R[M[i]] = 0;
-      C[M[i]] = 0;
+    TrialState S;
+    if (in_smem) {
+      i32* q = state + (size_t)t * 4 * s;
+      S.C = q;
+      S.R = q + s;
+      S.F = q + 2 * s;
+      S.posF = q + 3 * s;
+    } else {
+      i32* q = g_state + (size_t)t * 4 * n;   // [C | R | F | posF] of n each, this sub-problem at base_off
+      S.C = q + base_off;
+      S.R = q + n + base_off;
+      S.F = q + 2 * (size_t)n + base_off;
+      S.posF = q + 3 * (size_t)n + base_off;
     }
-    __syncwarp();
-    i64 wR = 0;
-    // ---- growth ----
-    // F = the members outside R with conn > 0 (the frontier).  A frontier
-    // vertex always outranks a non-frontier one, so while F is not empty the
-    // argmax over F equals the argmax over all unassigned members; the full
-    // scan is only needed when F is empty.
-    // F holds at most s entries: this sub-problem's slice [off, off + s) of
-    // the trial's list (sub-problems of one depth run concurrently)
-    i32* F = frontier + (i64)t * n + off[p0];
-    i32* posF = fpos + (i64)t * n;
-    i32 nF = 0;
-    i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0 * 1315423911ull + (u64)t) % (u32)s);
-    for (i32 step = 0; step < s; ++step) {
-      if (step > 0) {
-        u64 best = 0;
-        if (nF > 0) {
-          for (i32 f = lane; f < nF; f += 32) {
-            const i32 v = F[f];
-            const i32 c = C[v];
-            const u64 key = grow_key(true, 2 * c - degS[v], loc[v]);
-            best = best > key ? best : key;
-          }
-        } else {
-          for (i32 i = lane; i < s; i += 32) {
-            const i32 v = M[i];
-            if (!R[v]) {
-              const i32 c = C[v];
-              const u64 key = grow_key(c > 0, 2 * c - degS[v], i);
-              best = best > key ? best : key;
-            }
-          }
-        }
-        best = warp_max_u64(best);
-        if (best == 0) break;
-        pick = key_idx(best);
-        const i64 vw = (u32)vwgt[M[pick]];
-        if (wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
-      }
-      const i32 v = M[pick];
-      // leave the frontier (swap-remove), enter R
-      if (lane == 0) {
-        R[v] = 1;
-        if (C[v] > 0) {
-          const i32 at = posF[v];
-          const i32 last = F[nF - 1];
-          F[at] = last;
-          posF[last] = at;
-        }
-      }
-      if (C[v] > 0) --nF;
-      wR += (u32)vwgt[v];
-      __syncwarp();
-      // neighbours gain connection; those reaching conn > 0 join the frontier
-      for (i32 e0 = xadj[v]; e0 < xadj[v + 1]; e0 += 32) {
-        const i32 e = e0 + lane;
-        bool join = false;
-        i32 u = 0;
-        if (e < xadj[v + 1]) {
-          u = adjncy[e];
-          if (lo[u] == p0) {
-            const i32 old = C[u];
-            C[u] = old + adjwgt[e];
-            join = !R[u] && old <= 0 && old + adjwgt[e] > 0;
-          }
-        }
-        const u32 m = __ballot_sync(kFull32, join);
-        if (join) {
-          const i32 at = nF + __popc(m & ((1u << lane) - 1));
-          F[at] = u;
-          posF[u] = at;
-        }
-        nF += __popc(m);
-      }
-      __syncwarp();
-      if (wR >= TL) break;
-    }
-    // ---- refinement: positive-gain moves within the side caps ----
-    const i32 max_moves = s / 4 + 32;
-    for (i32 mv = 0; mv < max_moves; ++mv) {
-      u64 best = 0;
-      for (i32 i = lane; i < s; i += 32) {
-        const i32 v = M[i];
-        const i32 r = R[v];
-        const i32 c = C[v], d = degS[v];
-        const i32 g = r ? (d - 2 * c) : (2 * c - d);
-        if (g <= 0) continue;
-        const i64 vw = (u32)vwgt[v];
-        const bool ok = r ? ((WS - wR) + vw <= capR) : (wR + vw <= capL);
-        if (!ok) continue;
-        const u64 key = move_key2(g, i);
-        best = best > key ? best : key;
-      }
-      best = warp_max_u64(best);
-      if (best == 0) break;
-      const i32 v = M[key_idx(best)];
-      const i32 r = R[v];
-      __syncwarp();
-      if (lane == 0) R[v] = r ^ 1;
-      wR += r ? -(i64)(u32)vwgt[v] : (i64)(u32)vwgt[v];
-      const i32 sign = r ? -1 : 1;
-      for (i32 e = xadj[v] + lane; e < xadj[v + 1]; e += 32) {
-        const i32 u = adjncy[e];
-        if (lo[u] == p0) C[u] += sign * adjwgt[e];
-      }
-      __syncwarp();
-    }
-    // ---- cut of this trial ----
-    i64 cut = 0;
-    for (i32 i = lane; i < s; i += 32) {
-      const i32 v = M[i];
-      if (R[v]) cut += degS[v] - C[v];
-    }
-    cut = warp_sum_i64(cut);
+    const i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0 * 1315423911ull + (u64)t) % (u32)s);
+    i64 cut, dev;
+    gggp_trial(T, S, s, pick, TL, WS, capL, capR, cut, dev);
     if (lane == 0) {
       s_cut[t] = cut;
-      s_dev[t] = wR > TL ? wR - TL : TL - wR;
+      s_dev[t] = dev;
     }
   }
   __syncthreads();
@@ -277,10 +412,10 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     s_best = b;
   }
   __syncthreads();
-  const i32* R = inR + (i64)s_best * n;
+  const i32* Rb = in_smem ? state + (size_t)s_best * 4 * s + s : g_state + (size_t)s_best * 4 * n + n + base_off;
   for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
     const i32 v = M[i];
-    if (R[v]) { lo_out[v] = p0; hi_out[v] = pm; }
+    if (Rb[i]) { lo_out[v] = p0; hi_out[v] = pm; }
     else { lo_out[v] = pm; hi_out[v] = p1; }
   }
 }
@@ -301,12 +436,15 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   i32* cnt = h.scratch.alloc_n<i32>(k);
   i32* off = h.scratch.alloc_n<i32>(k);
   i32* mlist = h.scratch.alloc_n<i32>(n);
-  i32* degS = h.scratch.alloc_n<i32>(n);
-  i32* inR = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
-  i32* conn = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
   i32* loc = h.scratch.alloc_n<i32>(n);
-  i32* frontier = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
-  i32* fpos = h.scratch.alloc_n<i32>((i64)kInitTrials * n);
+  i32* g_rb = h.scratch.alloc_n<i32>(n);
+  i32* g_rn = h.scratch.alloc_n<i32>(n);
+  i32* g_deg = h.scratch.alloc_n<i32>(n);
+  i32* g_vw = h.scratch.alloc_n<i32>(n);
+  i32* g_nb = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
+  i32* g_nw = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
+  i32* g_state = h.scratch.alloc_n<i32>((size_t)kInitTrials * 4 * n);
+  GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
   const u32 nb = ceil_div(n, 256);
   launch(k_init_fill, nb, 256, 0, h.stream, n, lo[0], hi[0], k);
   GKW_CHECK_LAUNCH();
@@ -325,9 +463,9 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     launch(k_init_count, nb, 256, 0, h.stream, n, lo[a], cnt);
     GKW_CHECK_LAUNCH();
     exclusive_scan_i32(h, cnt, off, k, nullptr);
-    launch(k_gggp_depth, k, kInitTrials * 32, 0, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a], hi[a],
-                                                        cnt, off, mlist, degS, inR, conn, lo[b], hi[b], seed,
-                                                        eps, trials, loc, frontier, fpos);
+    launch(k_gggp_depth, k, kInitTrials * 32, kGggpSmem, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a],
+           hi[a], cnt, off, mlist, loc, lo[b], hi[b], seed, eps, trials, g_rb, g_rn, g_deg, g_vw, g_nb, g_nw,
+           g_state);
     GKW_CHECK_LAUNCH();
     if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));
   }
@@ -343,8 +481,7 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     for (auto& e : ev) cudaEventDestroy(e);
   }
   GKW_CUDA(cudaMemcpyAsync(d_part, lo[depth & 1], sizeof(i32) * n, cudaMemcpyDeviceToDevice, h.stream));
-  GKW_CUDA(cudaStreamSynchronize(h.stream));
-  h.scratch.release(mk);
+  h.scratch.release(mk);   // stream order keeps the scratch alive for the queued work
 }
 
 }  // namespace gkw

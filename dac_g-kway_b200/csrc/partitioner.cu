@@ -156,13 +156,9 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   }
   refine_init_coarsest(h, rc, cg, cpart);
   i64* d_metrics = h.hier.alloc_n<i64>(k + 2);   // [0] cut, [1] bad-part flag, [2..k+2) part weights
-  i64 init_cut = 0;
-  if (stats) {   // cut of the initial partition itself (before any balance move)
-    compute_cut_pw(h, cg, refine_part(rc), k, d_metrics, d_metrics + 2);
-    GKW_CUDA(cudaMemcpyAsync(h.h_pinned, d_metrics, sizeof(i64), cudaMemcpyDeviceToHost, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-    init_cut = h.h_pinned[0];
-  }
+  i64* d_init = h.hier.alloc_n<i64>(k + 2);      // the same for the initial partition
+  if (stats)   // cut of the initial partition itself (before any balance move), read at the end
+    compute_cut_pw(h, cg, refine_part(rc), k, d_init, d_init + 2);
   const i32 nl = (i32)lv.size();
   if (opt.enforce_balance) {
     LevelJob j;
@@ -185,7 +181,6 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     level_run(h, rc, lv[L].g, j, L);
   }
   GKW_CUDA(cudaEventRecord(tm.ev[3], h.stream));
-  std::vector<RefineLevelStats> rs = level_stats(h, rc, nl);
   // ---- output and final metrics (graph_partitioner.hpp:194-202) ----
   if (g0.n) {
     GKW_CUDA(cudaMemcpyAsync(d_part_out, refine_part(rc), sizeof(i32) * g0.n, cudaMemcpyDeviceToDevice,
@@ -194,8 +189,11 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   compute_cut_pw(h, g0, d_part_out, k, d_metrics, d_metrics + 2);
   std::vector<i64> hm(k + 2);
   GKW_CUDA(cudaMemcpyAsync(hm.data(), d_metrics, sizeof(i64) * (k + 2), cudaMemcpyDeviceToHost, h.stream));
+  i64 init_cut = 0;
+  if (stats) GKW_CUDA(cudaMemcpyAsync(&init_cut, d_init, sizeof(i64), cudaMemcpyDeviceToHost, h.stream));
   GKW_CUDA(cudaEventRecord(tm.ev[4], h.stream));
-  GKW_CUDA(cudaStreamSynchronize(h.stream));
+  // one host sync for the statistics, the error words and the metrics above
+  std::vector<RefineLevelStats> rs = level_stats(h, rc, nl);
   GKW_REQUIRE(hm[1] == 0, GKW_E_INTERNAL, "partition produced a part id out of range");
   if (cut_out) *cut_out = hm[0];
   if (stats) {
