@@ -135,6 +135,7 @@ _SIGS = [
     ("gkw_init_partition", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.c_double,
                                           ctypes.c_uint64, ctypes.c_int32, _VP]),
     ("gkw_cut", ctypes.c_int, [_VP, ctypes.POINTER(Csr), _VP, ctypes.c_int32, _i64p, _i64p]),
+    ("gkw_cut_noalloc", ctypes.c_int, [ctypes.POINTER(Csr), _VP, ctypes.c_int32, _VP, _i64p, _i64p]),
     ("gkw_read_metis", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _i32p, _i64p, ctypes.POINTER(_i32p),
                                       ctypes.POINTER(_i32p), ctypes.POINTER(_i32p), ctypes.POINTER(_i32p)]),
     ("gkw_write_partition", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _i32p]),
@@ -410,6 +411,18 @@ def _make_init_cb(init):
         except Exception:
             return -1
     return INIT_FN(cb)
+
+
+def cut_noalloc(g, part, k: int, stream: int = 0):
+    """gkw_cut_noalloc over torch CUDA tensors: (cut, part weights).  Allocates
+    no device memory and needs no handle; runs on `stream` (a cudaStream_t as
+    an int, 0 = the default stream) of the current device."""
+    c = _csr_dev(*g)
+    cut = ctypes.c_int64()
+    pw = np.zeros(k, np.int64)
+    check(lib().gkw_cut_noalloc(ctypes.byref(c), part.data_ptr() if part.numel() else None, int(k),
+                                ctypes.c_void_p(stream), ctypes.byref(cut), pw.ctypes.data_as(_i64p)))
+    return int(cut.value), pw
 
 
 def exported_symbols() -> list[str]:

@@ -235,6 +235,9 @@ float balance_cap(i64 total_vwgt, i32 k, double eps);
 // d_cut needs 2 slots ([0] cut, [1] nonzero if a part id was out of range);
 // d_pw needs k.
 void compute_cut_pw(Handle& h, const DevGraph& g, const i32* part, i32 k, i64* d_cut, i64* d_pw);
+// The cut / part-weight kernel alone: d_acc[0] cut, [1] bad-part flag,
+// [2..k+2) part weights; the caller zeroes d_acc first.
+void launch_cut_pw(cudaStream_t stream, i32 sm_count, const DevGraph& g, const i32* part, i32 k, i64* d_acc);
 void check_parts(Handle& h, i32 n, const i32* part, i32 k);
 
 // ---- initial partition (initpart.cu) ----

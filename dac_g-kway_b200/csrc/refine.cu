@@ -1168,15 +1168,19 @@ void check_parts(Handle& h, i32 n, const i32* part, i32 k) {
   GKW_REQUIRE(b == 0, GKW_E_INVALID, "part id out of range [0, k)");
 }
 
-void compute_cut_pw(Handle& h, const DevGraph& g, const i32* part, i32 k, i64* d_cut, i64* d_pw) {
-  GKW_CUDA(cudaMemsetAsync(d_cut, 0, sizeof(i64) * 2, h.stream));   // [0] cut, [1] bad-part flag
-  GKW_CUDA(cudaMemsetAsync(d_pw, 0, sizeof(i64) * k, h.stream));
+void launch_cut_pw(cudaStream_t stream, i32 sm_count, const DevGraph& g, const i32* part, i32 k, i64* d_acc) {
   if (g.n == 0) return;
   const size_t sm = k <= 4096 ? sizeof(unsigned long long) * k : 0;
-  const u32 grid = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)h.sm_count * 8));
-  launch(k_cut_pw, grid, 256, sm, h.stream, g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
-         (unsigned long long*)d_cut, (unsigned long long*)d_pw, (i32*)(d_cut + 1));
+  const u32 grid = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)sm_count * 8));
+  launch(k_cut_pw, grid, 256, sm, stream, g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
+         (unsigned long long*)d_acc, (unsigned long long*)(d_acc + 2), (i32*)(d_acc + 1));
   GKW_CHECK_LAUNCH();
+}
+
+void compute_cut_pw(Handle& h, const DevGraph& g, const i32* part, i32 k, i64* d_cut, i64* d_pw) {
+  GKW_REQUIRE(d_pw == d_cut + 2, GKW_E_INTERNAL, "cut accumulators must be contiguous");
+  GKW_CUDA(cudaMemsetAsync(d_cut, 0, sizeof(i64) * (k + 2), h.stream));   // [0] cut, [1] bad-part flag, pw
+  launch_cut_pw(h.stream, h.sm_count, g, part, k, d_cut);
 }
 
 }  // namespace gkw

@@ -197,6 +197,20 @@ gkw_status gkw_read_metis(const char* path, int32_t reference_quirks, int32_t* n
 gkw_status gkw_write_partition(const char* path, int32_t n, const int32_t* part);
 void gkw_free(void* p);
 
+/* Exact cut and part weights like gkw_cut, but with no device allocation and
+ * no handle.  No counterpart in the reference.  For callers that may not
+ * allocate device memory while they run (a serving loop with a fixed memory
+ * budget, a plugin that only receives pre-allocated buffers): the kernel's
+ * accumulators live in a fixed array inside the library (8192 int64 words,
+ * 64 KB, held on every device that loads the library until exit), so k is
+ * limited to 8190.  Runs on `stream` (a cudaStream_t, NULL = the default
+ * stream) of the current device and returns when that stream is idle; cut_out
+ * and pw_out (k entries, may be NULL) are host memory.  The first call on a
+ * device looks up the array's device address; make it outside stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race. */
+gkw_status gkw_cut_noalloc(const gkw_csr* d_graph, const int32_t* d_part, int32_t k, void* stream,
+                           int64_t* cut_out, int64_t* pw_out);
+
 /* MAX_PARTITION_WGT as the reference computes it (graph_partitioner.hpp:230). */
 float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps);
 
