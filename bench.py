@@ -65,52 +65,98 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons of this GPU, sampled by a
+    background thread every few milliseconds while the timed region runs.
+    NVML (the library nvidia-smi reads) is used directly so that short timed
+    regions still get many samples; nvidia-smi is the fallback."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.rows = []
+    def __init__(self, device_index: int, period_s: float = 0.005):
+        self.dev = device_index
+        self.period = period_s
+        self.rows = []           # (sm_mhz, max_mhz, reason bits)
+        self.stop_evt = threading.Event()
+        self.mode = None
         self.proc = None
+        self.t = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            idx = int(vis.split(",")[self.dev]) if vis and vis.split(",")[self.dev].isdigit() else self.dev
+            return pynvml.nvmlDeviceGetHandleByIndex(idx)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+            import pynvml
+            hnd = self._nvml_handle()
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(hnd, pynvml.NVML_CLOCK_SM)
+
+            def run():
+                while not self.stop_evt.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(hnd, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(hnd)
+                        self.rows.append((float(sm), float(mx), int(rs)))
+                    except Exception:
+                        pass
+                    self.stop_evt.wait(self.period)
+
+            self.mode = "nvml"
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            pass
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+
+            def read():
+                for line in self.proc.stdout:
+                    r = [x.strip() for x in line.split(",")]
+                    if len(r) < 9 or not r[1].replace(".", "").isdigit():
+                        continue
+                    bits = 0
+                    for i, (_, bit) in enumerate(self.REASONS[:4]):
+                        if r[5 + i].lower().startswith("active"):
+                            bits |= bit
+                    self.rows.append((float(r[1]), float(r[2]), bits))
+
+            self.mode = "nvidia-smi"
+            self.t = threading.Thread(target=read, daemon=True)
             self.t.start()
         except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.mode = None
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
+        if self.mode is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
+        self.stop_evt.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
         self.t.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            if len(r) < 9:
-                continue
-            for i, nm in enumerate(names):
-                if r[5 + i].lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        rows = list(self.rows)
+        reasons = sorted({nm for _, _, bits in rows for nm, bit in self.REASONS if bits & bit})
+        return {"sm_mhz": statistics.median(r[0] for r in rows) if rows else None,
+                "sm_max_mhz": max(r[1] for r in rows) if rows else None,
+                "reasons": reasons, "samples": len(rows), "source": self.mode}
 
 
 def metis_cpu_baseline(g, budget_s: float = 12.0) -> dict:
@@ -175,6 +221,7 @@ def bench_ours(args):
     launches = 0
     cut = None
     st = None
+    steps_stats = []
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -184,6 +231,7 @@ def bench_ours(args):
         l0 = pkg.launch_count()
         cut, st = h.partition_device(xadj, adjncy, adjwgt, vwgt, K, part, opts)
         launches += pkg.launch_count() - l0
+        steps_stats.append(st)
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -221,16 +269,14 @@ def bench_ours(args):
     e2e_max = float(e2e_t.item())
     assert int(cut_e) == int(cut), "host and device paths disagree"
 
-    # ---- roofline of the dominant kernel (contraction at level 0) ----
-    roof = None
-    if rank == 0:
-        roof = roofline_contract(pkg, h, g, stream, flush)
+    # ---- roofline of the dominant kernel, from the timed steps ----
+    roof, phase_roof = roofline_report(steps_stats)
 
     if rank == 0:
         part_np = part.cpu().numpy()
         pw = np.bincount(part_np, weights=g.vwgt, minlength=K)
         W = int(g.vwgt.sum())
-        cpu = metis_cpu_baseline(g)
+        cpu = metis_cpu_baseline(g) if world == 1 else None
         line = {
             "metric": METRIC, "value": world * g.n_edges / (ms_max / 1e3), "unit": "edges/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
@@ -244,6 +290,7 @@ def bench_ours(args):
                     "d2h_bytes_per_step": int(4 * g.n)},
             "gpu_launches": int(launches),
             "roofline": roof,
+            "phase_roofline": phase_roof,
             "cpu_baseline": cpu,
             "quality": {"cut": int(cut), "max_part_weight": int(pw.max()),
                         "balance": float(pw.max() * K / W), "maxw": st["maxw"] if st else None,
@@ -259,48 +306,90 @@ def bench_ours(args):
         torch.distributed.destroy_process_group()
 
 
-def roofline_contract(pkg, h, g, stream, flush):
-    """Contraction of level 0 timed alone (per-phase entry point), against the
-    measured HBM copy bandwidth.  Algorithmic bytes per launch:
-    4(n+1) + 8m (level CSR) + 8n (own + gathered cmap) + 4(n_c+1) + 8m_c."""
-    import torch
-    import oracle
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    dev = torch.device("cuda", torch.cuda.current_device())
-    dg = tuple(torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.adjwgt, g.vwgt))
-    cand = h.match(dg)
-    root, dist, _ = h.union_find(cand)
-    cmap, nc = h.group_map(root, dist, 6)
-    times = []
-    mc = 0
-    for i in range(8):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        cx, ca, cw, cv = h.contract(dg, cmap, nc)
-        e1.record(stream)
-        e1.synchronize()
-        if i >= 2:
-            times.append(e0.elapsed_time(e1))
-        mc = int(ca.shape[0])
-    ms = statistics.median(times)
-    alg = 4 * (g.n + 1) + 8 * g.m + 8 * g.n + 4 * (nc + 1) + 8 * mc
-    achieved = alg / (ms / 1e3) / 1e9
-    tr = None
-    tf = os.path.join(ROOT, "profiles", "contract_traffic.json")
-    if os.path.exists(tf):
-        try:
-            tr = json.load(open(tf)).get("bytes_per_launch")
-        except Exception:
-            tr = None
-    return {"kernel": "contraction, level 0 (gkw_contract: accum + scan + hash rows + scan + copy)",
+def load_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    return 6650.0, "fallback 6.65 TB/s (of fallback)"
+
+
+def level_kernel_launches(st):
+    """(algorithmic bytes, device ms) of each level-kernel launch of one
+    partition.  Per level of n vertices and m CSR entries (4-byte words, each
+    compulsory array once): one full gain pass 4(n+1) + 8m + 4n + 8n, the
+    projection from the coarser level 4n + 4n_c, and 8 bytes (adjncy, adjwgt)
+    per adjacency entry the gain updates of the rounds read."""
+    nl, ln, lm = st["n_levels"], st["level_n"], st["level_m"]
+    out = []
+    for i in range(nl):
+        ms = st["ms_level"][i]
+        if ms < 0:
+            continue
+        n, m = ln[i], lm[i]
+        b = 4 * (n + 1) + 8 * m + 4 * n + 8 * n + 8 * st["round_entries"][i]
+        if i + 1 < nl:
+            b += 4 * n + 4 * ln[i + 1]
+        out.append((i, b, ms))
+    return out
+
+
+def coarsen_bytes(st):
+    """Algorithmic bytes of coarsening, summed over the kept levels: match
+    4(n+1) + 8m + 4n, grouping 12n + 4n_c, contraction 4(n+1) + 8m + 8n +
+    4(n_c+1) + 8m_c."""
+    nl, ln, lm = st["n_levels"], st["level_n"], st["level_m"]
+    tot = 0
+    for i in range(nl - 1):
+        n, m, nc, mc = ln[i], lm[i], ln[i + 1], lm[i + 1]
+        tot += 4 * (n + 1) + 8 * m + 4 * n
+        tot += 12 * n + 4 * nc
+        tot += 4 * (n + 1) + 8 * m + 8 * n + 4 * (nc + 1) + 8 * mc
+    return tot
+
+
+def read_traffic(kernel_file):
+    """DRAM bytes per launch from a committed ncu summary (a line
+    'traffic_bytes_per_launch: N'), or None."""
+    path = os.path.join(ROOT, "profiles", kernel_file)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        return None
+    return None
+
+
+def roofline_report(steps_stats):
+    """Roofline of the dominant kernel (the level kernel: projection, balance
+    and refinement rounds, one launch per level), from the CUDA events the
+    library records around each of its launches in the timed steps."""
+    peak, src = load_peak_gbs()
+    launches = [x for st in steps_stats for x in level_kernel_launches(st)]
+    tot_b = sum(b for _, b, _ in launches)
+    tot_ms = sum(ms for _, _, ms in launches)
+    nlaunch = max(len(launches), 1)
+    achieved = tot_b / (tot_ms / 1e3) / 1e9 if tot_ms > 0 else 0.0
+    roof = {"kernel": "k_level (one launch per level: projection, balance rounds, refinement rounds)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": tr, "algorithmic_bytes": int(alg), "ms": ms,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+            "traffic": read_traffic("k_level_delaunay2e20_k64.md"),
+            "algorithmic_bytes_per_launch": tot_b / nlaunch, "ms_per_launch": tot_ms / nlaunch,
+            "launches": len(launches), "peak_source": src,
+            "timing": "CUDA events on the library stream around each launch, every timed step"}
+    # phase fractions (coarsening, refinement) over the timed steps
+    cb = sum(coarsen_bytes(st) for st in steps_stats)
+    cms = sum(st["ms_coarsen"] for st in steps_stats)
+    rb = sum(b for st in steps_stats for i, b, _ in level_kernel_launches(st) if i + 1 < st["n_levels"])
+    rms = sum(st["ms_refine"] for st in steps_stats)
+    phases = {"coarsen": {"bytes_per_step": cb / len(steps_stats), "ms_per_step": cms / len(steps_stats),
+                          "frac": cb / (cms / 1e3) / 1e9 / peak if cms > 0 else None},
+              "uncoarsen": {"bytes_per_step": rb / len(steps_stats), "ms_per_step": rms / len(steps_stats),
+                            "frac": rb / (rms / 1e3) / 1e9 / peak if rms > 0 else None}}
+    return roof, phases
 
 
 # ---------------------------------------------------------------------------
@@ -382,14 +471,190 @@ def bench_reference(args):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# batched and served forms (not the headline line): --workload batched|served
+# ---------------------------------------------------------------------------
+BATCH_KS = (2, 4, 8, 16, 32)
+
+
+def _gen_one(spec):
+    """One seeded graph of a mixed workload: (kind, n, seed) -> CSR arrays."""
+    import __graft_entry__ as ge
+    gen = ge.load_generators()
+    kind, n, seed = spec
+    if kind == 0:
+        g = gen.delaunay(max(n, 4), seed)
+    elif kind == 1:
+        a = max(2, int(round(n ** (1.0 / 3.0))))
+        g = gen.grid27(a, a, max(2, int(round(n / (a * a)))))
+    else:
+        g = gen.circuit(max(n, 64), seed=seed, levels=min(200, max(8, n // 200)), hub_max=max(16, min(10000, n // 10)))
+    return g.xadj, g.adjncy, g.adjwgt, g.vwgt
+
+
+def mixed_graphs(count, n_lo, n_hi, seed, tag):
+    """``count`` seeded graphs, vertex counts log-uniform in [n_lo, n_hi],
+    generator uniform over 2D Delaunay, near-cubic 27-point grid and the
+    scaled circuit-like graph; cached under CACHE_DIR."""
+    import multiprocessing as mp
+    import __graft_entry__ as ge
+    gen = ge.load_generators()
+    path = os.path.join(CACHE_DIR, f"{tag}_{count}_{n_lo}_{n_hi}_s{seed}.npz")
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.integers(0, 3)), int(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))), 1000 + i)
+             for i in range(count)]
+    if os.path.exists(path):
+        with np.load(path) as d:   # each array read once
+            X, A, Wt, V, gp, ep = d["x"], d["a"], d["w"], d["v"], d["gp"], d["ep"]
+        return [gen.Csr(X[gp[i] + i:gp[i + 1] + i + 1], A[ep[i]:ep[i + 1]], Wt[ep[i]:ep[i + 1]],
+                        V[gp[i]:gp[i + 1]]) for i in range(count)], specs
+    with mp.get_context("spawn").Pool(max(1, min(32, os.cpu_count() or 1))) as pool:
+        arrs = pool.map(_gen_one, [(k, n, sd) for k, n, sd in specs], chunksize=4)
+    graphs = [gen.Csr(*a) for a in arrs]
+    os.makedirs(CACHE_DIR, exist_ok=True)
+    gp = np.zeros(count + 1, np.int64)
+    ep = np.zeros(count + 1, np.int64)
+    gp[1:] = np.cumsum([g.n for g in graphs])
+    ep[1:] = np.cumsum([g.m for g in graphs])
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, x=np.concatenate([g.xadj for g in graphs]), a=np.concatenate([g.adjncy for g in graphs]),
+             w=np.concatenate([g.adjwgt for g in graphs]), v=np.concatenate([g.vwgt for g in graphs]), gp=gp, ep=ep)
+    os.replace(tmp, path)
+    return graphs, specs
+
+
+def bench_batched(args):
+    """Config: many independent small graphs in one call (gkw_partition_batch)
+    against the plain path partitioning them one after another on the same
+    GPU.  Both sides go host arrays -> host parts; wall-clock time."""
+    import torch
+    import __graft_entry__ as ge
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    count = args.graphs
+    graphs, specs = mixed_graphs(count, 1000, 64000, 7, "batch")
+    rng = np.random.default_rng(11)
+    ks = [int(rng.choice(BATCH_KS)) for _ in graphs]
+    x, a, w, vw, gp = pkg.concat_graphs(graphs)
+    edges = int(sum(g.n_edges for g in graphs))
+    # plain path: one handle, one graph after another
+    h = pkg.Handle(0)
+    for g, k in list(zip(graphs, ks))[:8]:
+        h.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = [h.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k) for g, k in zip(graphs, ks)]
+    t_plain = time.perf_counter() - t0
+    h.close()
+    srv = pkg.Server(0, slots=args.slots)
+    srv.partition_batch(x[: gp[8] + 1], a[: x[gp[8]]], w[: x[gp[8]]], vw[: gp[8]], gp[:9], ks[:8])   # warm
+    times = []
+    part = cuts = None
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        part, cuts, sts = srv.partition_batch(x, a, w, vw, gp, ks)
+        times.append(time.perf_counter() - t0)
+    srv.close()
+    same = all(np.array_equal(part[gp[i]:gp[i + 1]], plain[i][0]) and int(cuts[i]) == plain[i][1]
+               for i in range(count))
+    t_b = statistics.median(times)
+    print(json.dumps({
+        "workload": "batched", "metric": "graphs/s partitioned (batched form)", "value": count / t_b,
+        "unit": "graphs/s", "edges_per_s": edges / t_b, "plain_graphs_per_s": count / t_plain,
+        "plain_edges_per_s": edges / t_plain, "speedup_vs_plain": t_plain / t_b, "identical_to_plain": bool(same),
+        "slots": args.slots, "steps": len(times), "timing": "wall clock, host arrays in, host parts out",
+        "config": {"graphs": count, "n": "log-uniform 1k-64k", "generators": "Delaunay / 27-point grid / circuit",
+                   "k": list(BATCH_KS), "eps": EPS, "vertices": int(gp[-1]), "edges": edges}}))
+
+
+def bench_served(args):
+    """Config: open-loop Poisson requests of mixed sizes at a sweep of offered
+    loads, through the server (continuous batching) and through the plain
+    path (one handle serving requests first come, first served)."""
+    import threading
+    import torch
+    import __graft_entry__ as ge
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    pool, _ = mixed_graphs(args.pool, 1000, args.max_n, 5, "served")
+    rng = np.random.default_rng(3)
+    ks_all = [2 ** int(rng.integers(1, 9)) for _ in range(4096)]
+    out = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        nreq = int(max(20, min(args.requests, rate * args.duration)))
+        arr = np.cumsum(rng.exponential(1.0 / rate, nreq))
+        which = rng.integers(0, len(pool), nreq)
+        ks = [ks_all[i % len(ks_all)] for i in range(nreq)]
+        res = {"offered_per_s": rate, "requests": nreq}
+        for mode in ("served", "plain"):
+            lat = [0.0] * nreq
+            done_t = [0.0] * nreq
+            if mode == "served":
+                srv = pkg.Server(0, slots=args.slots)
+                tickets = [None] * nreq
+                t0 = time.perf_counter()
+
+                def submit():
+                    for i in range(nreq):
+                        d = t0 + arr[i] - time.perf_counter()
+                        if d > 0:
+                            time.sleep(d)
+                        g = pool[which[i]]
+                        tickets[i] = srv.submit(g.xadj, g.adjncy, g.adjwgt, g.vwgt, ks[i])
+
+                th = threading.Thread(target=submit)
+                th.start()
+                for i in range(nreq):
+                    while tickets[i] is None:
+                        time.sleep(0.0002)
+                    r = srv.poll(tickets[i], pool[which[i]].n, wait_ms=-1)
+                    lat[i] = r[2]["latency_ms"]
+                    done_t[i] = time.perf_counter()
+                th.join()
+                srv.close()
+            else:
+                h = pkg.Handle(0)
+                t0 = time.perf_counter()
+                for i in range(nreq):
+                    d = t0 + arr[i] - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    g = pool[which[i]]
+                    h.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, ks[i])
+                    done_t[i] = time.perf_counter()
+                    lat[i] = (done_t[i] - (t0 + arr[i])) * 1e3
+                h.close()
+            span = max(done_t) - t0
+            res[mode] = {"graphs_per_s": nreq / span, "p50_ms": float(np.percentile(lat, 50)),
+                         "p99_ms": float(np.percentile(lat, 99))}
+        out.append(res)
+    print(json.dumps({"workload": "served", "metric": "served graphs/s and p50/p99 latency vs plain",
+                      "unit": "graphs/s", "slots": args.slots, "loads": out,
+                      "config": {"pool_graphs": len(pool), "n": f"log-uniform 1k-{args.max_n}",
+                                 "k": "2..256 powers of two", "eps": EPS,
+                                 "timing": "wall clock, submit to result on the host"}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--graphs", type=int, default=4096, help="batched: number of graphs")
+    ap.add_argument("--slots", type=int, default=8, help="batched/served: concurrent partitions")
+    ap.add_argument("--pool", type=int, default=48, help="served: distinct graphs requests draw from")
+    ap.add_argument("--max-n", type=int, default=2000000, help="served: largest graph")
+    ap.add_argument("--rates", default="10,50,200,500,1000,2000", help="served: offered loads (requests/s)")
+    ap.add_argument("--requests", type=int, default=400, help="served: most requests per load")
+    ap.add_argument("--duration", type=float, default=4.0, help="served: seconds of arrivals per load")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "batched":
+        bench_batched(args)
+    elif args.workload == "served":
+        bench_served(args)
+    elif args.impl == "reference":
         bench_reference(args)
     else:
         bench_ours(args)

@@ -30,6 +30,7 @@ GKW_E_NOMEM = 3
 GKW_E_UNSUPPORTED = 4
 GKW_E_INIT = 5
 GKW_E_INTERNAL = 6
+GKW_E_PENDING = 7
 INIT_DEVICE = 0
 INIT_CALLBACK = 1
 
@@ -91,6 +92,8 @@ class Stats(ctypes.Structure):
         ("ms_init", ctypes.c_double),
         ("ms_refine", ctypes.c_double),
         ("ms_total", ctypes.c_double),
+        ("ms_level", ctypes.c_double * MAX_LEVELS),
+        ("round_entries", ctypes.c_int64 * MAX_LEVELS),
     ]
 
     def as_dict(self) -> dict:
@@ -107,7 +110,59 @@ class Stats(ctypes.Structure):
             init_cut=int(self.init_cut), cut=int(self.cut), max_part_weight=int(self.max_part_weight),
             maxw=float(self.maxw), ms_coarsen=self.ms_coarsen, ms_init=self.ms_init,
             ms_refine=self.ms_refine, ms_total=self.ms_total,
+            ms_level=list(self.ms_level[:nl]), round_entries=list(self.round_entries[:nl]),
         )
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("slots", ctypes.c_int32),
+        ("narrow_max_n", ctypes.c_int32),
+        ("pool_bytes", ctypes.c_int64),
+        ("slot_keep_bytes", ctypes.c_int64),
+        ("max_bypass", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("queue_ms", ctypes.c_double),
+        ("run_ms", ctypes.c_double),
+        ("latency_ms", ctypes.c_double),
+        ("predicted_bytes", ctypes.c_int64),
+        ("slot", ctypes.c_int32),
+        ("n_levels", ctypes.c_int32),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64),
+        ("completed", ctypes.c_int64),
+        ("failed", ctypes.c_int64),
+        ("p50_ms", ctypes.c_double),
+        ("p99_ms", ctypes.c_double),
+        ("max_ms", ctypes.c_double),
+        ("mean_queue_ms", ctypes.c_double),
+        ("graphs_per_s", ctypes.c_double),
+        ("peak_reserved_bytes", ctypes.c_int64),
+        ("peak_running", ctypes.c_int32),
+        ("slots", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class CsrBatch(ctypes.Structure):
+    _fields_ = [
+        ("graph", Csr),
+        ("n_graphs", ctypes.c_int32),
+        ("graph_ptr", ctypes.c_void_p),
+        ("k", ctypes.c_void_p),
+        ("eps", ctypes.c_void_p),
+    ]
 
 
 # (name, restype, argtypes) of every C-ABI entry point
@@ -144,6 +199,17 @@ _SIGS = [
     ("gkw_balance_cap", ctypes.c_float, [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]),
     ("gkw_balance", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.c_float, ctypes.c_int32, _VP,
                                    _VP, _VP, _VP, _VP, _i32p, _i64p]),
+    ("gkw_server_default_config", None, [ctypes.POINTER(ServerConfig)]),
+    ("gkw_server_create", ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(ServerConfig)]),
+    ("gkw_server_destroy", ctypes.c_int, [_VP]),
+    ("gkw_predict_footprint", ctypes.c_int64, [ctypes.c_int32, ctypes.c_int64, ctypes.c_int32]),
+    ("gkw_server_submit", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.POINTER(Options),
+                                         _i64p]),
+    ("gkw_server_poll", ctypes.c_int, [_VP, ctypes.c_int64, ctypes.c_int32, _VP, _i64p,
+                                       ctypes.POINTER(RequestInfo)]),
+    ("gkw_server_stats_get", ctypes.c_int, [_VP, ctypes.POINTER(ServerStats), ctypes.c_int32]),
+    ("gkw_partition_batch", ctypes.c_int, [_VP, ctypes.POINTER(CsrBatch), ctypes.POINTER(Options), _VP, _i64p,
+                                           _i32p]),
 ]
 
 _lib = None
@@ -390,6 +456,114 @@ class Handle:
         check(lib().gkw_cut(self._h, ctypes.byref(c), part.data_ptr(), int(k), ctypes.byref(cut),
                             pw.ctypes.data_as(_i64p)))
         return int(cut.value), pw
+
+
+def predict_footprint(n: int, nnz: int, k: int) -> int:
+    """Predicted device bytes of one partition (the server's admission measure)."""
+    return int(lib().gkw_predict_footprint(int(n), int(nnz), int(k)))
+
+
+def server_config(**kw) -> ServerConfig:
+    c = ServerConfig()
+    lib().gkw_server_default_config(ctypes.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def concat_graphs(graphs):
+    """Disjoint union of CSR graphs (objects with xadj/adjncy/adjwgt/vwgt) ->
+    (xadj, adjncy, adjwgt, vwgt, graph_ptr) with global 0-based ids."""
+    ns = [int(g.xadj.shape[0]) - 1 for g in graphs]
+    ms = [int(g.adjncy.shape[0]) for g in graphs]
+    vptr = np.zeros(len(graphs) + 1, np.int64)
+    eptr = np.zeros(len(graphs) + 1, np.int64)
+    vptr[1:] = np.cumsum(ns)
+    eptr[1:] = np.cumsum(ms)
+    if vptr[-1] >= 2 ** 31 or eptr[-1] >= 2 ** 31:
+        raise GkwError(GKW_E_UNSUPPORTED, "batch too large for int32 offsets")
+    xadj = np.zeros(int(vptr[-1]) + 1, np.int32)
+    adjncy = np.empty(int(eptr[-1]), np.int32)
+    adjwgt = np.empty(int(eptr[-1]), np.int32)
+    vwgt = np.empty(int(vptr[-1]), np.int32)
+    for i, g in enumerate(graphs):
+        v0, v1, e0, e1 = int(vptr[i]), int(vptr[i + 1]), int(eptr[i]), int(eptr[i + 1])
+        xadj[v0 + 1:v1 + 1] = g.xadj[1:].astype(np.int64) + e0
+        adjncy[e0:e1] = g.adjncy.astype(np.int64) + v0
+        adjwgt[e0:e1] = g.adjwgt
+        vwgt[v0:v1] = g.vwgt
+    return xadj, adjncy, adjwgt, vwgt, vptr.astype(np.int32)
+
+
+class Server:
+    """Batched and served partitioning on one device: ``slots`` concurrent
+    partitions fed from one queue, admitted by predicted device footprint."""
+
+    def __init__(self, device: int = 0, **cfg):
+        self._s = ctypes.c_void_p()
+        c = server_config(**cfg)
+        check(lib().gkw_server_create(ctypes.byref(self._s), int(device), ctypes.byref(c)))
+
+    def close(self):
+        if self._s:
+            lib().gkw_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, xadj, adjncy, adjwgt, vwgt, k: int, opts: Options | None = None) -> int:
+        c, keep = _csr_host(xadj, adjncy, adjwgt, vwgt)
+        o = opts if opts is not None else default_options()
+        t = ctypes.c_int64()
+        rc = lib().gkw_server_submit(self._s, ctypes.byref(c), int(k), ctypes.byref(o), ctypes.byref(t))
+        del keep
+        check(rc)
+        return int(t.value)
+
+    def poll(self, ticket: int, n: int, wait_ms: int = -1):
+        """(part, cut, info) when the request is done, None while it is pending."""
+        part = np.empty(max(n, 1), np.int32)
+        cut = ctypes.c_int64()
+        info = RequestInfo()
+        rc = lib().gkw_server_poll(self._s, int(ticket), int(wait_ms), part.ctypes.data, ctypes.byref(cut),
+                                   ctypes.byref(info))
+        if rc == GKW_E_PENDING:
+            return None
+        check(rc)
+        return part[:n], int(cut.value), {name: getattr(info, name) for name, _ in info._fields_}
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        check(lib().gkw_server_stats_get(self._s, ctypes.byref(st), int(reset)))
+        return st.as_dict()
+
+    def partition_batch(self, xadj, adjncy, adjwgt, vwgt, graph_ptr, ks, eps=None, opts: Options | None = None,
+                        raise_on_error: bool = True):
+        """Concatenated CSR (global ids) + graph_ptr -> (part with per-graph ids, cuts, statuses)."""
+        c, keep = _csr_host(xadj, adjncy, adjwgt, vwgt)
+        gp = _i32(graph_ptr)
+        kk = _i32(ks)
+        ee = None if eps is None else np.ascontiguousarray(eps, dtype=np.float64)
+        b = CsrBatch()
+        b.graph = c
+        b.n_graphs = int(kk.shape[0])
+        b.graph_ptr = gp.ctypes.data
+        b.k = kk.ctypes.data if kk.shape[0] else None
+        b.eps = None if ee is None else ee.ctypes.data
+        o = opts if opts is not None else default_options()
+        part = np.empty(max(c.n, 1), np.int32)
+        cuts = np.zeros(max(b.n_graphs, 1), np.int64)
+        sts = np.zeros(max(b.n_graphs, 1), np.int32)
+        rc = lib().gkw_partition_batch(self._s, ctypes.byref(b), ctypes.byref(o), part.ctypes.data,
+                                       cuts.ctypes.data_as(_i64p), sts.ctypes.data_as(_i32p))
+        del keep
+        if raise_on_error:
+            check(rc)
+        return part[:c.n], cuts[:b.n_graphs], sts[:b.n_graphs]
 
 
 def _make_init_cb(init):

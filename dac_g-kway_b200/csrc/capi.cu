@@ -14,6 +14,10 @@ struct gkw_handle {
 
 using namespace gkw;
 
+namespace gkw {
+Handle& handle_of(gkw_handle* h) { return h->h; }
+}  // namespace gkw
+
 namespace {
 
 template <class F>
@@ -58,11 +62,6 @@ DevGraph dev_view(const gkw_csr* g) {
 void need_weights(const DevGraph& d) {
   GKW_REQUIRE(d.m == 0 || d.adjwgt != nullptr, GKW_E_INVALID, "adjwgt is NULL");
   GKW_REQUIRE(d.n == 0 || d.vwgt != nullptr, GKW_E_INVALID, "vwgt is NULL");
-}
-
-__global__ void k_fill(i32* p, i64 n, i32 v) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
 }
 
 __global__ void k_unpack_keys(i32 n, const u64* __restrict__ keys, i32* __restrict__ root,
@@ -136,6 +135,9 @@ gkw_status gkw_create(gkw_handle** out, int32_t device) {
     int sms = 0;
     GKW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     h->h.sm_count = sms;
+    int optin = 0;
+    GKW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    h->h.smem_optin = optin;
     e = cudaMalloc(&h->h.coop, sizeof(CoopState));
     if (e == cudaSuccess) e = cudaMemset(h->h.coop, 0, sizeof(CoopState));
     if (e != cudaSuccess) {
@@ -158,6 +160,9 @@ gkw_status gkw_destroy(gkw_handle* h) {
     if (h->h.scan) cudaFree(h->h.scan);
     if (h->h.coop) cudaFree(h->h.coop);
     if (h->h.arena) cudaFree(h->h.arena);
+    if (h->h.tev_ready)
+      for (cudaEvent_t e : h->h.tev) cudaEventDestroy(e);
+    forget_coop_event(h->h);
     delete h;
   });
 }
@@ -194,38 +199,9 @@ gkw_status gkw_partition(gkw_handle* h, const gkw_csr* graph, int32_t k, const g
   return guard([&] {
     Handle& hh = H(h);
     DevGraph hg = dev_view(graph);
-    GKW_REQUIRE(hg.n == 0 || part_out != nullptr, GKW_E_INVALID, "part_out is NULL");
     gkw_options o;
     if (opt) o = *opt; else gkw_default_options(&o);
-    hh.hier.reset();
-    hh.scratch.reset();
-    const i64 n = hg.n, m = hg.m;
-    i32* x = hh.hier.alloc_n<i32>(n + 1);
-    i32* a = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
-    i32* w = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
-    i32* vw = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
-    i32* part = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
-    GKW_CUDA(cudaMemcpyAsync(x, hg.xadj, sizeof(i32) * (n + 1), cudaMemcpyHostToDevice, hh.stream));
-    if (m) GKW_CUDA(cudaMemcpyAsync(a, hg.adjncy, sizeof(i32) * m, cudaMemcpyHostToDevice, hh.stream));
-    if (m) {
-      if (hg.adjwgt) GKW_CUDA(cudaMemcpyAsync(w, hg.adjwgt, sizeof(i32) * m, cudaMemcpyHostToDevice, hh.stream));
-      else launch(k_fill, ceil_div(m, 256), 256, 0, hh.stream, w, m, 1);
-    }
-    if (n) {
-      if (hg.vwgt) GKW_CUDA(cudaMemcpyAsync(vw, hg.vwgt, sizeof(i32) * n, cudaMemcpyHostToDevice, hh.stream));
-      else launch(k_fill, ceil_div(n, 256), 256, 0, hh.stream, vw, n, 1);
-    }
-    GKW_CHECK_LAUNCH();
-    DevGraph g;
-    g.n = hg.n;
-    g.m = m;
-    g.xadj = x;
-    g.adjncy = a;
-    g.adjwgt = w;
-    g.vwgt = vw;
-    partition_impl(hh, g, k, o, part, cut_out, stats);
-    if (n) GKW_CUDA(cudaMemcpyAsync(part_out, part, sizeof(i32) * n, cudaMemcpyDeviceToHost, hh.stream));
-    sync(hh);
+    partition_host(hh, hg, 0, k, o, part_out, cut_out, stats);
   });
 }
 

@@ -150,13 +150,12 @@ void run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out, i32* d_rou
   GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_uf_persist, kUfThreads, 0));
   GKW_REQUIRE(bps >= 1, GKW_E_INTERNAL, "union-find kernel does not fit on an SM");
   i32 grid = std::min<i32>(h.sm_count * std::min(bps, 2), (i32)ceil_div(n, kUfThreads));
-  grid = std::max(grid, 1);
+  grid = coop_grid(h, (const void*)k_uf_persist, grid, kUfThreads, 0);
   i32 max_rounds = n + 2;
   GridBarrier* barp = &h.coop->bar;
   i32* errp = &h.coop->err;
   void* args[] = {&n, &cand, &keys_out, &kb, &chg, &barp, &errp, &d_rounds, &max_rounds};
-  GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_uf_persist, dim3(grid), dim3(kUfThreads), args, 0, h.stream));
-  count_launch();
+  launch_coop(h, (const void*)k_uf_persist, grid, kUfThreads, 0, args);
   h.scratch.release(mk);
 }
 
@@ -383,8 +382,8 @@ void run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap, i32* d
     GridBarrier* barp = &h.coop->bar;
     i32* errp = &h.coop->err;
     void* args[] = {&gl, &cn, (void*)&keys, &gs, &go, &cb, &mb, &capv, &cmap, &gscratch, &barp, &errp};
-    GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_giant_sort, dim3(h.sm_count), dim3(512), args, 0, h.stream));
-    count_launch();
+    const i32 grid = coop_grid(h, (const void*)k_giant_sort, h.sm_count, 512, 0);
+    launch_coop(h, (const void*)k_giant_sort, grid, 512, 0, args);
   }
   h.scratch.release(mk);
 }

@@ -1,7 +1,8 @@
 // Errors, the device pool, handles and the device-wide exclusive scan.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
-#include <atomic>
+#include <map>
 #include <mutex>
 
 #include "gkw_internal.cuh"
@@ -40,6 +41,7 @@ void* Pool::alloc(size_t bytes) {
     if (c.top + bytes <= c.cap) {
       void* p = c.base + c.top;
       c.top += bytes;
+      note_use();
       return p;
     }
     if (cur_ + 1 < chunks_.size()) {
@@ -61,7 +63,21 @@ void* Pool::alloc(size_t bytes) {
   }
   chunks_.push_back({base, cap, bytes});
   cur_ = chunks_.size() - 1;
+  note_use();
   return base;
+}
+
+void Pool::note_use() {
+  size_t used = chunks_[cur_].top;
+  for (size_t i = 0; i < cur_; ++i) used += chunks_[i].cap;
+  peak_ = std::max(peak_, used);
+}
+
+void Pool::trim() {
+  for (auto& c : chunks_) GKW_REQUIRE(c.top == 0, GKW_E_INTERNAL, "trim of a pool in use");
+  for (auto& c : chunks_) cudaFree(c.base);
+  chunks_.clear();
+  cur_ = 0;
 }
 
 void Pool::release(Mark m) {
@@ -142,6 +158,12 @@ __device__ __forceinline__ i32 block_exclusive_scan(i32 x, i32* s_warp, i32& tot
 // (the result is then reported as an error, never a hang).
 constexpr long long kScanSpinCycles = 2000000000ll;
 
+__device__ __forceinline__ u64 ld_relaxed_gpu_u64(const unsigned long long* p) {
+  u64 v;
+  asm volatile("ld.relaxed.gpu.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const i32* in, i32* out, i64 n, i32* total,
                                                              ScanState* ss, u64 base, u64 epoch, i32 ntiles) {
   __shared__ i32 s_warp[33];
@@ -160,34 +182,51 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const i32* in, i32*
   }
   i32 agg;
   const i32 off = block_exclusive_scan(sum, s_warp, agg);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    // warp 0 looks back 32 predecessors per step: every lane waits for its
+    // predecessor's word, the nearest inclusive prefix ends the walk
+    const int lane = threadIdx.x;
     unsigned long long* st = (unsigned long long*)ss->tiles;
     const u64 tag = epoch << 34;
     i32 excl = 0;
     if (tile == 0) {
-      atomicExch(&st[0], (unsigned long long)(tag | (2ull << 32) | (u32)agg));
+      if (lane == 0) atomicExch(&st[0], (unsigned long long)(tag | (2ull << 32) | (u32)agg));
     } else {
-      atomicExch(&st[tile], (unsigned long long)(tag | (1ull << 32) | (u32)agg));
-      i32 j = tile - 1;
+      if (lane == 0) atomicExch(&st[tile], (unsigned long long)(tag | (1ull << 32) | (u32)agg));
+      i64 hi = (i64)tile - 1;
       const long long t0 = clock64();
-      while (j >= 0) {
-        const u64 w = (u64)atomicAdd(&st[j], 0ull);
-        const u32 status = (w >> 34) == epoch ? (u32)((w >> 32) & 3u) : 0u;
-        if (status == 0) {
-          if (clock64() - t0 > kScanSpinCycles) {
-            atomicExch(&ss->err, 1);
-            break;
+      for (;;) {
+        const i64 j = hi - lane;
+        u32 status = 2, val = 0;   // before tile 0: an empty prefix
+        if (j >= 0) {
+          for (;;) {
+            const u64 w = ld_relaxed_gpu_u64(&st[j]);
+            status = (w >> 34) == epoch ? (u32)((w >> 32) & 3u) : 0u;
+            val = (u32)w;
+            if (status != 0) break;
+            if (clock64() - t0 > kScanSpinCycles) {
+              atomicExch(&ss->err, 1);
+              status = 2;
+              val = 0;
+              break;
+            }
           }
-          continue;
         }
-        excl += (i32)(u32)w;
-        if (status == 2) break;
-        --j;
+        const u32 m2 = __ballot_sync(0xffffffffu, status == 2);
+        const int first2 = m2 ? __ffs(m2) - 1 : 32;   // nearest published prefix
+        i32 add = lane <= first2 ? (i32)val : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) add += __shfl_xor_sync(0xffffffffu, add, o);
+        excl += add;
+        if (m2) break;
+        hi -= 32;
       }
-      atomicExch(&st[tile], (unsigned long long)(tag | (2ull << 32) | (u32)(excl + agg)));
+      if (lane == 0) atomicExch(&st[tile], (unsigned long long)(tag | (2ull << 32) | (u32)(excl + agg)));
     }
-    s_excl = excl;
-    if (tile == ntiles - 1 && total) *total = excl + agg;
+    if (lane == 0) {
+      s_excl = excl;
+      if (tile == ntiles - 1 && total) *total = excl + agg;
+    }
   }
   __syncthreads();
   i32 run = off + s_excl;
@@ -225,6 +264,112 @@ void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total) {
          nt);
   GKW_CHECK_LAUNCH();
   h.scan_tickets += (u64)nt;
+}
+
+namespace {
+struct ClusterKey {
+  const void* kern;
+  i32 block;
+  size_t smem;
+  int device;
+  bool operator<(const ClusterKey& o) const {
+    if (kern != o.kern) return kern < o.kern;
+    if (block != o.block) return block < o.block;
+    if (smem != o.smem) return smem < o.smem;
+    return device < o.device;
+  }
+};
+std::mutex g_cluster_mu;
+std::map<ClusterKey, i32> g_cluster_limit;
+constexpr int kMaxDevices = 64;
+std::mutex g_chain_mu[kMaxDevices];
+cudaEvent_t g_chain_last[kMaxDevices] = {};
+}  // namespace
+
+i32 coop_cluster_limit(Handle& h, const void* kern, i32 block, size_t smem) {
+  const ClusterKey key{kern, block, smem, h.device};
+  {
+    std::lock_guard<std::mutex> lk(g_cluster_mu);
+    auto it = g_cluster_limit.find(key);
+    if (it != g_cluster_limit.end()) return it->second;
+  }
+  i32 best = 1;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    cudaGetLastError();
+  for (i32 c = 16; c >= 2; c >>= 1) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = c;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) == cudaSuccess && nclusters >= 1) {
+      best = c;
+      break;
+    }
+    cudaGetLastError();
+  }
+  std::lock_guard<std::mutex> lk(g_cluster_mu);
+  g_cluster_limit[key] = best;
+  return best;
+}
+
+i32 coop_grid(Handle& h, const void* kern, i32 want, i32 block, size_t smem) {
+  want = std::max(want, 1);
+  if (!h.narrow) return want;
+  return std::min(want, coop_cluster_limit(h, kern, block, smem));
+}
+
+void launch_coop(Handle& h, const void* kern, i32 grid, i32 block, size_t smem, void** args) {
+  GKW_REQUIRE(grid >= 1, GKW_E_INTERNAL, "empty grid");
+  if (grid > 1 && grid <= coop_cluster_limit(h, kern, block, smem)) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = grid;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    GKW_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
+    count_launch();
+    return;
+  }
+  if (grid == 1) {   // one CTA waits on no other
+    GKW_CUDA(cudaLaunchKernel(kern, dim3(1), dim3(block), args, smem, h.stream));
+    count_launch();
+    return;
+  }
+  GKW_REQUIRE(h.device >= 0 && h.device < kMaxDevices, GKW_E_UNSUPPORTED, "device index too large");
+  if (!h.coop_ev) GKW_CUDA(cudaEventCreateWithFlags(&h.coop_ev, cudaEventDisableTiming));
+  std::lock_guard<std::mutex> lk(g_chain_mu[h.device]);
+  if (g_chain_last[h.device] && g_chain_last[h.device] != h.coop_ev)
+    GKW_CUDA(cudaStreamWaitEvent(h.stream, g_chain_last[h.device], 0));
+  GKW_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(block), args, smem, h.stream));
+  count_launch();
+  GKW_CUDA(cudaEventRecord(h.coop_ev, h.stream));
+  g_chain_last[h.device] = h.coop_ev;
+}
+
+// Drop a handle's chain event (the handle is going away).
+void forget_coop_event(Handle& h) {
+  if (!h.coop_ev) return;
+  if (h.device >= 0 && h.device < kMaxDevices) {
+    std::lock_guard<std::mutex> lk(g_chain_mu[h.device]);
+    if (g_chain_last[h.device] == h.coop_ev) g_chain_last[h.device] = nullptr;
+  }
+  cudaEventDestroy(h.coop_ev);
+  h.coop_ev = nullptr;
 }
 
 float balance_cap(i64 total_vwgt, i32 k, double eps) {

@@ -5,39 +5,60 @@
 
 namespace gkw {
 
-// Grid barrier for a cooperative launch: a counter and a generation word.  A
-// CTA that waits longer than kGridBarrierCycles sets *err and leaves; every
-// later barrier then reports failure, so the kernel ends with an error status
-// instead of a hang.
+// Grid barrier for a cooperative launch, on one 32-bit word.  Each CTA adds
+// to the word with release semantics: CTA 0 adds 2^31 - (gridDim - 1), the
+// others add 1, so the top bit flips exactly when the last CTA arrives and
+// the low 31 bits are back at zero for the next barrier.  Waiters spin on an
+// acquire load until the top bit differs from what their own add returned.
+// A CTA that waits longer than kGridBarrierCycles sets *err and returns false
+// (the kernel then leaves; the host zeroes the word before the next launch).
 constexpr long long kGridBarrierCycles = 4000000000ll;   // ~2 s at 2 GHz
+
+__device__ __forceinline__ u32 atom_add_release_gpu(u32* p, u32 v) {
+  u32 old;
+  asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ u32 ld_acquire_gpu(const u32* p) {
+  u32 v;
+  asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ u32 cluster_ncta() {
+  u32 r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* b, i32* err, i32* s_flag) {
   if (gridDim.x == 1) {   // a one-CTA launch: the block barrier is the grid barrier
     __syncthreads();
     return true;
   }
+  if (cluster_ncta() == gridDim.x) {
+    // the grid is one thread-block cluster (launch_coop): the hardware
+    // cluster barrier, release/acquire at cluster scope
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    return true;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile u32* vgen = &b->gen;
-    const u32 g = *vgen;
-    __threadfence();
-    const u32 arrived = atomicAdd(&b->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      b->count = 0;
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    } else {
+    const u32 add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+    const u32 old = atom_add_release_gpu(&b->count, add);
+    i32 bad = 0;
+    if (((old ^ ld_acquire_gpu(&b->count)) & 0x80000000u) == 0) {
       const long long t0 = clock64();
-      while (*vgen == g) {
+      while (((old ^ ld_acquire_gpu(&b->count)) & 0x80000000u) == 0) {
         if (clock64() - t0 > kGridBarrierCycles) {
           atomicExch(err, 1);
+          bad = 1;
           break;
         }
-        __nanosleep(20);
       }
     }
-    __threadfence();
-    *s_flag = *(volatile i32*)err;
+    *s_flag = bad;
   }
   __syncthreads();
   return *s_flag == 0;

@@ -60,12 +60,22 @@ class Pool {
   void reset() { release({0, 0}); }
   size_t capacity() const;
   void reserve(size_t bytes);   // make sure one chunk of at least `bytes` exists at the front
+  // Free every chunk.  Only when nothing is allocated (after reset()) and no
+  // queued work uses the memory; cudaFree waits for the whole device.
+  void trim();
+  void set_min_chunk(size_t bytes) { min_chunk_ = bytes; }
+  // Largest amount handed out since the last reset_peak() (chunk tails that
+  // could not be used count as handed out).
+  size_t peak() const { return peak_; }
+  void reset_peak() { peak_ = 0; }
 
  private:
   struct Chunk { char* base; size_t cap; size_t top; };
+  void note_use();
   std::vector<Chunk> chunks_;
   size_t cur_ = 0;
   size_t min_chunk_;
+  size_t peak_ = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -97,10 +107,11 @@ struct CoarsenOut {
   i32 uf_rounds = 0;
 };
 
-// Grid barrier words of a cooperative launch (see device_util.cuh).
+// Grid barrier word of a cooperative launch (see device_util.cuh); zero
+// before the launch.
 struct GridBarrier {
   u32 count;
-  u32 gen;
+  u32 pad;
 };
 
 // Device-side state of one handle shared by the cooperative kernels and the
@@ -144,6 +155,7 @@ struct Handle {
   Pool scratch;
   i64* h_pinned = nullptr;      // 64 pinned i64 slots for scalar readbacks
   i32 sm_count = 148;
+  i32 smem_optin = 232448;      // opt-in shared memory per block of the device
   ScanState* scan = nullptr;    // single-pass scan state
   CoopState* coop = nullptr;    // cooperative-kernel state and per-level scalars
   ArenaHdr* arena = nullptr;    // long-row hash tables: header + words
@@ -151,8 +163,35 @@ struct Handle {
   i32 scan_tiles_cap = 0;
   u64 scan_tickets = 0;         // tickets handed out so far
   u64 scan_epoch = 0;
+  // timing events of the partition driver: 5 phase marks, then a start/end
+  // pair per level-kernel launch; created on first use, destroyed with the handle
+  static constexpr int kTimerEvents = 5 + 2 * kMaxLevels;
+  cudaEvent_t tev[kTimerEvents] = {};
+  bool tev_ready = false;
+  // Grid-barrier kernels: with narrow set, their grids are capped at one
+  // thread-block cluster (a server's small jobs; see launch_coop)
+  bool narrow = false;
+  cudaEvent_t coop_ev = nullptr;   // this handle's last wide cooperative launch
   Handle() : hier(size_t(256) << 20), scratch(size_t(256) << 20) {}
 };
+void ensure_timer_events(Handle& h);
+
+// ---- kernels with grid barriers (common.cu) ----
+// Largest thread-block cluster the kernel can be launched as with this block
+// size and dynamic shared memory (1 if none).
+i32 coop_cluster_limit(Handle& h, const void* kern, i32 block, size_t smem);
+// Grid size for a barrier kernel: `want`, capped at the cluster limit in
+// narrow mode.
+i32 coop_grid(Handle& h, const void* kern, i32 want, i32 block, size_t smem);
+// Launch a kernel whose CTAs wait on one another (grid_barrier).  A grid that
+// fits in one cluster is launched as that cluster: the hardware schedules all
+// of its CTAs together, so it cannot wait on CTAs that never start, whatever
+// else runs.  A wider grid is a cooperative launch, and the wide launches of
+// all handles of the process on one device are chained (each waits for the
+// previous one to finish): two wide grids running at once could each hold
+// part of the SMs and wait for the rest.
+void launch_coop(Handle& h, const void* kern, i32 grid, i32 block, size_t smem, void** args);
+void forget_coop_event(Handle& h);   // before the handle is destroyed
 
 // ---- kernel launches ----
 // Every kernel of the library is launched through launch(), which counts the
@@ -197,6 +236,7 @@ struct RefineLevelStats {
   i64 gain_sum = 0;
   i32 brounds = 0;
   i64 bmoves = 0;
+  i64 rows = 0;   // adjacency entries read by the gain updates of the rounds
 };
 // One persistent launch over one level.  With cmap: project the state held in
 // the context (the coarser level) onto this level and update the gains of its
@@ -212,6 +252,8 @@ struct LevelJob {
   bool refine = false;
   float maxw = 0.f;
   i32 move_cap = 1024;
+  cudaEvent_t ev_start = nullptr;   // optional: recorded right before / after the launch
+  cudaEvent_t ev_end = nullptr;
 };
 RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap);
 RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
@@ -248,6 +290,11 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
 i64 validate(Handle& h, const DevGraph& g);   // total vertex weight; throws on malformed input
 void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
                     i64* cut_out, gkw_stats* stats);
+// The same from host arrays (a slice of a concatenated CSR: xadj values offset
+// by xadj[0], neighbour ids by vbase); part_out is host memory.
+void partition_host(Handle& h, const DevGraph& host_graph, i64 vbase, i32 k, const gkw_options& opt,
+                    i32* part_out, i64* cut_out, gkw_stats* stats);
+Handle& handle_of(gkw_handle* h);   // the handle behind a C-ABI handle (capi.cu)
 const char* last_error_cstr();
 
 // ---- host helpers ----

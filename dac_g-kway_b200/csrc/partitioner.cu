@@ -55,6 +55,11 @@ __global__ void k_fill_i32(i32* p, i64 n, i32 v) {
   if (i < n) p[i] = v;
 }
 
+__global__ void k_sub_i32(i32* p, i64 n, i32 v) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] -= v;
+}
+
 // returns total vertex weight; throws on malformed input
 i64 validate(Handle& h, const DevGraph& g) {
   Pool::Mark mk = h.scratch.mark();
@@ -80,16 +85,11 @@ i64 validate(Handle& h, const DevGraph& g) {
   return W;
 }
 
-struct PhaseTimer {
-  cudaEvent_t ev[5];
-  explicit PhaseTimer(cudaStream_t s) {
-    for (auto& e : ev) GKW_CUDA(cudaEventCreate(&e));
-    (void)s;
-  }
-  ~PhaseTimer() {
-    for (auto& e : ev) cudaEventDestroy(e);
-  }
-};
+void ensure_timer_events(Handle& h) {
+  if (h.tev_ready) return;
+  for (cudaEvent_t& e : h.tev) GKW_CUDA(cudaEventCreate(&e));
+  h.tev_ready = true;
+}
 
 void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
                            i64* cut_out, gkw_stats* stats) {
@@ -100,8 +100,10 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   GKW_REQUIRE(opt.threshold_factor >= 0, GKW_E_INVALID, "threshold_factor must be >= 0");
   GKW_REQUIRE(opt.init_method == GKW_INIT_DEVICE || (opt.init_method == GKW_INIT_CALLBACK && opt.init_fn),
               GKW_E_INVALID, "init_method CALLBACK needs init_fn");
-  PhaseTimer tm(h.stream);
-  GKW_CUDA(cudaEventRecord(tm.ev[0], h.stream));
+  ensure_timer_events(h);
+  cudaEvent_t* ev = h.tev;              // phase marks
+  cudaEvent_t* lev = h.tev + 5;         // level kernel of slot s: lev[2s], lev[2s+1]
+  GKW_CUDA(cudaEventRecord(ev[0], h.stream));
   const i64 W = validate(h, g0);
   // the reference's MAX_PARTITION_WGT, or the default mode's strict cap
   const float maxw = opt.enforce_balance ? balance_cap(W, k, opt.eps) : max_part_weight(W, k, opt.eps);
@@ -126,7 +128,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     uf_rounds.push_back(co.uf_rounds);
     lv.push_back(nl);
   }
-  GKW_CUDA(cudaEventRecord(tm.ev[1], h.stream));
+  GKW_CUDA(cudaEventRecord(ev[1], h.stream));
 
   // ---- initial partition of the coarsest level ----
   const DevGraph& cg = lv.back().g;
@@ -165,9 +167,11 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     j.balance = true;
     j.bcap = maxw;
     j.move_cap = opt.move_cap;
+    j.ev_start = lev[2 * (nl - 1)];
+    j.ev_end = lev[2 * (nl - 1) + 1];
     level_run(h, rc, cg, j, nl - 1);
   }
-  GKW_CUDA(cudaEventRecord(tm.ev[2], h.stream));
+  GKW_CUDA(cudaEventRecord(ev[2], h.stream));
 
   // ---- uncoarsening (graph_partitioner.hpp:174-192): one launch per level ----
   for (i32 L = nl - 2; L >= 0; --L) {
@@ -178,9 +182,11 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     j.refine = true;
     j.maxw = maxw;
     j.move_cap = opt.move_cap;
+    j.ev_start = lev[2 * L];
+    j.ev_end = lev[2 * L + 1];
     level_run(h, rc, lv[L].g, j, L);
   }
-  GKW_CUDA(cudaEventRecord(tm.ev[3], h.stream));
+  GKW_CUDA(cudaEventRecord(ev[3], h.stream));
   // ---- output and final metrics (graph_partitioner.hpp:194-202) ----
   if (g0.n) {
     GKW_CUDA(cudaMemcpyAsync(d_part_out, refine_part(rc), sizeof(i32) * g0.n, cudaMemcpyDeviceToDevice,
@@ -191,7 +197,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   GKW_CUDA(cudaMemcpyAsync(hm.data(), d_metrics, sizeof(i64) * (k + 2), cudaMemcpyDeviceToHost, h.stream));
   i64 init_cut = 0;
   if (stats) GKW_CUDA(cudaMemcpyAsync(&init_cut, d_init, sizeof(i64), cudaMemcpyDeviceToHost, h.stream));
-  GKW_CUDA(cudaEventRecord(tm.ev[4], h.stream));
+  GKW_CUDA(cudaEventRecord(ev[4], h.stream));
   // one host sync for the statistics, the error words and the metrics above
   std::vector<RefineLevelStats> rs = level_stats(h, rc, nl);
   GKW_REQUIRE(hm[1] == 0, GKW_E_INTERNAL, "partition produced a part id out of range");
@@ -211,6 +217,11 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     for (size_t i = 0; i < lv.size(); ++i) {
       stats->balance_rounds[i] = rs[i].brounds;
       stats->balance_moves[i] = rs[i].bmoves;
+      stats->round_entries[i] = rs[i].rows;
+      const bool ran = (i + 1 < lv.size()) || opt.enforce_balance;
+      float t = 0;
+      if (ran) cudaEventElapsedTime(&t, lev[2 * i], lev[2 * i + 1]);
+      stats->ms_level[i] = ran ? t : -1.0;
     }
     stats->init_cut = init_cut;
     stats->cut = hm[0];
@@ -219,15 +230,64 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     stats->max_part_weight = mx;
     stats->maxw = maxw;
     float a = 0, b = 0, c = 0, d = 0;
-    cudaEventElapsedTime(&a, tm.ev[0], tm.ev[1]);
-    cudaEventElapsedTime(&b, tm.ev[1], tm.ev[2]);
-    cudaEventElapsedTime(&c, tm.ev[2], tm.ev[3]);
-    cudaEventElapsedTime(&d, tm.ev[0], tm.ev[4]);
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    cudaEventElapsedTime(&c, ev[2], ev[3]);
+    cudaEventElapsedTime(&d, ev[0], ev[4]);
     stats->ms_coarsen = a;
     stats->ms_init = b;
     stats->ms_refine = c;
     stats->ms_total = d;
   }
+}
+
+// Partition of a graph held in host memory: copy it into the handle's pool,
+// partition, copy the part ids back.  The host arrays may be a slice of a
+// larger concatenated CSR: `xadj` values are then offset by xadj[0] and
+// neighbour ids by `vbase`, and both are rebased on the device.
+void partition_host(Handle& hh, const DevGraph& hg, i64 vbase, i32 k, const gkw_options& o, i32* part_out,
+                    i64* cut_out, gkw_stats* stats) {
+  GKW_REQUIRE(hg.n >= 0 && hg.m >= 0, GKW_E_INVALID, "negative size");
+  GKW_REQUIRE(hg.n == 0 || part_out != nullptr, GKW_E_INVALID, "part_out is NULL");
+  GKW_REQUIRE(vbase >= 0 && vbase < ((i64)1 << 31), GKW_E_UNSUPPORTED, "vertex offset out of range");
+  hh.hier.reset();
+  hh.scratch.reset();
+  const i64 n = hg.n, m = hg.m;
+  i32* x = hh.hier.alloc_n<i32>(n + 1);
+  i32* a = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
+  i32* w = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
+  i32* vw = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
+  i32* part = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
+  GKW_CUDA(cudaMemcpyAsync(x, hg.xadj, sizeof(i32) * (n + 1), cudaMemcpyHostToDevice, hh.stream));
+  const i32 ebase = hg.xadj[0];
+  if (ebase != 0) {
+    launch(k_sub_i32, ceil_div(n + 1, 256), 256, 0, hh.stream, x, n + 1, ebase);
+    GKW_CHECK_LAUNCH();
+  }
+  if (m) {
+    GKW_CUDA(cudaMemcpyAsync(a, hg.adjncy, sizeof(i32) * m, cudaMemcpyHostToDevice, hh.stream));
+    if (vbase != 0) {
+      launch(k_sub_i32, ceil_div(m, 256), 256, 0, hh.stream, a, m, (i32)vbase);
+      GKW_CHECK_LAUNCH();
+    }
+    if (hg.adjwgt) GKW_CUDA(cudaMemcpyAsync(w, hg.adjwgt, sizeof(i32) * m, cudaMemcpyHostToDevice, hh.stream));
+    else launch(k_fill_i32, ceil_div(m, 256), 256, 0, hh.stream, w, m, 1);
+  }
+  if (n) {
+    if (hg.vwgt) GKW_CUDA(cudaMemcpyAsync(vw, hg.vwgt, sizeof(i32) * n, cudaMemcpyHostToDevice, hh.stream));
+    else launch(k_fill_i32, ceil_div(n, 256), 256, 0, hh.stream, vw, n, 1);
+  }
+  GKW_CHECK_LAUNCH();
+  DevGraph g;
+  g.n = hg.n;
+  g.m = m;
+  g.xadj = x;
+  g.adjncy = a;
+  g.adjwgt = w;
+  g.vwgt = vw;
+  partition_impl(hh, g, k, o, part, cut_out, stats);
+  if (n) GKW_CUDA(cudaMemcpyAsync(part_out, part, sizeof(i32) * n, cudaMemcpyDeviceToHost, hh.stream));
+  GKW_CUDA(cudaStreamSynchronize(hh.stream));
 }
 
 }  // namespace gkw

@@ -27,10 +27,10 @@ namespace gkw {
 static constexpr u32 kFullMask = 0xffffffffu;
 constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pass
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
-constexpr i32 kBadWords = kMaxMoveCap / 32;
 constexpr int kLevelThreads = 512;
 constexpr i32 kGreedySmemParts = 4096;   // balance greedy pass: part weights in smem up to this k
 constexpr i32 kGreedyWords = 3 * kMaxMoveCap + kGreedySmemParts;
+static_assert((size_t)kGreedyWords * 4 >= (size_t)kSortMax * 8, "the sort's second buffer aliases the greedy region");
 constexpr i32 kStatSlots = GKW_MAX_LEVELS + 2;
 constexpr i32 kTraceCap = 4096;   // phase marks per level (diagnostic timeline)
 
@@ -44,7 +44,7 @@ struct RoundState {
   i32 rounds;
   i64 moves;
   i64 gain_sum;
-  u32 bad[kBadWords];
+  i32 pos;          // refinement: moves 0..pos of top are applied
   i32 bdone;
   i32 brounds;
   i64 bmoves;
@@ -52,12 +52,14 @@ struct RoundState {
   i32 firstbad;
   i32 light;
   u32 epoch;
+  u64 rows;   // adjacency entries read by the gain updates of the rounds
 };
 
 
 struct LevelStatsDev {
   i32 rounds, brounds;
   i64 moves, gain_sum, bmoves;
+  i64 rows;
   i32 err;
   i32 pad;
 };
@@ -257,7 +259,9 @@ __device__ void ph_lists(const LevelArgs& a) {
 // than the own part, ties to the smaller part id, taken only if that value is
 // > 0 -- the reference's `if (gain > max_gain)` with an unsigned max_gain.
 // Vertices whose new gain is positive join P.
-__device__ void ph_update(const LevelArgs& a, u32* acc_all) {
+// `count`: add the row lengths read to the level's entry counter (the update
+// passes of the rounds; the first pass of a level is counted as a full pass).
+__device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid >= a.acc_warps) return;
   u32* acc = acc_all + (size_t)wid * a.k;
@@ -266,10 +270,12 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all) {
   i32* Pout = a.P0;          // P is never compacted within a level: entries whose
   i32* pcount = &st->pcount[0];   // gain dropped stay and are skipped by gain
   const i64 nw = (i64)gridDim.x * a.acc_warps;
+  unsigned long long rows = 0;
   for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nU; i += nw) {
     const i32 v = ldc(a.U + i);
     const i32 p = ldc(a.part + v);
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+    rows += (unsigned long long)(end - beg);
     bool bl = false;
     for (i32 e = beg + lane; e < end; e += 32) {
       const i32 q = ldc(a.part + a.adjncy[e]);
@@ -308,6 +314,7 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all) {
     for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
     __syncwarp();
   }
+  if (count && lane == 0 && rows) atomicAdd(reinterpret_cast<unsigned long long*>(&st->rows), rows);
 }
 
 // Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
@@ -356,7 +363,237 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
 // (uncoarsen.hpp:471-476 with move_request.hpp:36-41).  Block 0 only; more than
 // kSortMax candidates are streamed through shared memory keeping the running
 // top `cap`.  Resets the per-round counters.
-__device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, bool balance_mode) {
+// Block-wide exclusive scan of one u32 per thread (blockDim <= 1024).
+__device__ __forceinline__ u32 block_exscan_u32(u32 x, u32* s_warp, u32& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  u32 inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(kFullMask, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_warp[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    const u32 w = lane < nw ? s_warp[lane] : 0;
+    u32 wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 y = __shfl_up_sync(kFullMask, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < nw) s_warp[lane] = wi - w;
+    if (lane == nw - 1) s_warp[32] = wi;
+  }
+  __syncthreads();
+  const u32 r = inc - x + s_warp[wid];
+  total = s_warp[32];
+  __syncthreads();
+  return r;
+}
+
+// Ascending sort of one u64 per lane across a warp (bitonic network).
+__device__ __forceinline__ u64 warp_sort_u64(u64 x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const u64 y = __shfl_xor_sync(kFullMask, x, j);
+      const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+      x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
+    }
+  return x;
+}
+
+// Ascending block sort of s[0..P), P a power of two >= 32, by the whole
+// block: every warp sorts runs of 32 in registers, then runs are merged
+// pairwise (merge path: each thread finds where its outputs start by binary
+// search, then merges them sequentially), ping-ponging between s and t.
+// Returns the buffer holding the result.
+__device__ u64* block_merge_sort(u64* s, u64* t, i32 P) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (i32 r = wid; r < (P >> 5); r += nw) s[r * 32 + lane] = warp_sort_u64(s[r * 32 + lane]);
+  __syncthreads();
+  u64* src = s;
+  u64* dst = t;
+  const i32 E = P > (i32)blockDim.x ? P / (i32)blockDim.x : 1;   // outputs per thread
+  for (i32 L = 32; L < P; L <<= 1) {
+    for (i32 o0 = threadIdx.x * E; o0 < P; o0 += blockDim.x * E) {
+      const i32 b = o0 & ~(2 * L - 1);
+      const i32 d = o0 - b;
+      const u64* A = src + b;
+      const u64* Bv = src + b + L;
+      i32 lo = d > L ? d - L : 0, hi = d < L ? d : L;
+      while (lo < hi) {
+        const i32 mid = (lo + hi) >> 1;
+        if (A[mid] <= Bv[d - 1 - mid]) lo = mid + 1;
+        else hi = mid;
+      }
+      i32 i = lo, j = d - lo;
+      for (i32 e = 0; e < E; ++e) {
+        const bool takeA = j >= L || (i < L && A[i] <= Bv[j]);
+        dst[o0 + e] = takeA ? A[i++] : Bv[j++];
+      }
+    }
+    __syncthreads();
+    u64* tmp = src;
+    src = dst;
+    dst = tmp;
+  }
+  return src;
+}
+
+// Largest balanced prefix index of the sorted moves s[0..B)
+// (uncoarsen.hpp:239-288, find_mv_wgt_sequence + find_balance_sequence):
+// D[p][j] = the weight moved into part p minus the weight moved out of it by
+// moves 0..j; index j is balanced when every part with D[p][j] > 0 keeps
+// (float)(pw[p] + D[p][j]) <= MAXW.  Each move is two events (part, index,
+// +-w).  Sorted by (part, index), a segmented scan gives D after each event,
+// and D holds until the part's next event; an event that breaks the cap marks
+// that index range in a difference array.  The result is the largest
+// unmarked index, 0 if every index is marked (move 0 is applied regardless,
+// as in the reference: its -1 case is dead code, uncoarsen.hpp:481-488).
+// Block 0 only; t is a second buffer of kSortMax keys; s is overwritten.
+__device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u32* s_warp) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const i32 E = 2 * B;
+  i32 P = 32;
+  while (P < E) P <<= 1;
+  for (i32 m = threadIdx.x; m < B; m += blockDim.x) {
+    const i32 v = (i32)(u32)s[m];
+    const i32 src = ldc(a.part + v), dst = ldc(a.target + v);
+    const u32 w = (u32)a.vwgt[v];
+    t[2 * m] = ((u64)(u32)dst << 43) | ((u64)m << 32) | w;
+    t[2 * m + 1] = ((u64)(u32)src << 43) | ((u64)m << 32) | (u32)(0u - w);
+  }
+  for (i32 i = E + threadIdx.x; i < P; i += blockDim.x) t[i] = ~0ull;
+  __syncthreads();
+  u64* ev = block_merge_sort(t, s, P);
+  i32* diff = reinterpret_cast<i32*>(ev == t ? s : t);   // B + 1 counters
+  for (i32 j = threadIdx.x; j <= B; j += blockDim.x) diff[j] = 0;
+  // segmented inclusive scan of the deltas, R consecutive events per thread
+  constexpr i32 kMaxR = kSortMax / kLevelThreads;
+  const i32 R = P > (i32)blockDim.x ? P / (i32)blockDim.x : 1;
+  const i32 i0 = threadIdx.x * R;
+  i32 val[kMaxR];
+  u32 head_seen = 0;
+  i32 acc = 0;
+#pragma unroll
+  for (i32 r = 0; r < kMaxR; ++r) {
+    val[r] = 0;
+    const i32 i = i0 + r;
+    if (r < R && i < E) {
+      const u64 e = ev[i];
+      const bool head = i == 0 || (ev[i - 1] >> 43) != (e >> 43);
+      const i32 d = (i32)(u32)e;
+      acc = head ? d : acc + d;
+      head_seen |= head ? (1u << r) : 0u;
+      val[r] = acc;
+    }
+  }
+  // exclusive scan over threads of (has head, running sum) pairs:
+  // (f1, v1) + (f2, v2) = (f1 | f2, f2 ? v2 : v1 + v2)
+  u32 f = head_seen ? 1u : 0u;
+  i32 v = acc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 fo = __shfl_up_sync(kFullMask, f, o);
+    const i32 vo = __shfl_up_sync(kFullMask, v, o);
+    if (lane >= o) {
+      if (!f) v += vo;
+      f |= fo;
+    }
+  }
+  u32 fe = __shfl_up_sync(kFullMask, f, 1);
+  i32 ve = __shfl_up_sync(kFullMask, v, 1);
+  if (lane == 0) {
+    fe = 0;
+    ve = 0;
+  }
+  if (lane == 31) {
+    s_warp[wid] = (u32)v;
+    s_warp[16 + wid] = f;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    u32 wf = lane < nw ? s_warp[16 + lane] : 0u;
+    i32 wv = lane < nw ? (i32)s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 fo = __shfl_up_sync(kFullMask, wf, o);
+      const i32 vo = __shfl_up_sync(kFullMask, wv, o);
+      if (lane >= o) {
+        if (!wf) wv += vo;
+        wf |= fo;
+      }
+    }
+    // exclusive prefix of each warp
+    u32 pf = __shfl_up_sync(kFullMask, wf, 1);
+    i32 pv = __shfl_up_sync(kFullMask, wv, 1);
+    if (lane == 0) {
+      pf = 0;
+      pv = 0;
+    }
+    __syncwarp();
+    if (lane < nw) {
+      s_warp[lane] = (u32)pv;
+      s_warp[16 + lane] = pf;
+    }
+  }
+  __syncthreads();
+  {
+    const u32 pf = s_warp[16 + wid];
+    const i32 pv = (i32)s_warp[wid];
+    const i32 carry = fe ? ve : pv + ve;   // running sum entering this thread
+    (void)pf;
+    const float maxw = a.maxw;
+#pragma unroll
+    for (i32 r = 0; r < kMaxR; ++r) {
+      const i32 i = i0 + r;
+      if (r < R && i < E) {
+        const bool before_head = (head_seen & ((2u << r) - 1u)) == 0;
+        const i32 D = before_head ? val[r] + carry : val[r];
+        const u64 e = ev[i];
+        const u32 p = (u32)(e >> 43);
+        if (D > 0 && __uint2float_rn((u32)D + ldc(a.pw + p)) > maxw) {
+          const i32 m = (i32)((e >> 32) & 0x7FFu);
+          const i32 end = (i + 1 < E && (ev[i + 1] >> 43) == (e >> 43)) ? (i32)((ev[i + 1] >> 32) & 0x7FFu) : B;
+          atomicAdd(&diff[m], 1);
+          atomicAdd(&diff[end], -1);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // marks per index = prefix of diff; the largest index with none
+  const i32 R2 = (B + (i32)blockDim.x - 1) / (i32)blockDim.x;
+  const i32 j0 = threadIdx.x * R2;
+  i32 loc = 0;
+  for (i32 j = j0; j < j0 + R2 && j < B; ++j) loc += diff[j];
+  u32 tot;
+  i32 run = (i32)block_exscan_u32((u32)loc, s_warp, tot);
+  i32 best = -1;
+  for (i32 j = j0; j < j0 + R2 && j < B; ++j) {
+    run += diff[j];
+    if (run == 0) best = j;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const i32 y = __shfl_xor_sync(kFullMask, best, o);
+    best = best > y ? best : y;
+  }
+  __syncthreads();
+  if (lane == 0) s_warp[wid] = (u32)best;
+  __syncthreads();
+  i32 pos = -1;
+  for (i32 w = 0; w < nw; ++w) pos = pos > (i32)s_warp[w] ? pos : (i32)s_warp[w];
+  __syncthreads();
+  return pos < 0 ? 0 : pos;
+}
+
+__device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, bool balance_mode) {
   if (blockIdx.x != 0) return;
   RoundState* st = a.st;
   const i32 cnt = ldc(&st->ccount);
@@ -394,7 +631,12 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, bool balance_
     while (P < cnt) P <<= 1;
     for (i32 i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cnt ? ldc(a.cands + i) : ~0ull;
     __syncthreads();
-    bitonic(P);
+    // the greedy region is free until the greedy pass and holds kSortMax keys
+    u64* t = reinterpret_cast<u64*>(greedy);
+    if (block_merge_sort(s, t, P) == t) {
+      for (i32 i = threadIdx.x; i < B; i += blockDim.x) s[i] = t[i];
+      __syncthreads();
+    }
   } else {
     i32 next = 0;
     bool first = true;
@@ -412,7 +654,8 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, bool balance_
   }
   if (!balance_mode) {
     for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
-    for (i32 i = threadIdx.x; i < (B + 31) / 32; i += blockDim.x) st->bad[i] = 0;
+    const i32 pos = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp);
+    if (threadIdx.x == 0) st->pos = pos;
   } else {
     // greedy pass in sorted order: take a move while its source is still
     // overweight and its destination stays within the cap, skip the others.
@@ -453,72 +696,6 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, bool balance_
   }
 }
 
-// Block-wide exclusive scan of one u32 per thread (blockDim <= 1024).
-__device__ __forceinline__ u32 block_exscan_u32(u32 x, u32* s_warp, u32& total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  u32 inc = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const u32 y = __shfl_up_sync(kFullMask, inc, o);
-    if (lane >= o) inc += y;
-  }
-  if (lane == 31) s_warp[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    const int nw = blockDim.x >> 5;
-    const u32 w = lane < nw ? s_warp[lane] : 0;
-    u32 wi = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const u32 y = __shfl_up_sync(kFullMask, wi, o);
-      if (lane >= o) wi += y;
-    }
-    if (lane < nw) s_warp[lane] = wi - w;
-    if (lane == nw - 1) s_warp[32] = wi;
-  }
-  __syncthreads();
-  const u32 r = inc - x + s_warp[wid];
-  total = s_warp[32];
-  __syncthreads();
-  return r;
-}
-
-constexpr int kIT = kMaxMoveCap / kLevelThreads;   // moves per thread in the per-part checks
-
-// Refinement balance check (uncoarsen.hpp:239-288): part p's weight change
-// prefix over the sorted moves; every prefix index j whose change is positive
-// and pushes p over MAXW is flagged.  A prefix is balanced when no part flags it.
-__device__ void ph_check_refine(const LevelArgs& a, u32* s_warp) {
-  RoundState* st = a.st;
-  const i32 B = ldc(&st->B);
-  for (i32 p = blockIdx.x; p < a.k; p += gridDim.x) {
-    i32 e[kIT];
-    i32 sum = 0;
-#pragma unroll
-    for (int i = 0; i < kIT; ++i) {
-      const i32 j = threadIdx.x * kIT + i;
-      i32 d = 0;
-      if (j < B) {
-        const i32 v = (i32)(u32)ldc(a.top + j);
-        const i32 w = a.vwgt[v];
-        if (ldc(a.target + v) == p) d += w;
-        if (ldc(a.part + v) == p) d -= w;
-      }
-      e[i] = d;
-      sum += d;
-    }
-    u32 tot;
-    i32 run = (i32)block_exscan_u32((u32)sum, s_warp, tot);
-    const u32 base = ldc(a.pw + p);
-#pragma unroll
-    for (int i = 0; i < kIT; ++i) {
-      const i32 j = threadIdx.x * kIT + i;
-      run += e[i];
-      if (j < B && run > 0 && __uint2float_rn((u32)run + base) > a.maxw) atomicOr(&st->bad[j >> 5], 1u << (j & 31));
-    }
-  }
-}
-
 // U appends of one apply phase, staged per CTA in shared memory (one global
 // atomic per CTA); entries beyond the stage go to U directly.
 constexpr i32 kUStage = 1024;
@@ -547,18 +724,7 @@ __device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
 // (uncoarsen.hpp:290-323).  One warp per move.
 __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
-  const i32 B = ldc(&st->B);
-  i32 pos = 0;
-  const i32 nwords = (B + 31) >> 5;
-  for (i32 w = nwords - 1; w >= 0; --w) {
-    u32 valid = kFullMask;
-    if (w == nwords - 1 && (B & 31)) valid = (1u << (B & 31)) - 1;
-    const u32 zeros = ~ldc(&st->bad[w]) & valid;
-    if (zeros) {
-      pos = w * 32 + 31 - __clz(zeros);
-      break;
-    }
-  }
+  const i32 pos = ldc(&st->pos);
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
@@ -576,6 +742,7 @@ __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
     const u64 key = ldc(a.top + j);
     const i32 v = (i32)(u32)key;
     const i32 s = ldc(a.part + v), d = ldc(a.target + v);
+    const i32 beg = a.xadj[v], end = a.xadj[v + 1];   // issued beside the loads above
     if (lane == 0) {
       const u32 w = (u32)a.vwgt[v];
       atomicAdd(&a.pw[d], w);
@@ -584,7 +751,6 @@ __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
       atomicAdd(&s_gsum, (unsigned long long)(i64)key_gain(key));
       if (atomicExch(&a.updflag[v], 1) == 0) ustage_push(S, v, a.U, &st->ucount);
     }
-    const i32 beg = a.xadj[v], end = a.xadj[v + 1];
     for (i32 e = beg + lane; e < end; e += 32) {
       const i32 u = a.adjncy[e];
       if (atomicExch(&a.updflag[u], 1) == 0) ustage_push(S, u, a.U, &st->ucount);
@@ -790,7 +956,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
     trace_mark(a, 2);
   }
-  if (a.flags & LF_UPDATE) ph_update(a, acc_all);
+  if (a.flags & LF_UPDATE) ph_update(a, acc_all, false);
   if (a.flags & LF_BALANCE) ph_bal_prep(a, s_tmp);
   if (a.flags & (LF_UPDATE | LF_BALANCE)) {
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
@@ -812,14 +978,14 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       ph_bal_emit(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 11);
-      ph_select(a, s_sort, greedy, true);
+      ph_select(a, s_sort, greedy, s_warp, true);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 12);
       if (ldc(&st->bdone)) break;
       ph_apply_balance(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 14);
-      ph_update(a, acc_all);
+      ph_update(a, acc_all, true);
       ph_bal_prep(a, s_tmp);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 15);
@@ -834,17 +1000,14 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       ph_candidates(a, &s_cnt, &s_base);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 20);
-      ph_select(a, s_sort, greedy, false);
+      ph_select(a, s_sort, greedy, s_warp, false);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 21);
       if (ldc(&st->done)) break;
-      ph_check_refine(a, s_warp);
-      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
-      trace_mark(a, 22);
       ph_apply_refine(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 23);
-      ph_update(a, acc_all);
+      ph_update(a, acc_all, true);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 24);
     }
@@ -856,6 +1019,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
     o->gain_sum = ldc(&st->gain_sum);
     o->brounds = ldc(&st->brounds);
     o->bmoves = ldc(&st->bmoves);
+    o->rows = (i64)ldc(&st->rows);
     o->err = *(volatile i32*)a.err;
   }
 }
@@ -919,7 +1083,14 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   const i32 w = (i32)std::min<size_t>(kLevelThreads / 32, budget / (4 * (size_t)c->k));
   c->acc_warps = std::max(1, w);
   c->smem = (size_t)kSortMax * 8 + (size_t)kGreedyWords * 4 + (size_t)c->acc_warps * c->k * 4;
-  GKW_CUDA(cudaFuncSetAttribute(k_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+  // one value for every handle of the process (handles of a server launch
+  // this kernel concurrently with different sizes): the device's opt-in limit
+  // less the kernel's static shared memory
+  cudaFuncAttributes fa;
+  GKW_CUDA(cudaFuncGetAttributes(&fa, k_level));
+  const int max_dyn = h.smem_optin - (int)fa.sharedSizeBytes;
+  GKW_REQUIRE(c->smem <= (size_t)max_dyn, GKW_E_UNSUPPORTED, "level kernel needs too much shared memory");
+  GKW_CUDA(cudaFuncSetAttribute(k_level, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
   int bps = 0;
   GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_level, kLevelThreads, c->smem));
   GKW_REQUIRE(bps >= 1, GKW_E_UNSUPPORTED, "level kernel does not fit on an SM");
@@ -1051,13 +1222,14 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   }
   // small levels use fewer CTAs: the barrier gets cheaper and the work fits;
   // at least enough CTAs for the per-part checks to run in few passes
-  i32 grid = (i32)ceil_div(std::max(g.n, 1), 2048);
+  i32 grid = (i32)ceil_div(std::max(g.n, 1), 512);
   grid = std::max(grid, std::max(32, c->k / 4));
   grid = std::min(grid, c->grid);
+  grid = coop_grid(h, (const void*)k_level, grid, kLevelThreads, c->smem);
   void* args[] = {&a};
-  GKW_CUDA(cudaLaunchCooperativeKernel((void*)k_level, dim3(grid), dim3(kLevelThreads), args, c->smem,
-                                       h.stream));
-  count_launch();
+  if (j.ev_start) GKW_CUDA(cudaEventRecord(j.ev_start, h.stream));
+  launch_coop(h, (const void*)k_level, grid, kLevelThreads, c->smem, args);
+  if (j.ev_end) GKW_CUDA(cudaEventRecord(j.ev_end, h.stream));
   c->cur = dst;
 }
 
@@ -1104,6 +1276,7 @@ std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots) {
     out[i].gain_sum = d[i].gain_sum;
     out[i].brounds = d[i].brounds;
     out[i].bmoves = d[i].bmoves;
+    out[i].rows = d[i].rows;
   }
   return out;
 }

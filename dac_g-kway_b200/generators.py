@@ -199,3 +199,53 @@ def check_csr(g: Csr) -> None:
     ro = np.argsort(rev)
     if not np.array_equal(fwd[fo], rev[ro]) or not np.array_equal(g.adjwgt[fo], g.adjwgt[ro]):
         raise ValueError("not symmetric")
+
+
+def write_metis(g: Csr, path: str) -> None:
+    """Write ``g`` as a METIS .graph file: header ``n |E|`` (unit weights) or
+    ``n |E| 011`` (vertex and edge weights), then one line per vertex with its
+    1-based neighbours (preceded by the vertex weight and followed each by its
+    edge weight in the weighted form)."""
+    weighted = bool(np.any(g.adjwgt != 1) or np.any(g.vwgt != 1))
+    deg = np.diff(g.xadj)
+    with open(path, "w") as f:
+        f.write(f"{g.n} {g.n_edges}" + (" 011" if weighted else "") + "\n")
+        adj1 = (g.adjncy.astype(np.int64) + 1).astype(str)
+        if weighted:
+            wstr = g.adjwgt.astype(str)
+        lines = []
+        for v in range(g.n):
+            a, b = int(g.xadj[v]), int(g.xadj[v + 1])
+            if weighted:
+                toks = [str(int(g.vwgt[v]))]
+                for e in range(a, b):
+                    toks.append(adj1[e])
+                    toks.append(wstr[e])
+                lines.append(" ".join(toks))
+            else:
+                lines.append(" ".join(adj1[a:b]) if deg[v] else "")
+            if len(lines) >= 65536:
+                f.write("\n".join(lines) + "\n")
+                lines = []
+        if lines:
+            f.write("\n".join(lines) + "\n")
+
+
+def _main(argv) -> int:
+    """``generators.py <delaunay|grid27|road|circuit> <args...> <out.graph>``:
+    delaunay N SEED | grid27 NX NY NZ | road N SEED | circuit N SEED."""
+    if len(argv) < 3:
+        print(_main.__doc__)
+        return 2
+    kind, out = argv[0], argv[-1]
+    a = [int(x) for x in argv[1:-1]]
+    g = {"delaunay": lambda: delaunay(a[0], a[1]), "grid27": lambda: grid27(a[0], a[1], a[2]),
+         "road": lambda: road(a[0], a[1]), "circuit": lambda: circuit(a[0], a[1])}[kind]()
+    write_metis(g, out)
+    print(f"{out}: n={g.n} edges={g.n_edges}")
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(_main(sys.argv[1:]))

@@ -36,7 +36,8 @@ typedef enum gkw_status {
   GKW_E_NOMEM = 3,        /* device allocation failed */
   GKW_E_UNSUPPORTED = 4,  /* input outside the supported range (e.g. k too large) */
   GKW_E_INIT = 5,         /* the initial-partition callback failed */
-  GKW_E_INTERNAL = 6
+  GKW_E_INTERNAL = 6,
+  GKW_E_PENDING = 7       /* served request not finished yet (gkw_server_poll) */
 } gkw_status;
 
 typedef struct gkw_handle gkw_handle;
@@ -90,6 +91,12 @@ typedef struct gkw_stats {
   int64_t max_part_weight;
   float maxw;                           /* MAX_PARTITION_WGT (graph_partitioner.hpp:230) */
   double ms_coarsen, ms_init, ms_refine, ms_total;   /* device time per phase */
+  /* Per level: device time of its level-kernel launch (projection, balance
+   * and refinement rounds; the coarsest level's is its balance pass, -1 when
+   * it has none), and the adjacency entries read by the gain updates of its
+   * rounds (the first full gain pass of the level not included). */
+  double ms_level[GKW_MAX_LEVELS];
+  int64_t round_entries[GKW_MAX_LEVELS];
 } gkw_stats;
 
 /* ---- handle ---------------------------------------------------------- */
@@ -213,6 +220,90 @@ gkw_status gkw_cut_noalloc(const gkw_csr* d_graph, const int32_t* d_part, int32_
 
 /* MAX_PARTITION_WGT as the reference computes it (graph_partitioner.hpp:230). */
 float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps);
+
+/* ---- batched and served forms -----------------------------------------
+ * No counterpart in the reference, whose driver partitions one graph per
+ * process run (main/main.cu:5-20).  A server owns `slots` partition slots on
+ * one device (each a handle with its own stream and device memory) and a
+ * queue of jobs; slots take jobs as they and the device-memory budget free
+ * up, so jobs of different sizes overlap on the GPU.  Every job runs the same
+ * pipeline as gkw_partition: a graph's result is the same alone, in a batch
+ * and among served requests.  Input graphs are host memory. */
+typedef struct gkw_server gkw_server;
+
+typedef struct gkw_server_config {
+  int32_t slots;             /* concurrent partitions (default 8) */
+  int32_t narrow_max_n;      /* jobs up to this many vertices run their barrier kernels as
+                                one thread-block cluster each, so any number of them can
+                                share the device; larger jobs take turns for their wide
+                                grids (default 262144) */
+  int64_t pool_bytes;        /* device-memory budget of all slots together (default 64 GiB,
+                                capped at 90% of the free memory at creation) */
+  int64_t slot_keep_bytes;   /* memory a slot keeps between jobs (default 256 MiB) */
+  int32_t max_bypass;        /* times the oldest waiting job may be overtaken by smaller
+                                jobs that fit when it does not (default 4 x slots) */
+  int32_t reserved[7];
+} gkw_server_config;
+
+void gkw_server_default_config(gkw_server_config* cfg);
+gkw_status gkw_server_create(gkw_server** out, int32_t device, const gkw_server_config* cfg);
+/* Waits for the running jobs, drops the queued ones, frees everything. */
+gkw_status gkw_server_destroy(gkw_server* s);
+
+/* Device memory one partition of a graph of n vertices and nnz CSR entries
+ * is predicted to need (input, level hierarchy, refinement state, scratch):
+ * the admission measure of the server. */
+int64_t gkw_predict_footprint(int32_t n, int64_t nnz, int32_t k);
+
+/* Served form.  submit copies the graph (the caller may free it on return) and
+ * queues it; `ticket_out` names the request.  poll waits up to wait_ms
+ * (0: no wait, <0: until done) and returns GKW_E_PENDING if the request is
+ * still queued or running, else its status; on GKW_OK it copies the n part
+ * ids to part_out (may be NULL) and the cut to cut_out (may be NULL).  A
+ * finished request is forgotten after the poll that reports it. */
+typedef struct gkw_request_info {
+  double queue_ms;           /* submit -> start on a slot */
+  double run_ms;             /* start -> result on the host */
+  double latency_ms;         /* submit -> result on the host */
+  int64_t predicted_bytes;
+  int32_t slot;
+  int32_t n_levels;
+} gkw_request_info;
+
+gkw_status gkw_server_submit(gkw_server* s, const gkw_csr* graph, int32_t k, const gkw_options* opt,
+                             int64_t* ticket_out);
+gkw_status gkw_server_poll(gkw_server* s, int64_t ticket, int32_t wait_ms, int32_t* part_out,
+                           int64_t* cut_out, gkw_request_info* info);
+
+typedef struct gkw_server_stats {
+  int64_t submitted, completed, failed;
+  double p50_ms, p99_ms, max_ms;   /* latency (submit -> result) of the completed requests */
+  double mean_queue_ms;
+  double graphs_per_s;             /* completed / (last completion - first submit) */
+  int64_t peak_reserved_bytes;     /* largest sum of predicted footprints admitted at once */
+  int32_t peak_running;            /* most jobs running at once */
+  int32_t slots;
+} gkw_server_stats;
+/* Statistics since creation or the last reset (reset != 0 clears them after reading). */
+gkw_status gkw_server_stats_get(gkw_server* s, gkw_server_stats* out, int32_t reset);
+
+/* Batched form: many independent graphs in one call, as one concatenated CSR.
+ * `graph` is their disjoint union with global 0-based ids (graph g owns the
+ * vertices [graph_ptr[g], graph_ptr[g+1]); no edge joins two graphs).
+ * part_out[v] receives v's part id within its own graph, in [0, k[g]).
+ * Graphs are scheduled largest first.  Returns GKW_OK if every graph was
+ * partitioned, else the status of the first graph that failed (its index in
+ * the message); status_out (may be NULL) gets each graph's status. */
+typedef struct gkw_csr_batch {
+  gkw_csr graph;             /* host memory; adjwgt / vwgt may be NULL */
+  int32_t n_graphs;
+  const int32_t* graph_ptr;  /* [n_graphs + 1] */
+  const int32_t* k;          /* [n_graphs] */
+  const double* eps;         /* [n_graphs], or NULL for opt->eps */
+} gkw_csr_batch;
+
+gkw_status gkw_partition_batch(gkw_server* s, const gkw_csr_batch* batch, const gkw_options* opt,
+                               int32_t* part_out, int64_t* cut_out, int32_t* status_out);
 
 #ifdef __cplusplus
 }

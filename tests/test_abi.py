@@ -120,3 +120,13 @@ def test_generators(gen):
     c = gen.circuit(20000, seed=3, levels=50, hub_max=2000)
     gen.check_csr(c)
     assert c.adjwgt.min() >= 1 and c.adjwgt.max() <= 8 and c.vwgt.min() >= 1 and c.vwgt.max() <= 4
+
+
+@pytest.mark.parametrize("kind", ["unit", "weighted"])
+def test_write_metis_round_trip(pkg, gen, tmp_path, kind):
+    g = gen.delaunay(3000, 5) if kind == "unit" else gen.circuit(5000, 3)
+    p = str(tmp_path / "g.graph")
+    gen.write_metis(g, p)
+    x, a, w, vw = pkg.read_metis(p)
+    assert np.array_equal(x, g.xadj) and np.array_equal(a, g.adjncy)
+    assert np.array_equal(w, g.adjwgt) and np.array_equal(vw, g.vwgt)
