@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(kUfThreads) k_uf_persist(i32 n, const i32* __r
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     chg[0] = 0;
     chg[1] = 0;
+    chg[2] = 0;
   }
   if (!grid_barrier(bar, err, &s_flag)) return;
   u64* buf[2] = {k0, k1};
@@ -122,11 +123,14 @@ __global__ void __launch_bounds__(kUfThreads) k_uf_persist(i32 n, const i32* __r
     }
     if (diff) s_any = 1;
     __syncthreads();
-    if (threadIdx.x == 0 && s_any) atomicOr(&chg[it & 1], 1);
-    // chg[(it+1)&1] was read by every CTA after the previous barrier
-    if (blockIdx.x == 0 && threadIdx.x == 0) chg[(it + 1) & 1] = 0;
+    // change flags rotate over three words: round it raises chg[it % 3], which
+    // every thread reads after this round's barrier; block 0 clears
+    // chg[(it + 1) % 3] now, whose last reads (round it - 2) all happened
+    // before their CTAs arrived at the previous barrier
+    if (threadIdx.x == 0 && s_any) atomicOr(&chg[it % 3], 1);
+    if (blockIdx.x == 0 && threadIdx.x == 0) chg[(it + 1) % 3] = 0;
     if (!grid_barrier(bar, err, &s_flag)) return;
-    if (ldcg(&chg[it & 1]) == 0) {
+    if (ldcg(&chg[it % 3]) == 0) {
       rounds = it;
       break;
     }
@@ -145,7 +149,7 @@ void run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out, i32* d_rou
   }
   Pool::Mark mk = h.scratch.mark();
   u64* kb = h.scratch.alloc_n<u64>(n);
-  i32* chg = h.scratch.alloc_n<i32>(2);
+  i32* chg = h.scratch.alloc_n<i32>(3);
   int bps = 0;
   GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_uf_persist, kUfThreads, 0));
   GKW_REQUIRE(bps >= 1, GKW_E_INTERNAL, "union-find kernel does not fit on an SM");

@@ -40,7 +40,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, i32* err, i32* s_fl
   if (cluster_ncta() == gridDim.x) {
     // the grid is one thread-block cluster (launch_coop): the hardware
     // cluster barrier, release/acquire at cluster scope
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
     return true;
   }
   __syncthreads();
