@@ -635,13 +635,72 @@ def bench_served(args):
                                  "timing": "wall clock, submit to result on the host"}}))
 
 
+def bench_configs(args):
+    """The other plain-method configurations at full size, each on one GPU:
+    27-point grid 100x100x96 (k=64), road-like graph of 12M points and
+    circuit-like graph of 4M vertices (k=256).  Device-resident timing with
+    CUDA events (L2 flushed between steps), as for the headline line."""
+    import torch
+    import __graft_entry__ as ge
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    gen = ge.load_generators()
+    dev = torch.device("cuda", 0)
+    cases = [("grid27 100x100x96", lambda: gen.grid27(100, 100, 96), 64),
+             ("road 12M points", lambda: gen.road(12000000, 1), 256),
+             ("circuit 4M vertices", lambda: gen.circuit(4000000, 1), 256)]
+    out = []
+    for name, make, k in cases:
+        path = os.path.join(CACHE_DIR, name.replace(" ", "_") + ".npz")
+        if os.path.exists(path):
+            with np.load(path) as d:
+                g = gen.Csr(d["x"], d["a"], d["w"], d["v"])
+        else:
+            g = make()
+            os.makedirs(CACHE_DIR, exist_ok=True)
+            np.savez(path + ".tmp.npz", x=g.xadj, a=g.adjncy, w=g.adjwgt, v=g.vwgt)
+            os.replace(path + ".tmp.npz", path)
+        h = pkg.Handle(0)
+        stream = torch.cuda.ExternalStream(h.stream, device=dev)
+        t = [torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.adjwgt, g.vwgt)]
+        part = torch.empty(g.n, dtype=torch.int32, device=dev)
+        flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+        for _ in range(max(1, args.warmup)):
+            h.partition_device(*t, k, part)
+        ms = []
+        cut = st = None
+        for _ in range(max(1, args.steps)):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cut, st = h.partition_device(*t, k, part)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        p = part.cpu().numpy()
+        W = int(g.vwgt.astype(np.int64).sum())
+        pw = np.bincount(p, weights=g.vwgt, minlength=k)
+        m = statistics.median(ms)
+        out.append({"config": name, "n": g.n, "edges": g.n_edges, "k": k, "ms": m, "edges_per_s": g.n_edges / (m / 1e3),
+                    "cut": int(cut), "balance": float(pw.max() * k / W), "levels": st["level_n"],
+                    "phase_ms": {"coarsen": st["ms_coarsen"], "init": st["ms_init"], "refine": st["ms_refine"]}})
+        print(json.dumps(out[-1]), flush=True)
+        h.close()
+        del t, part, flush
+        torch.cuda.empty_cache()
+    print(json.dumps({"workload": "configs", "metric": "edges/s partitioned, default mode", "steps": args.steps,
+                      "warmup": args.warmup, "results": out}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "configs"])
     ap.add_argument("--graphs", type=int, default=4096, help="batched: number of graphs")
     ap.add_argument("--slots", type=int, default=8, help="batched/served: concurrent partitions")
     ap.add_argument("--pool", type=int, default=48, help="served: distinct graphs requests draw from")
@@ -650,7 +709,9 @@ def main():
     ap.add_argument("--requests", type=int, default=400, help="served: most requests per load")
     ap.add_argument("--duration", type=float, default=4.0, help="served: seconds of arrivals per load")
     args = ap.parse_args()
-    if args.workload == "batched":
+    if args.workload == "configs":
+        bench_configs(args)
+    elif args.workload == "batched":
         bench_batched(args)
     elif args.workload == "served":
         bench_served(args)

@@ -104,6 +104,8 @@ void gkw_default_options(gkw_options* o) {
   o->seed = 1;
   o->init_trials = 8;
   o->enforce_balance = 1;
+  o->balance_levels = 3;
+  o->coarse_vertex_frac = 0.5;
 }
 
 float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps) {

@@ -817,6 +817,20 @@ CoopState read_coop(Handle& h) {
   return c;
 }
 
+// Heaviest coarse vertex (*out starts at 0).
+__global__ void k_max_cvw(const i32* __restrict__ ncp, const i32* __restrict__ cvw, i32* __restrict__ out) {
+  const i32 nc = *ncp;
+  i32 m = 0;
+  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x)
+    m = m > cvw[c] ? m : cvw[c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const i32 y = __shfl_xor_sync(kFull, m, o);
+    m = m > y ? m : y;
+  }
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+
 void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   Pool::Mark mk = h.scratch.mark();
   i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
@@ -833,6 +847,12 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   out.cadjwgt = h.hier.alloc_n<i32>(std::max<i64>(g.m, 1));
   run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
                &h.coop->mc);
+  GKW_CUDA(cudaMemsetAsync(&h.coop->max_cvw, 0, sizeof(i32), h.stream));
+  if (g.n > 0) {
+    const u32 gm = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)h.sm_count * 4));
+    launch(k_max_cvw, gm, 256, 0, h.stream, &h.coop->nc, out.cvwgt, &h.coop->max_cvw);
+    GKW_CHECK_LAUNCH();
+  }
   CoopState c = read_coop(h);
   if (c.arena_overflow) {   // very long coarse rows: grow the arena and redo the step
     ensure_arena(h, (u64)((double)(h.arena_words + (u64)c.arena_need) * 1.25) + 1024);
@@ -844,6 +864,7 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   out.nc = c.nc;
   out.mc = c.mc;
   out.uf_rounds = c.uf_rounds;
+  out.max_cvw = c.max_cvw;
 }
 
 }  // namespace gkw

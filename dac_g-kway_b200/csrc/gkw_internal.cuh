@@ -105,6 +105,7 @@ struct CoarsenOut {
   i32* cadjwgt = nullptr;
   i32* cvwgt = nullptr;
   i32 uf_rounds = 0;
+  i32 max_cvw = 0;   // heaviest coarse vertex
 };
 
 // Grid barrier word of a cooperative launch (see device_util.cuh); zero
@@ -125,6 +126,8 @@ struct CoopState {
   i32 scan_err;
   i32 arena_overflow;
   i64 arena_need;
+  i32 max_cvw;    // heaviest coarse vertex of the last coarsening step
+  i32 pad2;
 };
 
 // Bump arena for the hash tables of very long coarse rows (handle-owned,

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstring>
 #include <exception>
+#include <functional>
 #include <new>
 
 #include "gkw_internal.cuh"
@@ -85,6 +86,26 @@ i64 validate(Handle& h, const DevGraph& g) {
   return W;
 }
 
+// GKW_CHECK=1: validate every stage's output on the device before the next
+// stage reads it (coarse CSR, cmap range, part ids), so that a stage that
+// produced bad indices is reported by name instead of feeding them on.
+static bool stage_checks() {
+  static const bool on = [] {
+    const char* e = getenv("GKW_CHECK");
+    return e && *e == '1';
+  }();
+  return on;
+}
+
+static void check_stage(const char* what, i32 level, const std::function<void()>& f) {
+  try {
+    f();
+  } catch (const Error& e) {
+    throw Error{GKW_E_INTERNAL, std::string("stage check after ") + what + " (level " + std::to_string(level) +
+                                    "): " + e.msg};
+  }
+}
+
 void ensure_timer_events(Handle& h) {
   if (h.tev_ready) return;
   for (cudaEvent_t& e : h.tev) GKW_CUDA(cudaEventCreate(&e));
@@ -117,7 +138,24 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     CoarsenOut co;
     coarsen_level(h, lv.back().g, opt.group_cap, co);
     if (co.nc == lv.back().g.n || co.nc < k + 1) break;   // level discarded (:93-96)
+    // default mode: no coarse vertex may outweigh coarse_vertex_frac of a part
+    // (a whole component merged into one vertex cannot be balanced later)
+    if (opt.enforce_balance && opt.coarse_vertex_frac > 0 &&
+        (double)co.max_cvw > opt.coarse_vertex_frac * (double)W / (double)k)
+      break;
     lv.back().cmap = co.cmap;
+    if (stage_checks()) {
+      const i32 L = (i32)lv.size() - 1;
+      check_stage("grouping", L, [&] { check_parts(h, lv.back().g.n, co.cmap, co.nc); });
+      DevGraph cgc;
+      cgc.n = co.nc;
+      cgc.m = co.mc;
+      cgc.xadj = co.cxadj;
+      cgc.adjncy = co.cadjncy;
+      cgc.adjwgt = co.cadjwgt;
+      cgc.vwgt = co.cvwgt;
+      check_stage("contraction", L, [&] { validate(h, cgc); });
+    }
     Level nl;
     nl.g.n = co.nc;
     nl.g.m = co.mc;
@@ -156,13 +194,16 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   } else {
     device_init_partition(h, cg, k, opt.eps, opt.seed, std::max(1, std::min(8, opt.init_trials)), cpart);
   }
+  if (stage_checks()) check_stage("initial partition", (i32)lv.size() - 1, [&] { check_parts(h, cg.n, cpart, k); });
   refine_init_coarsest(h, rc, cg, cpart);
   i64* d_metrics = h.hier.alloc_n<i64>(k + 2);   // [0] cut, [1] bad-part flag, [2..k+2) part weights
   i64* d_init = h.hier.alloc_n<i64>(k + 2);      // the same for the initial partition
   if (stats)   // cut of the initial partition itself (before any balance move), read at the end
     compute_cut_pw(h, cg, refine_part(rc), k, d_init, d_init + 2);
   const i32 nl = (i32)lv.size();
-  if (opt.enforce_balance) {
+  // default mode: balance rounds at the balance_levels finest levels
+  auto balances = [&](i32 L) { return opt.enforce_balance && (opt.balance_levels <= 0 || L < opt.balance_levels); };
+  if (balances(nl - 1)) {
     LevelJob j;
     j.balance = true;
     j.bcap = maxw;
@@ -177,7 +218,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   for (i32 L = nl - 2; L >= 0; --L) {
     LevelJob j;
     j.cmap = lv[L].cmap;
-    j.balance = opt.enforce_balance != 0;
+    j.balance = balances(L);
     j.bcap = maxw;
     j.refine = true;
     j.maxw = maxw;
@@ -185,6 +226,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     j.ev_start = lev[2 * L];
     j.ev_end = lev[2 * L + 1];
     level_run(h, rc, lv[L].g, j, L);
+    if (stage_checks()) check_stage("refinement", L, [&] { check_parts(h, lv[L].g.n, refine_part(rc), k); });
   }
   GKW_CUDA(cudaEventRecord(ev[3], h.stream));
   // ---- output and final metrics (graph_partitioner.hpp:194-202) ----

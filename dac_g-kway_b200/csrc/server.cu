@@ -143,7 +143,8 @@ void gkw_server::run(Slot& s, Job& j) {
     j.n_levels = st.n_levels;
   } catch (const Error& e) {
     j.st = e.st;
-    j.err = e.msg;
+    j.err = e.msg + " (job: n=" + std::to_string(j.host.n) + ", nnz=" + std::to_string(j.host.m) +
+            ", k=" + std::to_string(j.k) + ")";
   } catch (const std::bad_alloc&) {
     j.st = GKW_E_NOMEM;
     j.err = "host allocation failed";

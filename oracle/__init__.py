@@ -36,6 +36,8 @@ class Opts(ctypes.Structure):
         ("init_fn", INIT_FN),
         ("init_user", ctypes.c_void_p),
         ("enforce_balance", ctypes.c_int32),
+        ("balance_levels", ctypes.c_int32),
+        ("coarse_vertex_frac", ctypes.c_double),
     ]
 
 
@@ -206,12 +208,13 @@ def refine(g, k, maxw, part, boundary, gain, target, updated, pw, move_cap=1024,
 
 
 def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_cap=1024, eps=0.03,
-              enforce_balance=False):
+              enforce_balance=False, balance_levels=3, coarse_vertex_frac=0.5):
     """Run the whole reference algorithm.
 
     ``init``: None -> the bundled METIS (the reference's initial partitioner);
     otherwise a callable ``init(coarse_csr_arrays..., k) -> part`` used for the
-    coarsest level.
+    coarsest level.  ``balance_levels`` and ``coarse_vertex_frac`` act in
+    default mode (``enforce_balance``) only, with the library's defaults.
     """
     opts = Opts()
     opts.group_cap = group_cap
@@ -219,6 +222,8 @@ def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_ca
     opts.move_cap = move_cap
     opts.eps = eps
     opts.enforce_balance = int(enforce_balance)
+    opts.balance_levels = int(balance_levels)
+    opts.coarse_vertex_frac = float(coarse_vertex_frac)
     keep = None
     if init is None:
         if not has_metis():

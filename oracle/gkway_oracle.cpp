@@ -524,6 +524,12 @@ typedef struct {
                  const i32* vwgt, i32 k, i32* part);
   void* init_user;
   i32 enforce_balance;   // 0 = the reference's behaviour; 1 = default mode (balance rounds, cap without +1)
+  // default mode only (partitioner.cu partition_impl): balance rounds at the
+  // balance_levels finest levels (<= 0: every level), and coarsening stops
+  // before a level whose heaviest vertex outweighs coarse_vertex_frac * W/k
+  // (<= 0: no such stop)
+  i32 balance_levels;
+  double coarse_vertex_frac;
 } orc_opts;
 
 typedef struct {
@@ -577,6 +583,11 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
     c.n = nc;
     c.vwgt.resize(nc);
     orc_coarse_vwgt(fn, f.vwgt.data(), f.cmap.data(), nc, c.vwgt.data());
+    if (opt->enforce_balance && opt->coarse_vertex_frac > 0) {
+      i64 mx = 0;
+      for (i32 v = 0; v < nc; ++v) mx = std::max<i64>(mx, (u32)c.vwgt[v]);
+      if ((double)mx > opt->coarse_vertex_frac * (double)total / (double)k) { f.cmap.clear(); break; }
+    }
     c.xadj.resize(nc + 1);
     std::vector<i32> ta(f.adjncy.size() + 1), tw(f.adjncy.size() + 1);
     i64 mc = orc_contract(fn, f.xadj.data(), f.adjncy.data(), f.adjwgt.data(), f.cmap.data(), nc,
@@ -620,7 +631,10 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
       if (part[cs.adjncy[e]] != part[v]) { boundary[v] = 1; break; }
   std::vector<u32> pw(k, 0);
   for (i32 v = 0; v < cs.n; ++v) pw[part[v]] += (u32)cs.vwgt[v];
-  if (opt->enforce_balance) {
+  auto balances = [&](i32 L) {
+    return opt->enforce_balance && (opt->balance_levels <= 0 || L < opt->balance_levels);
+  };
+  if (balances((i32)lv.size() - 1)) {
     RefineState s;
     s.n = cs.n; s.k = k;
     s.xadj = cs.xadj.data(); s.adjncy = cs.adjncy.data(); s.adjwgt = cs.adjwgt.data(); s.vwgt = cs.vwgt.data();
@@ -652,7 +666,7 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
     }
     s.pw = pw;
     update_all_flagged(s);                               // uncoarsen.hpp:385-386
-    if (opt->enforce_balance) {
+    if (balances(L)) {
       std::fill(s.updated.begin(), s.updated.end(), 0u);
       i64 bm = 0;
       res->balance_rounds[L] = balance_level(s, maxw, opt->move_cap, &bm);
