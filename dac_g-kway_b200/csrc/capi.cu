@@ -166,6 +166,7 @@ gkw_status gkw_destroy(gkw_handle* h) {
       for (cudaEvent_t e : h->h.tev) cudaEventDestroy(e);
     forget_coop_event(h->h);
     delete h;
+    cudaGetLastError();   // teardown is best effort: leave no error pending for later calls
   });
 }
 

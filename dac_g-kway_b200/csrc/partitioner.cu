@@ -106,6 +106,17 @@ static void check_stage(const char* what, i32 level, const std::function<void()>
   }
 }
 
+// Milliseconds between two recorded events; -1 (and no pending CUDA error
+// left behind) if either was never recorded.
+static double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float t = 0;
+  if (cudaEventElapsedTime(&t, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    return -1.0;
+  }
+  return t;
+}
+
 void ensure_timer_events(Handle& h) {
   if (h.tev_ready) return;
   for (cudaEvent_t& e : h.tev) GKW_CUDA(cudaEventCreate(&e));
@@ -260,10 +271,9 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
       stats->balance_rounds[i] = rs[i].brounds;
       stats->balance_moves[i] = rs[i].bmoves;
       stats->round_entries[i] = rs[i].rows;
-      const bool ran = (i + 1 < lv.size()) || opt.enforce_balance;
-      float t = 0;
-      if (ran) cudaEventElapsedTime(&t, lev[2 * i], lev[2 * i + 1]);
-      stats->ms_level[i] = ran ? t : -1.0;
+      // the coarsest level has a launch only when it runs balance rounds
+      const bool ran = (i + 1 < lv.size()) || balances(nl - 1);
+      stats->ms_level[i] = ran ? elapsed_ms(lev[2 * i], lev[2 * i + 1]) : -1.0;
     }
     stats->init_cut = init_cut;
     stats->cut = hm[0];
@@ -271,15 +281,10 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     for (i32 p = 0; p < k; ++p) mx = std::max(mx, hm[2 + p]);
     stats->max_part_weight = mx;
     stats->maxw = maxw;
-    float a = 0, b = 0, c = 0, d = 0;
-    cudaEventElapsedTime(&a, ev[0], ev[1]);
-    cudaEventElapsedTime(&b, ev[1], ev[2]);
-    cudaEventElapsedTime(&c, ev[2], ev[3]);
-    cudaEventElapsedTime(&d, ev[0], ev[4]);
-    stats->ms_coarsen = a;
-    stats->ms_init = b;
-    stats->ms_refine = c;
-    stats->ms_total = d;
+    stats->ms_coarsen = elapsed_ms(ev[0], ev[1]);
+    stats->ms_init = elapsed_ms(ev[1], ev[2]);
+    stats->ms_refine = elapsed_ms(ev[2], ev[3]);
+    stats->ms_total = elapsed_ms(ev[0], ev[4]);
   }
 }
 
