@@ -70,7 +70,7 @@ class Options(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("init_trials", ctypes.c_int32),
         ("enforce_balance", ctypes.c_int32),
-        ("balance_levels", ctypes.c_int32),
+        ("balance_skip_levels", ctypes.c_int32),
         ("reserved1", ctypes.c_int32),
         ("coarse_vertex_frac", ctypes.c_double),
         ("reserved", ctypes.c_int32 * 2),

@@ -104,7 +104,7 @@ void gkw_default_options(gkw_options* o) {
   o->seed = 1;
   o->init_trials = 8;
   o->enforce_balance = 1;
-  o->balance_levels = 3;
+  o->balance_skip_levels = 1;
   o->coarse_vertex_frac = 0.5;
 }
 

@@ -91,10 +91,20 @@ struct TrialState {
   i32* posF;   // position in F
 };
 
+// Refinement moves of one trial: s/4 + 32, at most 256 (each move scans the
+// whole sub-problem).
+__host__ __device__ __forceinline__ i32 gggp_max_moves(i32 s) { return s / 4 + 32 < 256 ? s / 4 + 32 : 256; }
+
+// Sub-problems above this size get their members sorted by (degS, index) once:
+// while the frontier is empty every unassigned member has conn = 0, so the
+// growth key's best is the first unassigned member in that order, and the
+// step walks a pointer instead of scanning all members.
+constexpr i32 kGggpOrderMin = 2048;
+
 // One GGGP trial by one warp (growth then positive-gain refinement); see the
 // file comment for the rules.  Returns the trial's cut and |W(R) - TL|.
 __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL, i64 WS, i64 capL,
-                           i64 capR, i64& cut_out, i64& dev_out) {
+                           i64 capR, const i32* order, i64& cut_out, i64& dev_out) {
   const int lane = threadIdx.x & 31;
   i32* C = S.C;
   i32* R = S.R;
@@ -107,6 +117,7 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
   __syncwarp();
   i64 wR = 0;
   i32 nF = 0;
+  i32 nxt = 0;   // pointer into order (empty-frontier steps)
   // ---- growth: F = members outside R with conn > 0; a frontier member
   // always outranks a non-frontier one, so the argmax over F equals the argmax
   // over all unassigned members, and the full scan is only needed when F is
@@ -121,6 +132,11 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
           const u64 key = grow_key(true, 2 * c - T.degS[i], i);
           best = best > key ? best : key;
         }
+      } else if (order) {
+        // empty frontier: the first unassigned member in (degS, index) order
+        // (assigned members never return, so the pointer only moves forward)
+        while (nxt < s && R[order[nxt]]) ++nxt;
+        if (nxt < s) best = grow_key(false, -T.degS[order[nxt]], order[nxt]);
       } else {
         for (i32 i = lane; i < s; i += 32) {
           if (!R[i]) {
@@ -173,7 +189,7 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
     if (wR >= TL) break;
   }
   // ---- refinement: positive-gain moves within the side caps ----
-  const i32 max_moves = s / 4 + 32;
+  const i32 max_moves = gggp_max_moves(s);
   for (i32 mv = 0; mv < max_moves; ++mv) {
     u64 best = 0;
     for (i32 i = lane; i < s; i += 32) {
@@ -249,7 +265,8 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     const i32* __restrict__ vwgt, const i32* __restrict__ lo, const i32* __restrict__ hi,
     const i32* __restrict__ cnt, const i32* __restrict__ off, i32* __restrict__ mlist, i32* __restrict__ loc,
     i32* __restrict__ lo_out, i32* __restrict__ hi_out, u64 seed, double eps, i32 trials,
-    i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state) {
+    i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state, i32* g_order,
+    u64* g_okeys) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_cnt;
   __shared__ i32 s_warp[33];
@@ -380,6 +397,32 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   T.nw = nw;
   T.degS = deg;
   T.vw = vw;
+  // large sub-problems: members in (degS, index) order for empty-frontier steps
+  const i32* order = nullptr;
+  if (s > kGggpOrderMin) {   // block-uniform
+    i64 P = 1;
+    while (P < s) P <<= 1;
+    u64* a = g_okeys + 2 * (i64)base_off;   // P <= 2s keys; sub-problems' ranges are disjoint
+    for (i64 i = threadIdx.x; i < P; i += blockDim.x)
+      a[i] = i < s ? (((u64)(u32)deg[i] << 32) | (u32)i) : ~0ull;
+    __syncthreads();
+    for (i64 kk = 2; kk <= P; kk <<= 1)
+      for (i64 j = kk >> 1; j > 0; j >>= 1) {
+        for (i64 i = threadIdx.x; i < P; i += blockDim.x) {
+          const i64 l = i ^ j;
+          if (l > i) {
+            const u64 x = a[i], y = a[l];
+            const bool up = (i & kk) == 0;
+            if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
+          }
+        }
+        __syncthreads();
+      }
+    i32* o = g_order + base_off;
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) o[i] = (i32)(u32)a[i];
+    __syncthreads();
+    order = o;
+  }
   const i32 t = wid;
   if (t < trials) {
     TrialState S;
@@ -398,7 +441,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     }
     const i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0 * 1315423911ull + (u64)t) % (u32)s);
     i64 cut, dev;
-    gggp_trial(T, S, s, pick, TL, WS, capL, capR, cut, dev);
+    gggp_trial(T, S, s, pick, TL, WS, capL, capR, order, cut, dev);
     if (lane == 0) {
       s_cut[t] = cut;
       s_dev[t] = dev;
@@ -444,6 +487,8 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   i32* g_nb = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
   i32* g_nw = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
   i32* g_state = h.scratch.alloc_n<i32>((size_t)kInitTrials * 4 * n);
+  i32* g_order = h.scratch.alloc_n<i32>(n);
+  u64* g_okeys = h.scratch.alloc_n<u64>(2 * (size_t)n);
   GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
   const u32 nb = ceil_div(n, 256);
   launch(k_init_fill, nb, 256, 0, h.stream, n, lo[0], hi[0], k);
@@ -465,7 +510,7 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     exclusive_scan_i32(h, cnt, off, k, nullptr);
     launch(k_gggp_depth, k, kInitTrials * 32, kGggpSmem, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a],
            hi[a], cnt, off, mlist, loc, lo[b], hi[b], seed, eps, trials, g_rb, g_rn, g_deg, g_vw, g_nb, g_nw,
-           g_state);
+           g_state, g_order, g_okeys);
     GKW_CHECK_LAUNCH();
     if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));
   }

@@ -212,8 +212,11 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   if (stats)   // cut of the initial partition itself (before any balance move), read at the end
     compute_cut_pw(h, cg, refine_part(rc), k, d_init, d_init + 2);
   const i32 nl = (i32)lv.size();
-  // default mode: balance rounds at the balance_levels finest levels
-  auto balances = [&](i32 L) { return opt.enforce_balance && (opt.balance_levels <= 0 || L < opt.balance_levels); };
+  // default mode: balance rounds at every level but the balance_skip_levels
+  // coarsest ones (the finest level always)
+  auto balances = [&](i32 L) {
+    return opt.enforce_balance && (L == 0 || L < nl - std::max(0, opt.balance_skip_levels));
+  };
   if (balances(nl - 1)) {
     LevelJob j;
     j.balance = true;

@@ -74,8 +74,8 @@ typedef struct gkw_options {
   int32_t enforce_balance;  /* 1 (default): every part <= (1+eps)W/k, balance rounds at each
                                level; 0: the reference's behaviour (MAX_PARTITION_WGT =
                                (1+eps)W/k + 1 checked on move destinations only) */
-  int32_t balance_levels;   /* default mode: balance rounds at this many finest levels (3; <= 0:
-                               every level); coarser levels are refined without them */
+  int32_t balance_skip_levels; /* default mode: the coarsest levels refined without balance rounds
+                                 (1; 0: every level balanced); the finest level always is */
   int32_t reserved1;
   double coarse_vertex_frac; /* default mode: coarsening stops before a level whose heaviest vertex
                                outweighs this fraction of W/k (0.5; <= 0: no such stop) */

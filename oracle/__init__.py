@@ -36,7 +36,7 @@ class Opts(ctypes.Structure):
         ("init_fn", INIT_FN),
         ("init_user", ctypes.c_void_p),
         ("enforce_balance", ctypes.c_int32),
-        ("balance_levels", ctypes.c_int32),
+        ("balance_skip_levels", ctypes.c_int32),
         ("coarse_vertex_frac", ctypes.c_double),
     ]
 
@@ -208,12 +208,12 @@ def refine(g, k, maxw, part, boundary, gain, target, updated, pw, move_cap=1024,
 
 
 def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_cap=1024, eps=0.03,
-              enforce_balance=False, balance_levels=3, coarse_vertex_frac=0.5):
+              enforce_balance=False, balance_skip_levels=1, coarse_vertex_frac=0.5):
     """Run the whole reference algorithm.
 
     ``init``: None -> the bundled METIS (the reference's initial partitioner);
     otherwise a callable ``init(coarse_csr_arrays..., k) -> part`` used for the
-    coarsest level.  ``balance_levels`` and ``coarse_vertex_frac`` act in
+    coarsest level.  ``balance_skip_levels`` and ``coarse_vertex_frac`` act in
     default mode (``enforce_balance``) only, with the library's defaults.
     """
     opts = Opts()
@@ -222,7 +222,7 @@ def partition(g, k: int, *, init=None, group_cap=6, threshold_factor=20, move_ca
     opts.move_cap = move_cap
     opts.eps = eps
     opts.enforce_balance = int(enforce_balance)
-    opts.balance_levels = int(balance_levels)
+    opts.balance_skip_levels = int(balance_skip_levels)
     opts.coarse_vertex_frac = float(coarse_vertex_frac)
     keep = None
     if init is None:

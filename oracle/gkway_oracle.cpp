@@ -524,11 +524,12 @@ typedef struct {
                  const i32* vwgt, i32 k, i32* part);
   void* init_user;
   i32 enforce_balance;   // 0 = the reference's behaviour; 1 = default mode (balance rounds, cap without +1)
-  // default mode only (partitioner.cu partition_impl): balance rounds at the
-  // balance_levels finest levels (<= 0: every level), and coarsening stops
+  // default mode only (partitioner.cu partition_impl): balance rounds at every
+  // level but the balance_skip_levels coarsest ones (the finest level always),
+  // and coarsening stops
   // before a level whose heaviest vertex outweighs coarse_vertex_frac * W/k
   // (<= 0: no such stop)
-  i32 balance_levels;
+  i32 balance_skip_levels;
   double coarse_vertex_frac;
 } orc_opts;
 
@@ -631,8 +632,9 @@ int orc_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, 
       if (part[cs.adjncy[e]] != part[v]) { boundary[v] = 1; break; }
   std::vector<u32> pw(k, 0);
   for (i32 v = 0; v < cs.n; ++v) pw[part[v]] += (u32)cs.vwgt[v];
+  const i32 nlv = (i32)lv.size();
   auto balances = [&](i32 L) {
-    return opt->enforce_balance && (opt->balance_levels <= 0 || L < opt->balance_levels);
+    return opt->enforce_balance && (L == 0 || L < nlv - std::max(0, opt->balance_skip_levels));
   };
   if (balances((i32)lv.size() - 1)) {
     RefineState s;
@@ -813,7 +815,7 @@ void orc_init_partition(i32 n, const i32* xadj, const i32* adjncy, const i32* ad
             if (lo[adjncy[e]] == p0) C[adjncy[e]] += adjwgt[e];
           if (wR >= TL) break;
         }
-        const i32 max_moves = s / 4 + 32;
+        const i32 max_moves = std::min(s / 4 + 32, 256);   // initpart.cu gggp_max_moves
         for (i32 mv = 0; mv < max_moves; ++mv) {
           u64 best = 0;
           for (i32 i = 0; i < s; ++i) {
