@@ -705,9 +705,9 @@ def main():
     ap.add_argument("--slots", type=int, default=8, help="batched/served: concurrent partitions")
     ap.add_argument("--pool", type=int, default=48, help="served: distinct graphs requests draw from")
     ap.add_argument("--max-n", type=int, default=2000000, help="served: largest graph")
-    ap.add_argument("--rates", default="10,50,200,500,1000,2000", help="served: offered loads (requests/s)")
-    ap.add_argument("--requests", type=int, default=400, help="served: most requests per load")
-    ap.add_argument("--duration", type=float, default=4.0, help="served: seconds of arrivals per load")
+    ap.add_argument("--rates", default="10,100,500,2000", help="served: offered loads (requests/s)")
+    ap.add_argument("--requests", type=int, default=200, help="served: most requests per load")
+    ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals per load")
     args = ap.parse_args()
     if args.workload == "configs":
         bench_configs(args)

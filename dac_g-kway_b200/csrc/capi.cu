@@ -140,8 +140,11 @@ gkw_status gkw_create(gkw_handle** out, int32_t device) {
     int optin = 0;
     GKW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     h->h.smem_optin = optin;
+    // the handle's stream does not wait for the legacy default stream: every
+    // initialisation goes on that stream and completes before the handle is used
     e = cudaMalloc(&h->h.coop, sizeof(CoopState));
-    if (e == cudaSuccess) e = cudaMemset(h->h.coop, 0, sizeof(CoopState));
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->h.coop, 0, sizeof(CoopState), h->h.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->h.stream);
     if (e != cudaSuccess) {
       cudaFreeHost(h->h.h_pinned);
       cudaStreamDestroy(h->h.stream);
@@ -262,14 +265,16 @@ gkw_status gkw_contract(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_
     i32 cap = 1;
     {
       std::vector<i32> hc(g.n);
-      if (g.n) GKW_CUDA(cudaMemcpy(hc.data(), d_cmap, sizeof(i32) * g.n, cudaMemcpyDeviceToHost));
+      if (g.n) GKW_CUDA(cudaMemcpyAsync(hc.data(), d_cmap, sizeof(i32) * g.n, cudaMemcpyDeviceToHost, hh.stream));
+      GKW_CUDA(cudaStreamSynchronize(hh.stream));
       std::vector<i32> cnt(std::max(nc, 1), 0);
       for (i32 v = 0; v < g.n; ++v) {
         GKW_REQUIRE(hc[v] >= 0 && hc[v] < nc, GKW_E_INVALID, "cmap entry out of range");
         cap = std::max(cap, ++cnt[hc[v]]);
       }
     }
-    GKW_CUDA(cudaMemcpy(&hh.coop->nc, &nc, sizeof(i32), cudaMemcpyHostToDevice));
+    GKW_CUDA(cudaMemcpyAsync(&hh.coop->nc, &nc, sizeof(i32), cudaMemcpyHostToDevice, hh.stream));
+    GKW_CUDA(cudaStreamSynchronize(hh.stream));
     run_contract(hh, g, d_cmap, &hh.coop->nc, nc, cap, d_cxadj, d_cadjncy, d_cadjwgt, d_cvwgt, &hh.coop->mc);
     CoopState c = read_coop(hh);
     if (c.arena_overflow) {

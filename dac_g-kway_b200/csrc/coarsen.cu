@@ -729,7 +729,8 @@ void ensure_arena(Handle& h, u64 words) {
   h.arena = nullptr;
   h.arena_words = 0;
   GKW_CUDA(cudaMalloc(&h.arena, sizeof(ArenaHdr) + sizeof(u32) * words));
-  GKW_CUDA(cudaMemset(h.arena, 0, sizeof(ArenaHdr)));
+  // on the handle's stream: that stream does not wait for the legacy stream
+  GKW_CUDA(cudaMemsetAsync(h.arena, 0, sizeof(ArenaHdr), h.stream));
   h.arena_words = words;
 }
 

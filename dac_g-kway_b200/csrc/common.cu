@@ -249,11 +249,15 @@ void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total) {
   GKW_REQUIRE(nt64 < (i64)1 << 30, GKW_E_UNSUPPORTED, "scan too large");
   const i32 nt = (i32)nt64;
   if (h.scan_tiles_cap < nt) {
+    // queued scans may still use the old state; the new state is cleared on
+    // the handle's stream (which does not wait for the legacy stream), so the
+    // scan below sees it cleared
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
     if (h.scan) GKW_CUDA(cudaFree(h.scan));
     h.scan = nullptr;
     const i32 cap = std::max(nt, 1024);
     GKW_CUDA(cudaMalloc(&h.scan, sizeof(ScanState) + sizeof(u64) * (size_t)cap));
-    GKW_CUDA(cudaMemset(h.scan, 0, sizeof(ScanState) + sizeof(u64) * (size_t)cap));
+    GKW_CUDA(cudaMemsetAsync(h.scan, 0, sizeof(ScanState) + sizeof(u64) * (size_t)cap, h.stream));
     h.scan_tiles_cap = cap;
     h.scan_tickets = 0;
     h.scan_epoch = 0;

@@ -1249,8 +1249,9 @@ std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots) {
   if (c->trace && nslots) {
     std::vector<i32> tn(nslots);
     std::vector<u64> tr((size_t)nslots * kTraceCap);
-    GKW_CUDA(cudaMemcpy(tn.data(), c->trace_n, sizeof(i32) * nslots, cudaMemcpyDeviceToHost));
-    GKW_CUDA(cudaMemcpy(tr.data(), c->trace, sizeof(u64) * tr.size(), cudaMemcpyDeviceToHost));
+    GKW_CUDA(cudaMemcpyAsync(tn.data(), c->trace_n, sizeof(i32) * nslots, cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaMemcpyAsync(tr.data(), c->trace, sizeof(u64) * tr.size(), cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
     for (i32 s = 0; s < nslots; ++s) {
       if (tn[s] < 2) continue;
       double acc[32] = {0};
@@ -1267,7 +1268,7 @@ std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots) {
         if (cnt[p]) fprintf(stderr, " ph%d x%d %.2fus", p, cnt[p], acc[p] / cnt[p] / 1e3);
       fprintf(stderr, "\n");
     }
-    GKW_CUDA(cudaMemset(c->trace_n, 0, sizeof(i32) * kStatSlots));
+    GKW_CUDA(cudaMemsetAsync(c->trace_n, 0, sizeof(i32) * kStatSlots, h.stream));
   }
   std::vector<RefineLevelStats> out((size_t)nslots);
   for (i32 i = 0; i < nslots; ++i) {
