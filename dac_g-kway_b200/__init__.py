@@ -124,7 +124,8 @@ class ServerConfig(ctypes.Structure):
         ("pool_bytes", ctypes.c_int64),
         ("slot_keep_bytes", ctypes.c_int64),
         ("max_bypass", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("batch_union", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 

@@ -229,7 +229,9 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc
 void ensure_arena(Handle& h, u64 words);
 // Reads the CoopState (one host sync) and throws on a recorded error.
 CoopState read_coop(Handle& h);
-void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out);
+// gid/gfrozen (batched levels): graphs with gfrozen[g] != 0 are copied unchanged
+void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out, const i32* gid = nullptr,
+                   const i32* gfrozen = nullptr);
 
 // ---- refinement (refine.cu) ----
 struct RefineCtx;   // opaque
@@ -257,8 +259,26 @@ struct LevelJob {
   i32 move_cap = 1024;
   cudaEvent_t ev_start = nullptr;   // optional: recorded right before / after the launch
   cudaEvent_t ev_end = nullptr;
+  const struct BatchLevel* batch = nullptr;   // a batched level (batch.cu), or null
 };
-RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap);
+// Per-level tables of a batched level: the disjoint union of G graphs with
+// global part ids (graph g owns parts [gpbase[g], gpbase[g] + gk[g])).
+struct BatchLevel {
+  i32 G = 0;
+  const i32* gid = nullptr;      // [n] graph of each vertex
+  const i32* gvbase = nullptr;   // [G + 1] vertex offsets at this level
+  const i32* gpbase = nullptr;   // [G]
+  const i32* gk = nullptr;       // [G]
+  const i32* gflags = nullptr;   // [G] bit 0 refine, bit 1 balance rounds at this level
+  const float* pmaxw = nullptr;  // [parts]
+  const float* pbcap = nullptr;  // [parts]
+  i32* gcc = nullptr;            // [G] zeroed
+  i32* glight = nullptr;         // [G]
+  i32* mcount = nullptr;         // [1] zeroed
+  i32* anyf = nullptr;           // [3] zeroed
+};
+// kacc: part-row length of the gain updates (largest k of a batch; 0 = k)
+RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap, i32 kacc = 0);
 RefineCtx* refine_create_ext(Handle& h, i32 n, i32 k, i32 move_cap, i32* part, i32* bnd, i32* gain,
                              i32* target);
 void refine_destroy(RefineCtx* c);
@@ -286,8 +306,20 @@ void launch_cut_pw(cudaStream_t stream, i32 sm_count, const DevGraph& g, const i
 void check_parts(Handle& h, i32 n, const i32* part, i32 k);
 
 // ---- initial partition (initpart.cu) ----
+// Batched initial partition: the disjoint union of graphs, global part ids;
+// every vertex starts in [gpbase[g], gpbase[g] + gk[g]) of its graph, and the
+// seeds name parts by part - part_base[part] as a lone run would.
+struct GggpBatch {
+  const i32* gid = nullptr;
+  const i32* gpbase = nullptr;
+  const i32* gk = nullptr;
+  const i32* part_base = nullptr;   // [parts] first part of the part's graph
+  const i32* part_v0 = nullptr;     // [parts] vertex range of the part's graph
+  const i32* part_v1 = nullptr;
+  i32 depth = 0;                    // recursion depth of the largest k
+};
 void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 seed, i32 trials,
-                           i32* d_part);
+                           i32* d_part, const GggpBatch* batch = nullptr);
 
 // ---- driver (partitioner.cu) ----
 i64 validate(Handle& h, const DevGraph& g);   // total vertex weight; throws on malformed input
@@ -298,6 +330,12 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
 void partition_host(Handle& h, const DevGraph& host_graph, i64 vbase, i32 k, const gkw_options& opt,
                     i32* part_out, i64* cut_out, gkw_stats* stats);
 Handle& handle_of(gkw_handle* h);   // the handle behind a C-ABI handle (capi.cu)
+// Many independent graphs partitioned as one disjoint union (batch.cu): host
+// arrays with global ids, graph g = vertices [graph_ptr[g], graph_ptr[g+1]).
+// part_out gets each graph's own part ids.  Returns false, having computed
+// nothing, if an edge joins two graphs.
+bool partition_batch_union(Handle& h, const DevGraph& host_union, i32 G, const i32* graph_ptr, const i32* ks,
+                           const gkw_options& opt, i32* part_out, i64* cuts_out);
 const char* last_error_cstr();
 
 // ---- host helpers ----

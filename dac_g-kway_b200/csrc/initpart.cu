@@ -266,7 +266,8 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     const i32* __restrict__ cnt, const i32* __restrict__ off, i32* __restrict__ mlist, i32* __restrict__ loc,
     i32* __restrict__ lo_out, i32* __restrict__ hi_out, u64 seed, double eps, i32 trials,
     i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state, i32* g_order,
-    u64* g_okeys) {
+    u64* g_okeys, const i32* __restrict__ part_base, const i32* __restrict__ part_v0,
+    const i32* __restrict__ part_v1) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_cnt;
   __shared__ i32 s_warp[33];
@@ -281,11 +282,13 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   const i32 base_off = off[p0];
   i32* M = mlist + base_off;
   // deterministic member list: all vertices with lo == p0, in id order
+  // (batched levels: only the part's own graph holds them)
+  const i32 v_lo = part_v0 ? part_v0[p0] : 0, v_hi = part_v1 ? part_v1[p0] : n;
   if (threadIdx.x == 0) s_cnt = 0;
   __syncthreads();
-  for (i32 base = 0; base < n; base += blockDim.x) {
+  for (i32 base = v_lo; base < v_hi; base += blockDim.x) {
     const i32 v = base + threadIdx.x;
-    const bool mine = v < n && lo[v] == p0;
+    const bool mine = v < v_hi && lo[v] == p0;
     const u32 bal = __ballot_sync(kFull32, mine);
     if (lane == 0) s_warp[wid] = __popc(bal);
     __syncthreads();
@@ -439,7 +442,9 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
       S.F = q + 2 * (size_t)n + base_off;
       S.posF = q + 3 * (size_t)n + base_off;
     }
-    const i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0 * 1315423911ull + (u64)t) % (u32)s);
+    // the seed names the part by its own graph's id (batched levels: parts are global)
+    const i32 p0_local = part_base ? p0 - part_base[p0] : p0;
+    const i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0_local * 1315423911ull + (u64)t) % (u32)s);
     i64 cut, dev;
     gggp_trial(T, S, s, pick, TL, WS, capL, capR, order, cut, dev);
     if (lane == 0) {
@@ -468,8 +473,18 @@ __global__ void k_init_fill(i32 n, i32* lo, i32* hi, i32 k) {
   if (v < n) { lo[v] = 0; hi[v] = k; }
 }
 
+__global__ void k_init_fill_batch(i32 n, const i32* __restrict__ gid, const i32* __restrict__ gpbase,
+                                  const i32* __restrict__ gk, i32* lo, i32* hi) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) {
+    const i32 g = gid[v];
+    lo[v] = gpbase[g];
+    hi[v] = gpbase[g] + gk[g];
+  }
+}
+
 void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 seed, i32 trials,
-                           i32* d_part) {
+                           i32* d_part, const GggpBatch* batch) {
   GKW_REQUIRE(trials >= 1 && trials <= kInitTrials, GKW_E_INVALID, "init trials must be in [1, 8]");
   const i32 n = g.n;
   if (n == 0) return;
@@ -491,10 +506,15 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   u64* g_okeys = h.scratch.alloc_n<u64>(2 * (size_t)n);
   GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
   const u32 nb = ceil_div(n, 256);
-  launch(k_init_fill, nb, 256, 0, h.stream, n, lo[0], hi[0], k);
-  GKW_CHECK_LAUNCH();
   i32 depth = 0;
-  while ((1 << depth) < k) ++depth;
+  if (batch) {
+    launch(k_init_fill_batch, nb, 256, 0, h.stream, n, batch->gid, batch->gpbase, batch->gk, lo[0], hi[0]);
+    depth = batch->depth;
+  } else {
+    launch(k_init_fill, nb, 256, 0, h.stream, n, lo[0], hi[0], k);
+    while ((1 << depth) < k) ++depth;
+  }
+  GKW_CHECK_LAUNCH();
   const bool trace = getenv("GKW_TRACE") && *getenv("GKW_TRACE") == '1';
   std::vector<cudaEvent_t> ev;
   if (trace) {
@@ -510,7 +530,8 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     exclusive_scan_i32(h, cnt, off, k, nullptr);
     launch(k_gggp_depth, k, kInitTrials * 32, kGggpSmem, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a],
            hi[a], cnt, off, mlist, loc, lo[b], hi[b], seed, eps, trials, g_rb, g_rn, g_deg, g_vw, g_nb, g_nw,
-           g_state, g_order, g_okeys);
+           g_state, g_order, g_okeys, batch ? batch->part_base : (const i32*)nullptr,
+           batch ? batch->part_v0 : (const i32*)nullptr, batch ? batch->part_v1 : (const i32*)nullptr);
     GKW_CHECK_LAUNCH();
     if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));
   }

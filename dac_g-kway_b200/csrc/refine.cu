@@ -66,6 +66,7 @@ struct LevelStatsDev {
 
 struct RefineCtx {
   i32 n_max = 0, k = 0, cap = 0;
+  i32 kacc = 0;   // part-row length of the gain updates (k, or the largest k of a batch)
   i32* part[2] = {nullptr, nullptr};
   i32* bnd[2] = {nullptr, nullptr};
   i32 cur = 0;
@@ -124,6 +125,26 @@ struct LevelArgs {
   u64* trace;        // optional phase timeline: (phase id << 56) | globaltimer ns
   i32 trace_cap;
   i32* trace_n;
+  // A batched level is the disjoint union of G independent graphs (batch.cu).
+  // Part ids are global (graph g owns [gpbase[g], gpbase[g] + gk[g])), caps
+  // are per part, and everything a round decides per graph -- the candidate
+  // order, the move cap, the balanced prefix, the lightest part, the end of
+  // the rounds -- is decided per graph, so each graph moves exactly as it
+  // would alone.
+  i32 batch;
+  i32 G;
+  i32 kacc;             // length of the per-warp part rows (largest k of a graph)
+  const i32* gid;       // graph of each vertex
+  const i32* gvbase;    // [G + 1] vertex offsets of the graphs at this level
+  const i32* gpbase;    // [G] first part of each graph
+  const i32* gk;        // [G] parts of each graph
+  const i32* gflags;    // [G] bit 0: refinement rounds at this level, bit 1: balance rounds
+  const float* pmaxw;   // [parts] MAXW of each part
+  const float* pbcap;   // [parts] balance cap of each part
+  i32* gcc;             // [G] candidate counts; graph g's candidates at cands[gvbase[g]..]
+  i32* glight;          // [G] lightest part of each graph (balance rounds)
+  i32* mcount;          // moves in the flat move list top[]
+  i32* anyf;            // [3] rotating flags: some graph had candidates / an overweight part
 };
 
 enum : i32 { LF_PROJECT = 1, LF_LISTS = 2, LF_UPDATE = 4, LF_BALANCE = 8, LF_REFINE = 16 };
@@ -143,6 +164,20 @@ __device__ __forceinline__ bool valid_move(u32 dest_w, u32 vw, float maxw) {
   return !(__uint2float_rn(dest_w + vw) > maxw);
 }
 __device__ __forceinline__ bool over_cap(u32 w, float cap) { return __uint2float_rn(w) > cap; }
+
+// per-graph values of a batched level (plain levels: one graph, part base 0)
+__device__ __forceinline__ i32 part_base_of(const LevelArgs& a, i32 v) {
+  return a.batch ? __ldg(a.gpbase + __ldg(a.gid + v)) : 0;
+}
+__device__ __forceinline__ float maxw_of(const LevelArgs& a, i32 part) {
+  return a.batch ? __ldg(a.pmaxw + part) : a.maxw;
+}
+__device__ __forceinline__ float bcap_of(const LevelArgs& a, i32 part) {
+  return a.batch ? __ldg(a.pbcap + part) : a.bcap;
+}
+__device__ __forceinline__ bool graph_flag(const LevelArgs& a, i32 v, i32 bit) {
+  return !a.batch || ((__ldg(a.gflags + __ldg(a.gid + v)) >> bit) & 1);
+}
 
 // candidate key: ascending order = gain descending, vertex id ascending
 // (INT_MAX - gain fits in 32 bits for every int32 gain)
@@ -227,8 +262,8 @@ __device__ void ph_project(const LevelArgs& a) {
       a.gain[v] = 0;
       a.target[v] = p;
       a.inP[v] = 0;
-      a.updflag[v] = bc ? 1 : 0;
-      b = bc != 0;
+      b = bc != 0 && (!a.batch || __ldg(a.gflags + __ldg(a.gid + v)) != 0);
+      a.updflag[v] = b ? 1 : 0;
     }
     warp_append(b, (i32)v, a.U, &a.st->ucount);
   }
@@ -264,7 +299,7 @@ __device__ void ph_lists(const LevelArgs& a) {
 __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid >= a.acc_warps) return;
-  u32* acc = acc_all + (size_t)wid * a.k;
+  u32* acc = acc_all + (size_t)wid * a.kacc;
   RoundState* st = a.st;
   const i32 nU = ldc(&st->ucount);
   i32* Pout = a.P0;          // P is never compacted within a level: entries whose
@@ -274,24 +309,26 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
   for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nU; i += nw) {
     const i32 v = ldc(a.U + i);
     const i32 p = ldc(a.part + v);
+    const i32 pb = part_base_of(a, v);   // rows are indexed by the graph's own part ids
+    u32* accb = acc - pb;
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
     rows += (unsigned long long)(end - beg);
     bool bl = false;
     for (i32 e = beg + lane; e < end; e += 32) {
       const i32 q = ldc(a.part + a.adjncy[e]);
-      atomicAdd(&acc[q], (u32)a.adjwgt[e]);
+      atomicAdd(&accb[q], (u32)a.adjwgt[e]);
       bl |= (q != p);
     }
     const bool b = __any_sync(kFullMask, bl);
     __syncwarp();
     u32 g = 0, q_best = (u32)p;
     if (b) {
-      const u32 id = acc[p];
+      const u32 id = accb[p];
       u64 best = 0;
       for (i32 e = beg + lane; e < end; e += 32) {
         const i32 q = ldc(a.part + a.adjncy[e]);
         if (q != p) {
-          const u64 key = ((u64)(acc[q] - id) << 32) | (u32)(~(u32)q);
+          const u64 key = ((u64)(accb[q] - id) << 32) | (u32)(~(u32)q);
           best = best > key ? best : key;
         }
       }
@@ -311,7 +348,7 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
       if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) Pout[atomicAdd(pcount, 1)] = v;
     }
     __syncwarp();
-    for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
+    for (i32 e = beg + lane; e < end; e += 32) accb[ldc(a.part + a.adjncy[e])] = 0;
     __syncwarp();
   }
   if (count && lane == 0 && rows) atomicAdd(reinterpret_cast<unsigned long long*>(&st->rows), rows);
@@ -322,6 +359,7 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
 // smaller id that is itself positive and valid.  P is compacted on the way.
 __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
   RoundState* st = a.st;
+  if (a.batch && blockIdx.x == 0 && threadIdx.x == 0) *a.mcount = 0;   // the round's moves
   const int lane = threadIdx.x & 31;
   const i32 nP = ldc(&st->pcount[0]);
   // entry r*32*W + lane*W + w goes to warp w, lane `lane`: the entries of a
@@ -335,8 +373,10 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
     if (i < nP) {
       v = ldc(a.P0 + i);
       g = ldc(a.gain + v);
-      if (g > 0 && ldc(a.bnd + v))
-        check = valid_move(ldc(a.pw + ldc(a.target + v)), (u32)a.vwgt[v], a.maxw);
+      if (g > 0 && ldc(a.bnd + v)) {
+        const i32 t = ldc(a.target + v);
+        check = valid_move(ldc(a.pw + t), (u32)a.vwgt[v], maxw_of(a, t));
+      }
     }
     // independent-set test, one candidate at a time, neighbours across lanes
     u32 pend = __ballot_sync(kFullMask, check);
@@ -349,13 +389,22 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
       bool blocked = false;
       for (i32 e = beg + lane; e < end && !blocked; e += 32) {
         const i32 u = a.adjncy[e];
-        blocked = u < cv && ldc(a.gain + u) > 0 &&
-                  valid_move(ldc(a.pw + ldc(a.target + u)), (u32)a.vwgt[u], a.maxw);
+        if (u < cv && ldc(a.gain + u) > 0) {
+          const i32 tu = ldc(a.target + u);
+          blocked = valid_move(ldc(a.pw + tu), (u32)a.vwgt[u], maxw_of(a, tu));
+        }
       }
       const bool any_blocked = __any_sync(kFullMask, blocked);
       if (lane == src) cand = !any_blocked;
     }
-    block_append64(cand, move_key(g, v), a.cands, &st->ccount, s_cnt, s_base);
+    if (a.batch) {   // graph g's candidates go to cands[gvbase[g]..]
+      if (cand) {
+        const i32 gv = __ldg(a.gid + v);
+        a.cands[__ldg(a.gvbase + gv) + atomicAdd(a.gcc + gv, 1)] = move_key(g, v);
+      }
+    } else {
+      block_append64(cand, move_key(g, v), a.cands, &st->ccount, s_cnt, s_base);
+    }
   }
 }
 
@@ -548,7 +597,7 @@ __device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u3
     const i32 pv = (i32)s_warp[wid];
     const i32 carry = fe ? ve : pv + ve;   // running sum entering this thread
     (void)pf;
-    const float maxw = a.maxw;
+    const float maxw_plain = a.maxw;
 #pragma unroll
     for (i32 r = 0; r < kMaxR; ++r) {
       const i32 i = i0 + r;
@@ -557,7 +606,7 @@ __device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u3
         const i32 D = before_head ? val[r] + carry : val[r];
         const u64 e = ev[i];
         const u32 p = (u32)(e >> 43);
-        if (D > 0 && __uint2float_rn((u32)D + ldc(a.pw + p)) > maxw) {
+        if (D > 0 && __uint2float_rn((u32)D + ldc(a.pw + p)) > (a.batch ? __ldg(a.pmaxw + p) : maxw_plain)) {
           const i32 m = (i32)((e >> 32) & 0x7FFu);
           const i32 end = (i + 1 < E && (ev[i + 1] >> 43) == (e >> 43)) ? (i32)((ev[i + 1] >> 32) & 0x7FFu) : B;
           atomicAdd(&diff[m], 1);
@@ -593,17 +642,11 @@ __device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u3
   return pos < 0 ? 0 : pos;
 }
 
-__device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, bool balance_mode) {
-  if (blockIdx.x != 0) return;
-  RoundState* st = a.st;
-  const i32 cnt = ldc(&st->ccount);
-  if (cnt == 0) {
-    if (threadIdx.x == 0) {
-      if (balance_mode) st->bdone = 1;
-      else st->done = 1;
-    }
-    return;
-  }
+// Sort one candidate set cands[0..cnt) into s by (gain desc, id asc) and keep
+// the first B = min(cnt, cap) (uncoarsen.hpp:471-476 with
+// move_request.hpp:36-41); more than kSortMax candidates are streamed
+// through shared memory keeping the running top `cap`.  Block-wide.
+__device__ i32 select_sort(const LevelArgs& a, const u64* cands, i32 cnt, u64* s, i32* greedy) {
   const i32 cap = a.move_cap;
   const i32 B = cnt < cap ? cnt : cap;
   // Element i is owned by thread i mod blockDim; for strides j < 32 both
@@ -629,7 +672,7 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, 
   if (cnt <= kSortMax) {
     i32 P = 32;
     while (P < cnt) P <<= 1;
-    for (i32 i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cnt ? ldc(a.cands + i) : ~0ull;
+    for (i32 i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cnt ? ldc(cands + i) : ~0ull;
     __syncthreads();
     // the greedy region is free until the greedy pass and holds kSortMax keys
     u64* t = reinterpret_cast<u64*>(greedy);
@@ -644,7 +687,7 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, 
       const i32 lo = first ? 0 : cap;
       for (i32 i = lo + threadIdx.x; i < kSortMax; i += blockDim.x) {
         const i32 src = next + (i - lo);
-        s[i] = src < cnt ? ldc(a.cands + src) : ~0ull;
+        s[i] = src < cnt ? ldc(cands + src) : ~0ull;
       }
       next += kSortMax - lo;
       first = false;
@@ -652,47 +695,115 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, 
       bitonic(kSortMax);
     }
   }
+  return B;
+}
+
+// Balance rounds: greedy pass in sorted order over s[0..B): take a move while
+// its source is still overweight and its destination stays within the cap,
+// skip the others.  Sources and destinations of one round are disjoint (a
+// destination had room, a source did not), so one running weight per part
+// suffices.  The kept moves are compacted to the front of s; returns their
+// number.  Parts of the candidate set are [pb, pb + k).
+__device__ i32 select_greedy(const LevelArgs& a, u64* s, i32* greedy, i32 B, i32 pb, i32 k) {
+  __shared__ i32 s_nsel;
+  i32* mv_src = greedy;
+  i32* mv_des = mv_src + kMaxMoveCap;
+  u32* mv_w = reinterpret_cast<u32*>(mv_des + kMaxMoveCap);
+  u32* rem = (k <= kGreedySmemParts ? mv_w + kMaxMoveCap : a.brem + pb) - pb;
+  for (i32 t = threadIdx.x; t < B; t += blockDim.x) {
+    const i32 v = (i32)(u32)s[t];
+    mv_src[t] = ldc(a.part + v);
+    mv_des[t] = ldc(a.btarget + v);
+    mv_w[t] = (u32)a.vwgt[v];
+  }
+  for (i32 q = threadIdx.x; q < k; q += blockDim.x) rem[pb + q] = ldc(a.pw + pb + q);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    i32 nsel = 0;
+    for (i32 t = 0; t < B; ++t) {
+      const u32 w = mv_w[t];
+      const i32 sp = mv_src[t], dp = mv_des[t];
+      if (over_cap(rem[sp], bcap_of(a, sp)) && !over_cap(rem[dp] + w, bcap_of(a, dp))) {
+        rem[sp] -= w;
+        rem[dp] += w;
+        s[nsel++] = s[t];
+      }
+    }
+    s_nsel = nsel;
+  }
+  __syncthreads();
+  const i32 nsel = s_nsel;
+  __syncthreads();
+  return nsel;
+}
+
+// Plain level: block 0 selects from all candidates.  Resets the per-round
+// counters.
+__device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, bool balance_mode) {
+  if (blockIdx.x != 0) return;
+  RoundState* st = a.st;
+  const i32 cnt = ldc(&st->ccount);
+  if (cnt == 0) {
+    if (threadIdx.x == 0) {
+      if (balance_mode) st->bdone = 1;
+      else st->done = 1;
+    }
+    return;
+  }
+  const i32 B = select_sort(a, a.cands, cnt, s, greedy);
   if (!balance_mode) {
     for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
     const i32 pos = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp);
     if (threadIdx.x == 0) st->pos = pos;
   } else {
-    // greedy pass in sorted order: take a move while its source is still
-    // overweight and its destination stays within the cap, skip the others.
-    // Sources and destinations of one round are disjoint (a destination had
-    // room, a source did not), so one running weight per part suffices.
-    i32* mv_src = greedy;
-    i32* mv_des = mv_src + kMaxMoveCap;
-    u32* mv_w = reinterpret_cast<u32*>(mv_des + kMaxMoveCap);
-    u32* rem = a.k <= kGreedySmemParts ? mv_w + kMaxMoveCap : a.brem;
-    for (i32 t = threadIdx.x; t < B; t += blockDim.x) {
-      const i32 v = (i32)(u32)s[t];
-      mv_src[t] = ldc(a.part + v);
-      mv_des[t] = ldc(a.btarget + v);
-      mv_w[t] = (u32)a.vwgt[v];
-    }
-    for (i32 q = threadIdx.x; q < a.k; q += blockDim.x) rem[q] = ldc(a.pw + q);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      i32 nsel = 0;
-      const float cap_f = a.bcap;
-      for (i32 t = 0; t < B; ++t) {
-        const u32 w = mv_w[t];
-        const i32 sp = mv_src[t], dp = mv_des[t];
-        if (over_cap(rem[sp], cap_f) && !over_cap(rem[dp] + w, cap_f)) {
-          rem[sp] -= w;
-          rem[dp] += w;
-          a.top[nsel++] = s[t];
-        }
-      }
-      st->firstbad = nsel;   // moves 0..nsel-1 of top are applied
-    }
+    const i32 nsel = select_greedy(a, s, greedy, B, 0, a.k);
+    for (i32 i = threadIdx.x; i < nsel; i += blockDim.x) a.top[i] = s[i];
+    if (threadIdx.x == 0) st->firstbad = nsel;   // moves 0..nsel-1 of top are applied
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     st->B = B;
     st->ccount = 0;
     st->ucount = 0;
+  }
+}
+
+// Batched level: CTA b selects for graphs b, b + grid, ... from their own
+// candidate buckets and appends the moves it keeps to the flat list
+// top[0..mcount).  A graph with candidates raises anyf[r % 3]; block 0
+// clears anyf[(r + 1) % 3], last read two barriers ago.
+__device__ void ph_select_batch(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, bool balance_mode, i64 r) {
+  __shared__ i32 s_cnt, s_base;
+  RoundState* st = a.st;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.anyf[(r + 1) % 3] = 0;
+    st->ucount = 0;
+  }
+  for (i32 g = blockIdx.x; g < a.G; g += gridDim.x) {
+    if (threadIdx.x == 0) {
+      s_cnt = ldc(a.gcc + g);
+      a.gcc[g] = 0;
+    }
+    __syncthreads();
+    const i32 cnt = s_cnt;
+    __syncthreads();
+    if (cnt == 0) continue;   // block-uniform
+    if (threadIdx.x == 0) atomicExch(a.anyf + r % 3, 1);
+    u64* cg = a.cands + __ldg(a.gvbase + g);
+    const i32 B = select_sort(a, cg, cnt, s, greedy);
+    i32 keep;
+    if (!balance_mode) {
+      // the check below overwrites s: park the sorted moves in the bucket
+      for (i32 i = threadIdx.x; i < B; i += blockDim.x) cg[i] = s[i];
+      keep = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp) + 1;
+    } else {
+      keep = select_greedy(a, s, greedy, B, __ldg(a.gpbase + g), __ldg(a.gk + g));
+      for (i32 i = threadIdx.x; i < keep; i += blockDim.x) cg[i] = s[i];
+    }
+    if (threadIdx.x == 0) s_base = atomicAdd(a.mcount, keep);
+    __syncthreads();
+    for (i32 i = threadIdx.x; i < keep; i += blockDim.x) a.top[s_base + i] = cg[i];
+    __syncthreads();
   }
 }
 
@@ -724,7 +835,7 @@ __device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
 // (uncoarsen.hpp:290-323).  One warp per move.
 __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
-  const i32 pos = ldc(&st->pos);
+  const i32 pos = a.batch ? ldc(a.mcount) - 1 : ldc(&st->pos);   // batched: every graph's kept moves
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
@@ -809,14 +920,61 @@ __device__ void ph_bal_prep(const LevelArgs& a, u64* s_tmp) {
   __syncthreads();
 }
 
+// Batched level: CTA b finds the lightest part of graphs b, b + grid, ...;
+// a balance-active graph with an overweight part raises anyf[r % 3] (block 0
+// clears anyf[(r + 1) % 3]).  Block 0 opens the round's epoch.
+__device__ void ph_bal_prep_batch(const LevelArgs& a, u64* s_tmp, i64 r) {
+  __shared__ u32 s_over[32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.st->epoch = ++(*a.epoch);
+    a.st->lcount = 0;
+    a.anyf[(r + 1) % 3] = 0;
+  }
+  for (i32 g = blockIdx.x; g < a.G; g += gridDim.x) {
+    const i32 pb = __ldg(a.gpbase + g), k = __ldg(a.gk + g);
+    u64 best = ~0ull;
+    u32 over = 0;
+    for (i32 p = pb + threadIdx.x; p < pb + k; p += blockDim.x) {
+      const u32 w = ldc(a.pw + p);
+      const u64 key = ((u64)w << 32) | (u32)p;
+      best = key < best ? key : best;
+      over |= over_cap(w, __ldg(a.pbcap + p)) ? 1u : 0u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const u64 y = __shfl_xor_sync(kFullMask, best, o);
+      best = y < best ? y : best;
+      over |= __shfl_xor_sync(kFullMask, over, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      s_tmp[threadIdx.x >> 5] = best;
+      s_over[threadIdx.x >> 5] = over;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        best = s_tmp[w] < best ? s_tmp[w] : best;
+        over |= s_over[w];
+      }
+      a.glight[g] = (i32)(u32)best;
+      if (over && ((__ldg(a.gflags + g) >> 1) & 1)) atomicExch(a.anyf + r % 3, 1);
+    }
+    __syncthreads();
+  }
+}
+
 // Boundary vertices of overweight parts -> blist.
 __device__ void ph_bal_filter(const LevelArgs& a) {
+  if (a.batch && blockIdx.x == 0 && threadIdx.x == 0) *a.mcount = 0;
   const int lane = threadIdx.x & 31;
   const i64 stride = (i64)gridDim.x * blockDim.x;
   for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += stride) {
     const i64 v = base + lane;
     bool want = false;
-    if (v < a.n) want = ldc(a.bnd + v) && over_cap(ldc(a.pw + ldc(a.part + v)), a.bcap);
+    if (v < a.n && ldc(a.bnd + v) && graph_flag(a, (i32)v, 1)) {
+      const i32 p = ldc(a.part + v);
+      want = over_cap(ldc(a.pw + p), bcap_of(a, p));
+    }
     warp_append(want, (i32)v, a.blist, &a.st->lcount);
   }
 }
@@ -824,26 +982,28 @@ __device__ void ph_bal_filter(const LevelArgs& a) {
 __device__ void ph_bal_eval(const LevelArgs& a, u32* acc_all) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid >= a.acc_warps) return;
-  u32* acc = acc_all + (size_t)wid * a.k;
+  u32* acc = acc_all + (size_t)wid * a.kacc;
   RoundState* st = a.st;
   const u32 ep = ldc(&st->epoch);
-  const i32 light = ldc(&st->light);
+  const i32 light_plain = a.batch ? 0 : ldc(&st->light);
   const i32 nl = ldc(&st->lcount);
-  const float cap = a.bcap;
   const i64 nw = (i64)gridDim.x * a.acc_warps;
   for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nl; i += nw) {
     const i32 v = ldc(a.blist + i);
     const i32 p = ldc(a.part + v);
     const u32 w = (u32)a.vwgt[v];
+    const i32 pb = part_base_of(a, v);
+    u32* accb = acc - pb;   // rows are indexed by the graph's own part ids
+    const i32 light = a.batch ? ldc(a.glight + __ldg(a.gid + v)) : light_plain;
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
-    for (i32 e = beg + lane; e < end; e += 32) atomicAdd(&acc[ldc(a.part + a.adjncy[e])], (u32)a.adjwgt[e]);
+    for (i32 e = beg + lane; e < end; e += 32) atomicAdd(&accb[ldc(a.part + a.adjncy[e])], (u32)a.adjwgt[e]);
     __syncwarp();
-    const u32 id = acc[p];
+    const u32 id = accb[p];
     u64 best = 0;
     for (i32 e = beg + lane; e < end; e += 32) {
       const i32 q = ldc(a.part + a.adjncy[e]);
-      if (q == p || over_cap(ldc(a.pw + q) + w, cap)) continue;
-      const i32 g = (i32)(acc[q] - id);
+      if (q == p || over_cap(ldc(a.pw + q) + w, bcap_of(a, q))) continue;
+      const i32 g = (i32)(accb[q] - id);
       const u64 key = (1ull << 63) | ((u64)((u32)g ^ 0x80000000u) << 31) | (u64)(0x7fffffffu - (u32)q);
       best = best > key ? best : key;
     }
@@ -856,9 +1016,9 @@ __device__ void ph_bal_eval(const LevelArgs& a, u32* acc_all) {
     if (best) {
       q_best = (i32)(0x7fffffffu - (u32)(best & 0x7fffffffu));
       g_best = (i32)((u32)(best >> 31) ^ 0x80000000u);
-    } else if (light != p && !over_cap(ldc(a.pw + light) + w, cap)) {
+    } else if (light != p && !over_cap(ldc(a.pw + light) + w, bcap_of(a, light))) {
       q_best = light;
-      g_best = (i32)(acc[light] - id);
+      g_best = (i32)(accb[light] - id);
     }
     if (lane == 0 && q_best >= 0) {
       a.bmark[v] = ep;
@@ -866,7 +1026,7 @@ __device__ void ph_bal_eval(const LevelArgs& a, u32* acc_all) {
       a.bgain[v] = g_best;
     }
     __syncwarp();
-    for (i32 e = beg + lane; e < end; e += 32) acc[ldc(a.part + a.adjncy[e])] = 0;
+    for (i32 e = beg + lane; e < end; e += 32) accb[ldc(a.part + a.adjncy[e])] = 0;
     __syncwarp();
   }
 }
@@ -890,13 +1050,20 @@ __device__ void ph_bal_emit(const LevelArgs& a) {
         if (u < v && ldc(a.bmark + u) == ep) { emit = false; break; }
       }
     }
-    warp_append64(emit, move_key(g, v), a.cands, &st->ccount);
+    if (a.batch) {   // graph buckets, as in ph_candidates
+      if (emit) {
+        const i32 gv = __ldg(a.gid + v);
+        a.cands[__ldg(a.gvbase + gv) + atomicAdd(a.gcc + gv, 1)] = move_key(g, v);
+      }
+    } else {
+      warp_append64(emit, move_key(g, v), a.cands, &st->ccount);
+    }
   }
 }
 
 __device__ void ph_apply_balance(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
-  const i32 pos = ldc(&st->firstbad) - 1;
+  const i32 pos = (a.batch ? ldc(a.mcount) : ldc(&st->firstbad)) - 1;
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
@@ -941,10 +1108,12 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
   {
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (wid < a.acc_warps)
-      for (i32 q = lane; q < a.k; q += 32) acc_all[(size_t)wid * a.k + q] = 0;
+      for (i32 q = lane; q < a.kacc; q += 32) acc_all[(size_t)wid * a.kacc + q] = 0;
   }
   __syncthreads();
   RoundState* st = a.st;
+  // batched levels: the rotating flag use counter (uniform over the grid)
+  i64 fr = 0;
   trace_mark(a, 0);
   if (a.flags & LF_PROJECT) {
     ph_project(a);
@@ -957,7 +1126,10 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
     trace_mark(a, 2);
   }
   if (a.flags & LF_UPDATE) ph_update(a, acc_all, false);
-  if (a.flags & LF_BALANCE) ph_bal_prep(a, s_tmp);
+  if (a.flags & LF_BALANCE) {
+    if (a.batch) ph_bal_prep_batch(a, s_tmp, fr);
+    else ph_bal_prep(a, s_tmp);
+  }
   if (a.flags & (LF_UPDATE | LF_BALANCE)) {
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
     trace_mark(a, 3);
@@ -968,7 +1140,9 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 2);
         return;
       }
-      if (ldc(&st->bdone)) break;   // nothing overweight (prep) or no candidate (select)
+      // nothing overweight (prep) or no candidate (select)
+      if (a.batch ? ldc(a.anyf + fr % 3) == 0 : ldc(&st->bdone) != 0) break;
+      ++fr;
       ph_bal_filter(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 9);
@@ -978,15 +1152,18 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       ph_bal_emit(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 11);
-      ph_select(a, s_sort, greedy, s_warp, true);
+      if (a.batch) ph_select_batch(a, s_sort, greedy, s_warp, true, fr);
+      else ph_select(a, s_sort, greedy, s_warp, true);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 12);
-      if (ldc(&st->bdone)) break;
+      if (a.batch ? ldc(a.anyf + fr % 3) == 0 : ldc(&st->bdone) != 0) break;
+      ++fr;
       ph_apply_balance(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 14);
       ph_update(a, acc_all, true);
-      ph_bal_prep(a, s_tmp);
+      if (a.batch) ph_bal_prep_batch(a, s_tmp, fr);
+      else ph_bal_prep(a, s_tmp);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 15);
     }
@@ -1000,10 +1177,15 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       ph_candidates(a, &s_cnt, &s_base);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 20);
-      ph_select(a, s_sort, greedy, s_warp, false);
+      if (a.batch) {
+        ++fr;
+        ph_select_batch(a, s_sort, greedy, s_warp, false, fr);
+      } else {
+        ph_select(a, s_sort, greedy, s_warp, false);
+      }
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 21);
-      if (ldc(&st->done)) break;
+      if (a.batch ? ldc(a.anyf + fr % 3) == 0 : ldc(&st->done) != 0) break;
       ph_apply_refine(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 23);
@@ -1056,7 +1238,10 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->P[0] = P.alloc_n<i32>(n);
   c->P[1] = P.alloc_n<i32>(n);
   c->cands = P.alloc_n<u64>(n);
-  c->top = P.alloc_n<u64>(kMaxMoveCap);
+  // a batch keeps up to move_cap moves per graph in one round; every vertex
+  // is a candidate at most once per round, so n entries always suffice
+  const bool batched = c->kacc > 0 && c->kacc < c->k;
+  c->top = P.alloc_n<u64>(batched ? std::max<size_t>(n, kMaxMoveCap) : kMaxMoveCap);
   c->pw = P.alloc_n<u32>(c->k);
   c->st = P.alloc_n<RoundState>(1);
   c->bmark = P.alloc_n<u32>(n);
@@ -1080,9 +1265,10 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   GKW_CUDA(cudaMemsetAsync(c->stats, 0, sizeof(LevelStatsDev) * kStatSlots, h.stream));
   // per-warp part-connection rows: as many warps as fit beside the sort buffer
   const size_t budget = 120 * 1024;
-  const i32 w = (i32)std::min<size_t>(kLevelThreads / 32, budget / (4 * (size_t)c->k));
+  if (c->kacc <= 0) c->kacc = c->k;
+  const i32 w = (i32)std::min<size_t>(kLevelThreads / 32, budget / (4 * (size_t)c->kacc));
   c->acc_warps = std::max(1, w);
-  c->smem = (size_t)kSortMax * 8 + (size_t)kGreedyWords * 4 + (size_t)c->acc_warps * c->k * 4;
+  c->smem = (size_t)kSortMax * 8 + (size_t)kGreedyWords * 4 + (size_t)c->acc_warps * c->kacc * 4;
   // one value for every handle of the process (handles of a server launch
   // this kernel concurrently with different sizes): the device's opt-in limit
   // less the kernel's static shared memory
@@ -1097,12 +1283,15 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->grid = h.sm_count * std::min(bps, 2);
 }
 
-RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap) {
+RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap, i32 kacc) {
   GKW_REQUIRE(move_cap >= 1 && move_cap <= kMaxMoveCap, GKW_E_UNSUPPORTED, "move_cap must be in [1, 2048]");
-  GKW_REQUIRE(k >= 1 && k <= 40000, GKW_E_UNSUPPORTED, "k must be in [1, 40000]");
+  if (kacc <= 0) kacc = k;
+  GKW_REQUIRE(kacc >= 1 && kacc <= 40000, GKW_E_UNSUPPORTED, "k must be in [1, 40000]");
+  GKW_REQUIRE(k >= kacc && k < (1 << 21), GKW_E_UNSUPPORTED, "too many parts");
   RefineCtx* c = new RefineCtx();
   c->n_max = n_max;
   c->k = k;
+  c->kacc = kacc;
   c->cap = move_cap;
   const size_t n = std::max(n_max, 1);
   Pool& P = h.hier;
@@ -1215,6 +1404,22 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.err = c->err;
   a.stat_slot = c->stats + slot;
   a.acc_warps = c->acc_warps;
+  a.kacc = c->kacc;
+  if (j.batch) {
+    a.batch = 1;
+    a.G = j.batch->G;
+    a.gid = j.batch->gid;
+    a.gvbase = j.batch->gvbase;
+    a.gpbase = j.batch->gpbase;
+    a.gk = j.batch->gk;
+    a.gflags = j.batch->gflags;
+    a.pmaxw = j.batch->pmaxw;
+    a.pbcap = j.batch->pbcap;
+    a.gcc = j.batch->gcc;
+    a.glight = j.batch->glight;
+    a.mcount = j.batch->mcount;
+    a.anyf = j.batch->anyf;
+  }
   if (c->trace) {
     a.trace = c->trace + (size_t)slot * kTraceCap;
     a.trace_cap = kTraceCap;
@@ -1223,7 +1428,7 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   // small levels use fewer CTAs: the barrier gets cheaper and the work fits;
   // at least enough CTAs for the per-part checks to run in few passes
   i32 grid = (i32)ceil_div(std::max(g.n, 1), 512);
-  grid = std::max(grid, std::max(32, c->k / 4));
+  grid = std::max(grid, std::max(32, c->kacc / 4));
   grid = std::min(grid, c->grid);
   grid = coop_grid(h, (const void*)k_level, grid, kLevelThreads, c->smem);
   void* args[] = {&a};

@@ -96,6 +96,9 @@ struct gkw_server {
   Clock::time_point first_submit, last_done;
   i64 peak_reserved = 0;
   i32 peak_running = 0;
+  // gkw_partition_batch's union path runs on its own handle (one batch at a time)
+  std::mutex batch_mu;
+  gkw_handle* batch_h = nullptr;
 
   i64 total_charge() const {
     i64 t = 0;
@@ -268,6 +271,7 @@ void gkw_server_default_config(gkw_server_config* c) {
   c->slot_keep_bytes = (int64_t)256 << 20;
   c->max_bypass = 0;   // 0: 4 x slots
   c->narrow_max_n = 262144;
+  c->batch_union = 1;
 }
 
 int64_t gkw_predict_footprint(int32_t n, int64_t nnz, int32_t k) {
@@ -340,6 +344,7 @@ gkw_status gkw_server_destroy(gkw_server* s) {
     s->cv_done.notify_all();
     for (std::thread& t : s->threads) t.join();
     for (Slot& sl : s->slots) gkw_destroy(sl.h);
+    if (s->batch_h) gkw_destroy(s->batch_h);
     delete s;
   });
 }
@@ -451,6 +456,7 @@ gkw_status gkw_server_stats_get(gkw_server* s, gkw_server_stats* out, int32_t re
 gkw_status gkw_partition_batch(gkw_server* s, const gkw_csr_batch* b, const gkw_options* opt, int32_t* part_out,
                                int64_t* cut_out, int32_t* status_out) {
   std::vector<JobPtr> jobs;
+  bool union_done = false;
   gkw_status st = guard_s([&] {
     GKW_REQUIRE(s != nullptr && b != nullptr, GKW_E_INVALID, "NULL argument");
     const gkw_csr& g = b->graph;
@@ -465,6 +471,63 @@ gkw_status gkw_partition_batch(gkw_server* s, const gkw_csr_batch* b, const gkw_
     GKW_REQUIRE(g.xadj[0] == 0 && g.xadj[g.n] == g.nnz, GKW_E_INVALID, "xadj does not span nnz");
     gkw_options base;
     if (opt) base = *opt; else gkw_default_options(&base);
+    for (i32 i = 0; i < b->n_graphs; ++i) {
+      GKW_REQUIRE(b->graph_ptr[i] <= b->graph_ptr[i + 1], GKW_E_INVALID, "graph_ptr must not decrease");
+      GKW_REQUIRE(b->k[i] >= 1, GKW_E_INVALID, "k must be >= 1 (graph " + std::to_string(i) + ")");
+    }
+    // the whole batch as one disjoint union (batch.cu) when every graph uses
+    // the same options: one pipeline for all graphs instead of one per graph
+    bool same_eps = true;
+    for (i32 i = 0; b->eps && i < b->n_graphs; ++i) same_eps &= b->eps[i] == b->eps[0];
+    if (s->cfg.batch_union && base.init_method == GKW_INIT_DEVICE && same_eps) {
+      gkw_options uo = base;
+      if (b->eps && b->n_graphs) uo.eps = b->eps[0];
+      std::lock_guard<std::mutex> lk(s->batch_mu);
+      if (!s->batch_h) {
+        const gkw_status cs = gkw_create(&s->batch_h, s->device);
+        if (cs != GKW_OK) throw Error{cs, gkw_last_error()};
+      }
+      DevGraph hg;
+      hg.n = g.n;
+      hg.m = g.nnz;
+      hg.xadj = g.xadj;
+      hg.adjncy = g.adjncy;
+      hg.adjwgt = g.adjwgt;
+      hg.vwgt = g.vwgt;
+      Handle& bh = handle_of(s->batch_h);
+      bh.narrow = false;
+      std::vector<i64> cuts(std::max(b->n_graphs, 1));
+      const auto t0 = Clock::now();
+      bool ok = false;
+      try {
+        ok = partition_batch_union(bh, hg, b->n_graphs, b->graph_ptr, b->k, uo, part_out, cuts.data());
+      } catch (const Error& e) {
+        if (e.st != GKW_E_INVALID) throw;   // a bad graph: the per-graph path reports which one
+      }
+      if (ok) {
+        const auto t1 = Clock::now();
+        for (i32 i = 0; i < b->n_graphs; ++i) {
+          if (cut_out) cut_out[i] = cuts[i];
+          if (status_out) status_out[i] = GKW_OK;
+        }
+        std::lock_guard<std::mutex> lk2(s->mu);
+        if (!s->have_first && b->n_graphs) {
+          s->have_first = true;
+          s->first_submit = t0;
+        }
+        s->submitted += b->n_graphs;
+        s->completed += b->n_graphs;
+        for (i32 i = 0; i < b->n_graphs; ++i) {   // every graph of the batch completes with it
+          s->latencies.push_back(ms_between(t0, t1));
+          s->queue_waits.push_back(0.0);
+        }
+        s->last_done = t1;
+        union_done = true;
+        return;
+      }
+      // an edge joins two graphs, or a graph is malformed: the per-graph path
+      // reports which graph
+    }
     for (i32 i = 0; i < b->n_graphs; ++i) {
       const i32 v0 = b->graph_ptr[i], v1 = b->graph_ptr[i + 1];
       GKW_REQUIRE(v0 <= v1, GKW_E_INVALID, "graph_ptr must not decrease");
@@ -514,7 +577,7 @@ gkw_status gkw_partition_batch(gkw_server* s, const gkw_csr_batch* b, const gkw_
       return true;
     });
   });
-  if (st != GKW_OK) return st;
+  if (st != GKW_OK || union_done) return st;
   gkw_status first = GKW_OK;
   for (size_t i = 0; i < jobs.size(); ++i) {
     if (cut_out) cut_out[i] = jobs[i]->cut;

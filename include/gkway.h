@@ -247,7 +247,10 @@ typedef struct gkw_server_config {
   int64_t slot_keep_bytes;   /* memory a slot keeps between jobs (default 256 MiB) */
   int32_t max_bypass;        /* times the oldest waiting job may be overtaken by smaller
                                 jobs that fit when it does not (default 4 x slots) */
-  int32_t reserved[7];
+  int32_t batch_union;       /* 1 (default): gkw_partition_batch partitions the whole batch as one
+                                disjoint union when all graphs share the options; 0: one job per
+                                graph on the slots */
+  int32_t reserved[6];
 } gkw_server_config;
 
 void gkw_server_default_config(gkw_server_config* cfg);

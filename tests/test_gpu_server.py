@@ -2,8 +2,9 @@
 
 The alone result is the host entry point gkw_partition on a plain handle; the
 batched result comes from one gkw_partition_batch call over the concatenated
-CSR, the served result from requests submitted by several host threads while
-others run.  Part vectors and cuts must be identical (integer work: exact)."""
+CSR (as one disjoint union, or one job per graph on the slots), the served
+result from requests submitted by several host threads while others run.
+Part vectors and cuts must be identical (integer work: exact)."""
 import threading
 import time
 
@@ -49,11 +50,73 @@ def alone(pkg, gs, ks, opts=None):
     return out
 
 
+def shuffled_rows(g, seed):
+    """The same graph with every adjacency row in a random order."""
+    rng = np.random.default_rng(seed)
+    a = g.adjncy.copy()
+    w = g.adjwgt.copy()
+    for v in range(g.n):
+        lo, hi = int(g.xadj[v]), int(g.xadj[v + 1])
+        p = rng.permutation(hi - lo) + lo
+        a[lo:hi] = a[p]
+        w[lo:hi] = w[p]
+    return type(g)(g.xadj.copy(), a, w, g.vwgt.copy())
+
+
+def check_batch(pkg, srv, gs, ks, opts=None):
+    ref = alone(pkg, gs, ks, opts)
+    x, a, w, vw, gp = pkg.concat_graphs(gs)
+    part, cuts, sts = srv.partition_batch(x, a, w, vw, gp, ks, opts=opts)
+    assert list(sts) == [0] * len(gs)
+    for i, (p_ref, c_ref) in enumerate(ref):
+        assert np.array_equal(part[gp[i]:gp[i + 1]], p_ref), i
+        assert cuts[i] == c_ref, i
+
+
+def test_union_batch_matches_alone(pkg, gen):
+    """One pipeline over the disjoint union: small graphs that stop coarsening
+    at once (rows in random order), graphs that stop at different depths, k = 1,
+    empty and one-vertex graphs, in both modes and with other balance-skip
+    settings."""
+    gs, ks = mixed_graphs(gen)
+    for i in (0, 5, 6, 8):
+        gs[i] = shuffled_rows(gs[i], 40 + i)
+    srv = pkg.Server(0, slots=2)
+    check_batch(pkg, srv, gs, ks)
+    check_batch(pkg, srv, gs, ks, pkg.default_options(enforce_balance=0))
+    check_batch(pkg, srv, gs, ks, pkg.default_options(balance_skip_levels=0, coarse_vertex_frac=0.0))
+    check_batch(pkg, srv, gs[:12], ks[:12], pkg.default_options(balance_skip_levels=2, eps=0.05))
+    st = srv.stats()
+    assert st["completed"] == 3 * len(gs) + 12 and st["failed"] == 0
+    assert st["peak_running"] == 0      # no slot job ran: every batch went through the union
+    srv.close()
+
+
+def test_union_batch_falls_back_on_duplicate_edges(pkg, gen):
+    # a small graph whose rows hold a duplicate edge cannot be carried verbatim
+    # through the union's levels: the batch runs graph by graph instead
+    g = gen.delaunay(600, 7)
+    u = int(g.adjncy[g.xadj[0]])   # edge 0-u listed twice in both rows
+    rows = [list(zip(g.adjncy[g.xadj[v]:g.xadj[v + 1]], g.adjwgt[g.xadj[v]:g.xadj[v + 1]])) for v in range(g.n)]
+    rows[0].append((u, 1))
+    rows[u].append((0, 1))
+    x = np.zeros(g.n + 1, np.int32)
+    x[1:] = np.cumsum([len(r) for r in rows])
+    a = np.array([e for r in rows for e, _ in r], np.int32)
+    w = np.array([c for r in rows for _, c in r], np.int32)
+    gd = type(g)(x, a, w, g.vwgt.copy())
+    gs = [gen.delaunay(30000, 3), gd]
+    ks = [8, 4]
+    srv = pkg.Server(0, slots=2)
+    check_batch(pkg, srv, gs, ks)
+    srv.close()
+
+
 def test_batch_matches_alone(pkg, gen):
     gs, ks = mixed_graphs(gen)
     ref = alone(pkg, gs, ks)
     x, a, w, vw, gp = pkg.concat_graphs(gs)
-    srv = pkg.Server(0, slots=6)
+    srv = pkg.Server(0, slots=6, batch_union=0)
     part, cuts, sts = srv.partition_batch(x, a, w, vw, gp, ks)
     assert list(sts) == [0] * len(gs)
     for i, (p_ref, c_ref) in enumerate(ref):
@@ -122,7 +185,7 @@ def test_server_budget_serialises_jobs(pkg, gen):
     gs, ks = mixed_graphs(gen, seed=2)
     gs, ks = gs[:8], ks[:8]
     ref = alone(pkg, gs, ks)
-    srv = pkg.Server(0, slots=4, pool_bytes=1)   # nothing fits beside a running job
+    srv = pkg.Server(0, slots=4, pool_bytes=1, batch_union=0)   # nothing fits beside a running job
     x, a, w, vw, gp = pkg.concat_graphs(gs)
     part, cuts, sts = srv.partition_batch(x, a, w, vw, gp, ks)
     for i, (p_ref, c_ref) in enumerate(ref):
@@ -138,7 +201,7 @@ def test_wide_jobs_take_turns(pkg, gen):
     gs, ks = mixed_graphs(gen, seed=3)
     gs, ks = gs[:10], ks[:10]
     ref = alone(pkg, gs, ks)
-    srv = pkg.Server(0, slots=4, narrow_max_n=0)
+    srv = pkg.Server(0, slots=4, narrow_max_n=0, batch_union=0)
     x, a, w, vw, gp = pkg.concat_graphs(gs)
     part, cuts, sts = srv.partition_batch(x, a, w, vw, gp, ks)
     for i, (p_ref, c_ref) in enumerate(ref):
