@@ -589,6 +589,7 @@ def bench_served(args):
         for mode in ("served", "plain"):
             lat = [0.0] * nreq
             done_t = [0.0] * nreq
+            together = [1] * nreq
             if mode == "served":
                 srv = pkg.Server(0, slots=args.slots)
                 tickets = [None] * nreq
@@ -609,6 +610,7 @@ def bench_served(args):
                         time.sleep(0.0002)
                     r = srv.poll(tickets[i], pool[which[i]].n, wait_ms=-1)
                     lat[i] = r[2]["latency_ms"]
+                    together[i] = r[2]["batch_graphs"]
                     done_t[i] = time.perf_counter()
                 th.join()
                 srv.close()
@@ -627,6 +629,8 @@ def bench_served(args):
             span = max(done_t) - t0
             res[mode] = {"graphs_per_s": nreq / span, "p50_ms": float(np.percentile(lat, 50)),
                          "p99_ms": float(np.percentile(lat, 99))}
+            if mode == "served":   # graphs partitioned together with a request, on average
+                res[mode]["mean_union_graphs"] = float(np.mean(together))
         out.append(res)
     print(json.dumps({"workload": "served", "metric": "served graphs/s and p50/p99 latency vs plain",
                       "unit": "graphs/s", "slots": args.slots, "loads": out,

@@ -125,7 +125,8 @@ class ServerConfig(ctypes.Structure):
         ("slot_keep_bytes", ctypes.c_int64),
         ("max_bypass", ctypes.c_int32),
         ("batch_union", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("batch_max_n", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -137,6 +138,8 @@ class RequestInfo(ctypes.Structure):
         ("predicted_bytes", ctypes.c_int64),
         ("slot", ctypes.c_int32),
         ("n_levels", ctypes.c_int32),
+        ("batch_graphs", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

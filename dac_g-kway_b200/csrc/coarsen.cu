@@ -66,13 +66,6 @@ void run_match(Handle& h, const DevGraph& g, i32* cand) {
   GKW_CHECK_LAUNCH();
 }
 
-// Batched levels: vertices of graphs that stopped coarsening take no partner,
-// so each such graph passes to the next level unchanged.
-__global__ void k_freeze(i32 n, const i32* __restrict__ gid, const i32* __restrict__ gfrozen, i32* __restrict__ cand) {
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < n && gfrozen[gid[v]]) cand[v] = (i32)v;
-}
-
 // ===========================================================================
 // Union-find label propagation (coarsen.hpp:80-118, loop :461-469), Jacobi
 // schedule, as one persistent cooperative kernel.  Keys are
@@ -839,15 +832,11 @@ __global__ void k_max_cvw(const i32* __restrict__ ncp, const i32* __restrict__ c
   if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
 }
 
-void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out, const i32* gid, const i32* gfrozen) {
+void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   Pool::Mark mk = h.scratch.mark();
   i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
   u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
   run_match(h, g, cand);
-  if (gfrozen && g.n > 0) {
-    launch(k_freeze, ceil_div(g.n, 256), 256, 0, h.stream, g.n, gid, gfrozen, cand);
-    GKW_CHECK_LAUNCH();
-  }
   run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
   out.cmap = h.hier.alloc_n<i32>(std::max(g.n, 1));
   run_group_map(h, g.n, keys, cap, out.cmap, &h.coop->nc);

@@ -229,9 +229,7 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc
 void ensure_arena(Handle& h, u64 words);
 // Reads the CoopState (one host sync) and throws on a recorded error.
 CoopState read_coop(Handle& h);
-// gid/gfrozen (batched levels): graphs with gfrozen[g] != 0 are copied unchanged
-void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out, const i32* gid = nullptr,
-                   const i32* gfrozen = nullptr);
+void coarsen_level(Handle& h, const DevGraph& g, i32 group_cap, CoarsenOut& out);
 
 // ---- refinement (refine.cu) ----
 struct RefineCtx;   // opaque
@@ -269,13 +267,17 @@ struct BatchLevel {
   const i32* gvbase = nullptr;   // [G + 1] vertex offsets at this level
   const i32* gpbase = nullptr;   // [G]
   const i32* gk = nullptr;       // [G]
-  const i32* gflags = nullptr;   // [G] bit 0 refine, bit 1 balance rounds at this level
+  const i32* gflags = nullptr;   // [G] bit 0 refine, bit 1 balance rounds, bit 2 coarsest level here
   const float* pmaxw = nullptr;  // [parts]
   const float* pbcap = nullptr;  // [parts]
   i32* gcc = nullptr;            // [G] zeroed
   i32* glight = nullptr;         // [G]
   i32* mcount = nullptr;         // [1] zeroed
   i32* anyf = nullptr;           // [3] zeroed
+  // graphs entering at this level (gflags bit 2): cmap[v] = -(1 + i) names
+  // entry i of their initial parts and boundary flags
+  const i32* part_init = nullptr;
+  const i32* bnd_init = nullptr;
 };
 // kacc: part-row length of the gain updates (largest k of a batch; 0 = k)
 RefineCtx* refine_create(Handle& h, i32 n_max, i32 k, i32 move_cap, i32 kacc = 0);
@@ -289,6 +291,9 @@ i32* refine_target(RefineCtx* c);
 u32* refine_pw(RefineCtx* c);
 // Coarsest level: part given; computes boundary flags and part weights.
 void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32* d_part_in);
+// Batched levels: part weights (global part ids) and boundary flags of the
+// initial parts of the coarsest union.
+void refine_init_union(Handle& h, RefineCtx* c, const DevGraph& cu, const i32* part, i32* bnd_out);
 void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i32 stats_slot);
 // Reads the per-level statistics of slots [0, nslots) (one host sync); throws
 // if a level kernel reported an error.
@@ -334,8 +339,9 @@ Handle& handle_of(gkw_handle* h);   // the handle behind a C-ABI handle (capi.cu
 // arrays with global ids, graph g = vertices [graph_ptr[g], graph_ptr[g+1]).
 // part_out gets each graph's own part ids.  Returns false, having computed
 // nothing, if an edge joins two graphs.
+// levels_out (optional): levels each graph kept, its input included.
 bool partition_batch_union(Handle& h, const DevGraph& host_union, i32 G, const i32* graph_ptr, const i32* ks,
-                           const gkw_options& opt, i32* part_out, i64* cuts_out);
+                           const gkw_options& opt, i32* part_out, i64* cuts_out, i32* levels_out = nullptr);
 const char* last_error_cstr();
 
 // ---- host helpers ----

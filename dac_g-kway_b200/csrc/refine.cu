@@ -138,7 +138,10 @@ struct LevelArgs {
   const i32* gvbase;    // [G + 1] vertex offsets of the graphs at this level
   const i32* gpbase;    // [G] first part of each graph
   const i32* gk;        // [G] parts of each graph
-  const i32* gflags;    // [G] bit 0: refinement rounds at this level, bit 1: balance rounds
+  const i32* gflags;    // [G] bit 0: refinement rounds at this level, bit 1: balance rounds,
+                        // bit 2: the graph's coarsest level (it enters with its initial parts)
+  const i32* part_init; // entering graphs: cmap[v] = -(1 + i) names entry i of these
+  const i32* bnd_init;
   const float* pmaxw;   // [parts] MAXW of each part
   const float* pbcap;   // [parts] balance cap of each part
   i32* gcc;             // [G] candidate counts; graph g's candidates at cands[gvbase[g]..]
@@ -255,14 +258,22 @@ __device__ void ph_project(const LevelArgs& a) {
     bool b = false;
     if (v < a.n) {
       const i32 c = a.cmap[v];
-      const i32 p = a.part_c[c];
-      const i32 bc = a.bnd_c[c];
+      i32 p, bc;
+      bool enter = false;
+      if (a.batch && c < 0) {   // the graph's coarsest level: its initial parts, no gain pass
+        p = a.part_init[-1 - c];
+        bc = a.bnd_init[-1 - c];
+        enter = true;
+      } else {
+        p = a.part_c[c];
+        bc = a.bnd_c[c];
+      }
       a.part[v] = p;
       a.bnd[v] = bc;
       a.gain[v] = 0;
       a.target[v] = p;
       a.inP[v] = 0;
-      b = bc != 0 && (!a.batch || __ldg(a.gflags + __ldg(a.gid + v)) != 0);
+      b = bc != 0 && !enter && (!a.batch || __ldg(a.gflags + __ldg(a.gid + v)) != 0);
       a.updflag[v] = b ? 1 : 0;
     }
     warp_append(b, (i32)v, a.U, &a.st->ucount);
@@ -373,7 +384,7 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
     if (i < nP) {
       v = ldc(a.P0 + i);
       g = ldc(a.gain + v);
-      if (g > 0 && ldc(a.bnd + v)) {
+      if (g > 0 && ldc(a.bnd + v) && graph_flag(a, v, 0)) {   // batched: graphs that refine here
         const i32 t = ldc(a.target + v);
         check = valid_move(ldc(a.pw + t), (u32)a.vwgt[v], maxw_of(a, t));
       }
@@ -1345,6 +1356,15 @@ void refine_init_coarsest(Handle& h, RefineCtx* c, const DevGraph& g, const i32*
   GKW_CUDA(cudaMemsetAsync(c->gain, 0, sizeof(i32) * g.n, h.stream));
 }
 
+void refine_init_union(Handle& h, RefineCtx* c, const DevGraph& cu, const i32* part, i32* bnd_out) {
+  c->cur = 0;
+  GKW_CUDA(cudaMemsetAsync(c->pw, 0, sizeof(u32) * c->k, h.stream));
+  if (cu.n == 0) return;
+  launch(k_boundary_pw, ceil_div(cu.n, 256), 256, 0, h.stream, cu.n, cu.xadj, cu.adjncy, cu.vwgt, part, bnd_out,
+         c->pw);
+  GKW_CHECK_LAUNCH();
+}
+
 void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i32 slot) {
   GKW_REQUIRE(j.move_cap >= 1 && j.move_cap <= c->cap, GKW_E_INVALID, "move_cap out of range");
   GKW_REQUIRE(slot >= 0 && slot < kStatSlots, GKW_E_INTERNAL, "stats slot out of range");
@@ -1419,6 +1439,8 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
     a.glight = j.batch->glight;
     a.mcount = j.batch->mcount;
     a.anyf = j.batch->anyf;
+    a.part_init = j.batch->part_init;
+    a.bnd_init = j.batch->bnd_init;
   }
   if (c->trace) {
     a.trace = c->trace + (size_t)slot * kTraceCap;

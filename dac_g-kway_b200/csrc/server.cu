@@ -22,6 +22,13 @@
 // so small requests are co-scheduled beside a large one without starving it.
 // A job that does not fit an empty device runs anyway and fails with
 // GKW_E_NOMEM if the memory really is not there.
+//
+// Dynamic batching: a slot that takes a small job (up to narrow_max_n
+// vertices, device initial partition) also drains the queued small jobs with
+// the same options, up to batch_max_n vertices together, and partitions them
+// as one disjoint union (batch.cu).  Each graph's result is still exactly its
+// lone result; under load the queue is emptied a batch at a time instead of a
+// graph at a time.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -61,6 +68,7 @@ struct Job {
   std::string err;
   i32 slot = -1;
   i32 n_levels = 0;
+  i32 batch_graphs = 1;     // graphs of the union run this job was part of
   bool done = false;
   Clock::time_point t_submit, t_start, t_end;
 };
@@ -71,7 +79,20 @@ struct Slot {
   bool busy = false;
   i64 held = 0;     // device memory the slot's pools hold
   i64 charge = 0;   // what admission counts for the slot
+  // host staging of a union batch (kept between batches)
+  std::vector<i32> ux, ua, uw, uv, upart, ugp, uk, ulev;
+  std::vector<i64> ucut;
 };
+
+// Options under which two jobs partition identically side by side in a union.
+bool same_options(const gkw_options& a, const gkw_options& b) {
+  return a.eps == b.eps && a.group_cap == b.group_cap && a.threshold_factor == b.threshold_factor &&
+         a.move_cap == b.move_cap && a.init_method == b.init_method && a.seed == b.seed &&
+         a.init_trials == b.init_trials && a.enforce_balance == b.enforce_balance &&
+         a.balance_skip_levels == b.balance_skip_levels && a.coarse_vertex_frac == b.coarse_vertex_frac;
+}
+
+constexpr size_t kMaxUnionJobs = 4096;
 
 }  // namespace
 
@@ -107,9 +128,42 @@ struct gkw_server {
   }
   // Next job for free slot `si` (caller holds mu), or null.
   JobPtr pick(size_t si);
+  // Queued jobs that join `first` in one union run (caller holds mu).
+  std::vector<JobPtr> drain_batch(size_t si, const Job& first);
   void worker(size_t si);
   void run(Slot& s, Job& j);
+  void run_union(Slot& s, std::vector<JobPtr>& jobs);
+  bool batchable(const Job& j) const {
+    return cfg.batch_union && cfg.batch_max_n > 0 && j.opt.init_method == GKW_INIT_DEVICE &&
+           j.host.n <= cfg.narrow_max_n;
+  }
 };
+
+std::vector<JobPtr> gkw_server::drain_batch(size_t si, const Job& first) {
+  std::vector<JobPtr> out;
+  if (!batchable(first) || queue.empty()) return out;
+  const Slot& me = slots[si];
+  const i64 others = total_charge() - me.charge;
+  i64 tn = first.host.n, tm = first.host.m, tk = first.k;
+  for (auto it = queue.begin(); it != queue.end() && out.size() + 1 < kMaxUnionJobs;) {
+    const Job& c = **it;
+    const i64 n2 = tn + c.host.n, m2 = tm + c.host.m, k2 = tk + c.k;
+    const bool ok = batchable(c) && same_options(c.opt, first.opt) && n2 <= cfg.batch_max_n &&
+                    m2 < ((i64)1 << 31) && k2 < ((i64)1 << 20) &&
+                    (running == 0 || others + std::max(me.held, gkw_predict_footprint((i32)n2, m2, (i32)k2)) <=
+                                         cfg.pool_bytes);
+    if (ok) {
+      tn = n2;
+      tm = m2;
+      tk = k2;
+      out.push_back(*it);
+      it = queue.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  return out;
+}
 
 JobPtr gkw_server::pick(size_t si) {
   if (queue.empty()) return nullptr;
@@ -173,28 +227,149 @@ void gkw_server::run(Slot& s, Job& j) {
   }
 }
 
+// Partition jobs[0..] as one disjoint union on slot s.  When the union cannot
+// take them (a malformed graph: an edge out of its own range), every job runs
+// alone and reports its own error.
+void gkw_server::run_union(Slot& s, std::vector<JobPtr>& jobs) {
+  Handle& hh = handle_of(s.h);
+  const i32 G = (i32)jobs.size();
+  bool fallback = false;
+  try {
+    GKW_CUDA(cudaSetDevice(hh.device));
+    i64 tn = 0, tm = 0;
+    bool any_w = false, any_v = false;
+    for (const JobPtr& j : jobs) {
+      tn += j->host.n;
+      tm += j->host.m;
+      any_w |= j->host.adjwgt != nullptr;
+      any_v |= j->host.vwgt != nullptr;
+    }
+    s.ux.resize(tn + 1);
+    s.ua.resize(std::max<i64>(tm, 1));
+    if (any_w) s.uw.resize(std::max<i64>(tm, 1));
+    if (any_v) s.uv.resize(std::max<i64>(tn, 1));
+    s.upart.resize(std::max<i64>(tn, 1));
+    s.ugp.resize(G + 1);
+    s.uk.resize(G);
+    s.ucut.resize(G);
+    s.ulev.resize(G);
+    i64 vo = 0, eo = 0;
+    for (i32 i = 0; i < G; ++i) {
+      const DevGraph& g = jobs[i]->host;
+      const i32 x0 = g.xadj[0];
+      const i64 vb = jobs[i]->vbase;
+      s.ugp[i] = (i32)vo;
+      s.uk[i] = jobs[i]->k;
+      for (i32 v = 0; v < g.n; ++v) s.ux[vo + v] = (i32)(g.xadj[v] - x0 + eo);
+      for (i64 e = 0; e < g.m; ++e) s.ua[eo + e] = (i32)(g.adjncy[e] - vb + vo);
+      if (any_w) {
+        if (g.adjwgt) std::memcpy(s.uw.data() + eo, g.adjwgt, sizeof(i32) * g.m);
+        else std::fill(s.uw.begin() + eo, s.uw.begin() + eo + g.m, 1);
+      }
+      if (any_v) {
+        if (g.vwgt) std::memcpy(s.uv.data() + vo, g.vwgt, sizeof(i32) * g.n);
+        else std::fill(s.uv.begin() + vo, s.uv.begin() + vo + g.n, 1);
+      }
+      vo += g.n;
+      eo += g.m;
+    }
+    s.ux[tn] = (i32)tm;
+    s.ugp[G] = (i32)tn;
+    DevGraph hg;
+    hg.n = (i32)tn;
+    hg.m = tm;
+    hg.xadj = s.ux.data();
+    hg.adjncy = s.ua.data();
+    hg.adjwgt = any_w ? s.uw.data() : nullptr;
+    hg.vwgt = any_v ? s.uv.data() : nullptr;
+    hh.narrow = false;   // one wide grid for the whole union (wide launches take turns)
+    if (partition_batch_union(hh, hg, G, s.ugp.data(), s.uk.data(), jobs[0]->opt, s.upart.data(),
+                              s.ucut.data(), s.ulev.data())) {
+      for (i32 i = 0; i < G; ++i) {
+        Job& j = *jobs[i];
+        if (j.host.n) std::memcpy(j.part_out, s.upart.data() + s.ugp[i], sizeof(i32) * j.host.n);
+        j.cut = s.ucut[i];
+        j.n_levels = s.ulev[i];
+      }
+    } else {
+      fallback = true;
+    }
+  } catch (const Error& e) {
+    if (e.st == GKW_E_INVALID) {
+      fallback = true;
+    } else {
+      for (JobPtr& j : jobs) {
+        j->st = e.st;
+        j->err = e.msg + " (union batch of " + std::to_string(G) + " graphs)";
+      }
+    }
+  } catch (const std::bad_alloc&) {
+    for (JobPtr& j : jobs) {
+      j->st = GKW_E_NOMEM;
+      j->err = "host allocation failed";
+    }
+  }
+  if (fallback || jobs[0]->st != GKW_OK) {
+    cudaStreamSynchronize(hh.stream);
+    cudaGetLastError();
+  }
+  if (fallback) {
+    for (JobPtr& j : jobs) run(s, *j);
+    return;
+  }
+  hh.hier.reset();
+  hh.scratch.reset();
+  const i64 held = (i64)(hh.hier.capacity() + hh.scratch.capacity());
+  if (held > cfg.slot_keep_bytes) {
+    try {
+      hh.hier.trim();
+      hh.scratch.trim();
+    } catch (const Error&) {
+    }
+  }
+}
+
 void gkw_server::worker(size_t si) {
   cudaSetDevice(device);
+  std::vector<JobPtr> jobs;
   for (;;) {
-    JobPtr j;
+    jobs.clear();
     {
       std::unique_lock<std::mutex> lk(mu);
+      JobPtr j;
       for (;;) {
         if (stop) return;
         j = pick(si);
         if (j) break;
         cv_work.wait(lk);
       }
+      jobs.push_back(j);
+      for (JobPtr& c : drain_batch(si, *j)) jobs.push_back(c);
       Slot& s = slots[si];
       s.busy = true;
-      s.charge = std::max(s.held, j->predicted);
+      i64 pred = j->predicted;
+      if (jobs.size() > 1) {
+        i64 tn = 0, tm = 0, tk = 0;
+        for (const JobPtr& c : jobs) {
+          tn += c->host.n;
+          tm += c->host.m;
+          tk += c->k;
+        }
+        pred = gkw_predict_footprint((i32)tn, tm, (i32)std::min<i64>(tk, INT32_MAX));
+      }
+      s.charge = std::max(s.held, pred);
       ++running;
       peak_running = std::max(peak_running, running);
       peak_reserved = std::max(peak_reserved, total_charge());
-      j->slot = (i32)si;
-      j->t_start = Clock::now();
+      const auto now = Clock::now();
+      for (JobPtr& c : jobs) {
+        c->slot = (i32)si;
+        c->t_start = now;
+        c->batch_graphs = (i32)jobs.size();
+      }
     }
-    run(slots[si], *j);
+    if (jobs.size() == 1) run(slots[si], *jobs[0]);
+    else run_union(slots[si], jobs);
     {
       std::lock_guard<std::mutex> lk(mu);
       Slot& s = slots[si];
@@ -203,16 +378,19 @@ void gkw_server::worker(size_t si) {
       s.charge = s.held;
       s.busy = false;
       --running;
-      j->t_end = Clock::now();
-      j->done = true;
-      if (j->st == GKW_OK) {
-        ++completed;
-        latencies.push_back(ms_between(j->t_submit, j->t_end));
-        queue_waits.push_back(ms_between(j->t_submit, j->t_start));
-      } else {
-        ++failed;
+      const auto now = Clock::now();
+      for (JobPtr& j : jobs) {
+        j->t_end = now;
+        j->done = true;
+        if (j->st == GKW_OK) {
+          ++completed;
+          latencies.push_back(ms_between(j->t_submit, j->t_end));
+          queue_waits.push_back(ms_between(j->t_submit, j->t_start));
+        } else {
+          ++failed;
+        }
       }
-      last_done = j->t_end;
+      last_done = now;
     }
     cv_done.notify_all();
     cv_work.notify_all();
@@ -272,6 +450,7 @@ void gkw_server_default_config(gkw_server_config* c) {
   c->max_bypass = 0;   // 0: 4 x slots
   c->narrow_max_n = 262144;
   c->batch_union = 1;
+  c->batch_max_n = 1 << 22;
 }
 
 int64_t gkw_predict_footprint(int32_t n, int64_t nnz, int32_t k) {
@@ -298,6 +477,7 @@ gkw_status gkw_server_create(gkw_server** out, int32_t device, const gkw_server_
     GKW_REQUIRE(c.slots >= 1 && c.slots <= 256, GKW_E_INVALID, "slots must be in [1, 256]");
     GKW_REQUIRE(c.pool_bytes > 0 && c.slot_keep_bytes >= 0, GKW_E_INVALID, "bad memory budget");
     GKW_REQUIRE(c.narrow_max_n >= 0, GKW_E_INVALID, "narrow_max_n must be >= 0");
+    GKW_REQUIRE(c.batch_max_n >= 0, GKW_E_INVALID, "batch_max_n must be >= 0");
     if (c.max_bypass <= 0) c.max_bypass = 4 * c.slots;
     int ndev = 0;
     GKW_CUDA(cudaGetDeviceCount(&ndev));
@@ -413,6 +593,8 @@ gkw_status gkw_server_poll(gkw_server* s, int64_t ticket, int32_t wait_ms, int32
     info->predicted_bytes = j->predicted;
     info->slot = j->slot;
     info->n_levels = j->n_levels;
+    info->batch_graphs = j->batch_graphs;
+    info->reserved = 0;
   }
   if (j->st != GKW_OK) {
     set_error(j->err);

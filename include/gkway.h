@@ -247,10 +247,13 @@ typedef struct gkw_server_config {
   int64_t slot_keep_bytes;   /* memory a slot keeps between jobs (default 256 MiB) */
   int32_t max_bypass;        /* times the oldest waiting job may be overtaken by smaller
                                 jobs that fit when it does not (default 4 x slots) */
-  int32_t batch_union;       /* 1 (default): gkw_partition_batch partitions the whole batch as one
-                                disjoint union when all graphs share the options; 0: one job per
-                                graph on the slots */
-  int32_t reserved[6];
+  int32_t batch_union;       /* 1 (default): graphs that share the options run as one disjoint
+                                union -- a whole gkw_partition_batch call, and queued served
+                                requests of up to narrow_max_n vertices drained together;
+                                0: one job per graph on the slots */
+  int32_t batch_max_n;       /* served requests drained into one union: at most this many
+                                vertices together (default 4194304) */
+  int32_t reserved[5];
 } gkw_server_config;
 
 void gkw_server_default_config(gkw_server_config* cfg);
@@ -276,6 +279,8 @@ typedef struct gkw_request_info {
   int64_t predicted_bytes;
   int32_t slot;
   int32_t n_levels;
+  int32_t batch_graphs;      /* graphs partitioned together with this one as one union (1: alone) */
+  int32_t reserved;
 } gkw_request_info;
 
 gkw_status gkw_server_submit(gkw_server* s, const gkw_csr* graph, int32_t k, const gkw_options* opt,

@@ -75,9 +75,9 @@ def check_batch(pkg, srv, gs, ks, opts=None):
 
 def test_union_batch_matches_alone(pkg, gen):
     """One pipeline over the disjoint union: small graphs that stop coarsening
-    at once (rows in random order), graphs that stop at different depths, k = 1,
-    empty and one-vertex graphs, in both modes and with other balance-skip
-    settings."""
+    at once (rows in random order), graphs that stop at different depths (each
+    union level holds only the graphs still present), k = 1, empty and
+    one-vertex graphs, in both modes and with other balance-skip settings."""
     gs, ks = mixed_graphs(gen)
     for i in (0, 5, 6, 8):
         gs[i] = shuffled_rows(gs[i], 40 + i)
@@ -92,9 +92,10 @@ def test_union_batch_matches_alone(pkg, gen):
     srv.close()
 
 
-def test_union_batch_falls_back_on_duplicate_edges(pkg, gen):
-    # a small graph whose rows hold a duplicate edge cannot be carried verbatim
-    # through the union's levels: the batch runs graph by graph instead
+def test_union_batch_keeps_duplicate_edges(pkg, gen):
+    # a small graph that stops coarsening at its input level, with a duplicated
+    # edge in two rows, beside a graph that coarsens: the small graph is
+    # partitioned on its own rows as given
     g = gen.delaunay(600, 7)
     u = int(g.adjncy[g.xadj[0]])   # edge 0-u listed twice in both rows
     rows = [list(zip(g.adjncy[g.xadj[v]:g.xadj[v + 1]], g.adjwgt[g.xadj[v]:g.xadj[v + 1]])) for v in range(g.n)]
@@ -178,6 +179,39 @@ def test_served_matches_alone_under_load(pkg, gen):
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
     assert st["graphs_per_s"] > 0
     assert srv.stats()["completed"] == 0
+    srv.close()
+
+
+def test_served_requests_drained_as_unions(pkg, gen):
+    """Small requests queued faster than they run are drained into union runs;
+    each result is still the graph's lone result.  A malformed request among
+    them fails alone."""
+    rng = np.random.default_rng(5)
+    gs, ks = [], []
+    for i in range(48):
+        n = int(rng.integers(500, 6000))
+        gs.append(gen.delaunay(n, 300 + i) if i % 2 else gen.grid27(8, 8, max(2, n // 64)))
+        ks.append(int(rng.choice([2, 4, 8, 16])))
+    ref = alone(pkg, gs, ks)
+    bad = gen.delaunay(700, 9)
+    bad_a = bad.adjncy.copy()
+    bad_a[3] = bad.n + 50                    # neighbour id outside the graph
+    srv = pkg.Server(0, slots=2)
+    tickets = [srv.submit(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k) for g, k in zip(gs[:24], ks[:24])]
+    t_bad = srv.submit(bad.xadj, bad_a, bad.adjwgt, bad.vwgt, 4)
+    tickets += [srv.submit(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k) for g, k in zip(gs[24:], ks[24:])]
+    sizes = []
+    for i, t in enumerate(tickets):
+        part, cut, info = srv.poll(t, gs[i].n, wait_ms=-1)
+        assert np.array_equal(part, ref[i][0]), i
+        assert cut == ref[i][1], i
+        assert info["n_levels"] >= 1
+        sizes.append(info["batch_graphs"])
+    with pytest.raises(pkg.GkwError):
+        srv.poll(t_bad, bad.n, wait_ms=-1)
+    assert max(sizes) > 1                    # some requests ran together
+    st = srv.stats()
+    assert st["completed"] == len(gs) and st["failed"] == 1
     srv.close()
 
 
