@@ -706,7 +706,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "configs"])
     ap.add_argument("--graphs", type=int, default=4096, help="batched: number of graphs")
-    ap.add_argument("--slots", type=int, default=8, help="batched/served: concurrent partitions")
+    ap.add_argument("--slots", type=int, default=2, help="batched/served: concurrent partitions")
     ap.add_argument("--pool", type=int, default=48, help="served: distinct graphs requests draw from")
     ap.add_argument("--max-n", type=int, default=2000000, help="served: largest graph")
     ap.add_argument("--rates", default="10,100,500,2000", help="served: offered loads (requests/s)")

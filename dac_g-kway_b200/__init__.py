@@ -126,7 +126,8 @@ class ServerConfig(ctypes.Structure):
         ("max_bypass", ctypes.c_int32),
         ("batch_union", ctypes.c_int32),
         ("batch_max_n", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("batch_graph_max_n", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 

@@ -84,108 +84,104 @@ struct LocalTopo {
   const i32* vw;     // vertex weight
 };
 
+// Growth keys of one trial: K[i] = grow_key of unassigned member i (0 once
+// assigned), B1[b] = max of K over members [32b, 32b + 32), B2[c] = max of B1
+// over blocks [32c, 32c + 32).  A key only rises while its member is
+// unassigned (conn only grows), so updates are atomic maxima; assigning a
+// member recomputes its two blocks.  The argmax over all unassigned members
+// is then a scan of B2.
 struct TrialState {
   i32* C;      // connection weight to the region R
   i32* R;      // in R
-  i32* F;      // frontier list
-  i32* posF;   // position in F
+  u64* K;
+  u64* B1;
+  u64* B2;
 };
+
+__host__ __device__ __forceinline__ i32 gggp_nb1(i32 s) { return (s + 31) >> 5; }
+__host__ __device__ __forceinline__ i32 gggp_nb2(i32 s) { return (s + 1023) >> 10; }
+// i32 words of one trial's state in shared memory (C, R, K, B1, B2; even, so
+// every trial's u64 arrays stay 8-byte aligned)
+__host__ __device__ __forceinline__ i32 gggp_state_words(i32 s) {
+  return 2 * s + 2 * s + 2 * gggp_nb1(s) + 2 * gggp_nb2(s) + ((2 * s) & 1);
+}
 
 // Refinement moves of one trial: s/4 + 32, at most 256 (each move scans the
 // whole sub-problem).
 __host__ __device__ __forceinline__ i32 gggp_max_moves(i32 s) { return s / 4 + 32 < 256 ? s / 4 + 32 : 256; }
 
-// Sub-problems above this size get their members sorted by (degS, index) once:
-// while the frontier is empty every unassigned member has conn = 0, so the
-// growth key's best is the first unassigned member in that order, and the
-// step walks a pointer instead of scanning all members.
-constexpr i32 kGggpOrderMin = 2048;
-
 // One GGGP trial by one warp (growth then positive-gain refinement); see the
 // file comment for the rules.  Returns the trial's cut and |W(R) - TL|.
 __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL, i64 WS, i64 capL,
-                           i64 capR, const i32* order, i64& cut_out, i64& dev_out) {
+                           i64 capR, i64& cut_out, i64& dev_out) {
   const int lane = threadIdx.x & 31;
   i32* C = S.C;
   i32* R = S.R;
-  i32* F = S.F;
-  i32* posF = S.posF;
+  u64* K = S.K;
+  u64* B1 = S.B1;
+  u64* B2 = S.B2;
+  const i32 nb1 = gggp_nb1(s), nb2 = gggp_nb2(s);
   for (i32 i = lane; i < s; i += 32) {
     R[i] = 0;
     C[i] = 0;
+    K[i] = grow_key(false, -T.degS[i], i);
+  }
+  __syncwarp();
+  for (i32 b = lane; b < nb1; b += 32) {
+    u64 m = 0;
+    for (i32 i = b << 5; i < s && i < (b + 1) << 5; ++i) m = m > K[i] ? m : K[i];
+    B1[b] = m;
+  }
+  __syncwarp();
+  for (i32 c = lane; c < nb2; c += 32) {
+    u64 m = 0;
+    for (i32 b = c << 5; b < nb1 && b < (c + 1) << 5; ++b) m = m > B1[b] ? m : B1[b];
+    B2[c] = m;
   }
   __syncwarp();
   i64 wR = 0;
-  i32 nF = 0;
-  i32 nxt = 0;   // pointer into order (empty-frontier steps)
-  // ---- growth: F = members outside R with conn > 0; a frontier member
-  // always outranks a non-frontier one, so the argmax over F equals the argmax
-  // over all unassigned members, and the full scan is only needed when F is
-  // empty
+  // ---- growth: the unassigned member with the largest key (a member joined
+  // to the region outranks every other; then gain, then smaller index)
   for (i32 step = 0; step < s; ++step) {
     if (step > 0) {
       u64 best = 0;
-      if (nF > 0) {
-        for (i32 f = lane; f < nF; f += 32) {
-          const i32 i = F[f];
-          const i32 c = C[i];
-          const u64 key = grow_key(true, 2 * c - T.degS[i], i);
-          best = best > key ? best : key;
-        }
-      } else if (order) {
-        // empty frontier: the first unassigned member in (degS, index) order
-        // (assigned members never return, so the pointer only moves forward)
-        while (nxt < s && R[order[nxt]]) ++nxt;
-        if (nxt < s) best = grow_key(false, -T.degS[order[nxt]], order[nxt]);
-      } else {
-        for (i32 i = lane; i < s; i += 32) {
-          if (!R[i]) {
-            const i32 c = C[i];
-            const u64 key = grow_key(c > 0, 2 * c - T.degS[i], i);
-            best = best > key ? best : key;
-          }
-        }
-      }
+      for (i32 c = lane; c < nb2; c += 32) best = best > B2[c] ? best : B2[c];
       best = warp_max_u64(best);
       if (best == 0) break;
       pick = key_idx(best);
       const i64 vw = (u32)T.vw[pick];
       if (wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
     }
-    const i32 cp = C[pick];
     if (lane == 0) {
       R[pick] = 1;
-      if (cp > 0) {   // leave the frontier (swap-remove)
-        const i32 at = posF[pick];
-        const i32 last = F[nF - 1];
-        F[at] = last;
-        posF[last] = at;
-      }
+      K[pick] = 0;
     }
-    if (cp > 0) --nF;
     wR += (u32)T.vw[pick];
     __syncwarp();
     const i32 rb = T.rb[pick], rn = T.rn[pick];
-    for (i32 j0 = 0; j0 < rn; j0 += 32) {
-      const i32 j = j0 + lane;
-      bool join = false;
-      i32 u = 0;
-      if (j < rn) {
-        u = T.nb[rb + j];
-        const i32 w = T.nw[rb + j];
-        const i32 old = C[u];
-        C[u] = old + w;
-        join = !R[u] && old <= 0 && old + w > 0;
+    for (i32 j = lane; j < rn; j += 32) {
+      const i32 u = T.nb[rb + j];
+      const i32 w = T.nw[rb + j];
+      const i32 c = atomicAdd(&C[u], w) + w;
+      if (!R[u]) {
+        const unsigned long long key = grow_key(c > 0, 2 * c - T.degS[u], u);
+        atomicMax(reinterpret_cast<unsigned long long*>(&K[u]), key);
+        atomicMax(reinterpret_cast<unsigned long long*>(&B1[u >> 5]), key);
+        atomicMax(reinterpret_cast<unsigned long long*>(&B2[u >> 10]), key);
       }
-      const u32 m = __ballot_sync(kFull32, join);
-      if (join) {
-        const i32 at = nF + __popc(m & ((1u << lane) - 1));
-        F[at] = u;
-        posF[u] = at;
-      }
-      nF += __popc(m);
     }
     __syncwarp();
+    // the picked member leaves its blocks
+    {
+      const i32 b = pick >> 5, i = (b << 5) + lane;
+      const u64 m = warp_max_u64(i < s ? K[i] : 0ull);
+      if (lane == 0) B1[b] = m;
+      __syncwarp();
+      const i32 c = pick >> 10, bb = (c << 5) + lane;
+      const u64 m2 = warp_max_u64(bb < nb1 ? B1[bb] : 0ull);
+      if (lane == 0) B2[c] = m2;
+      __syncwarp();
+    }
     if (wR >= TL) break;
   }
   // ---- refinement: positive-gain moves within the side caps ----
@@ -265,8 +261,8 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     const i32* __restrict__ vwgt, const i32* __restrict__ lo, const i32* __restrict__ hi,
     const i32* __restrict__ cnt, const i32* __restrict__ off, i32* __restrict__ mlist, i32* __restrict__ loc,
     i32* __restrict__ lo_out, i32* __restrict__ hi_out, u64 seed, double eps, i32 trials,
-    i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state, i32* g_order,
-    u64* g_okeys, const i32* __restrict__ part_base, const i32* __restrict__ part_v0,
+    i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state, u64* g_keys,
+    u64* g_b1, u64* g_b2, size_t b1_stride, size_t b2_stride, const i32* __restrict__ part_base, const i32* __restrict__ part_v0,
     const i32* __restrict__ part_v1) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_cnt;
@@ -348,7 +344,8 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   const i64 capL = (i64)((double)TL * (1.0 + eps * 0.5));
   const i64 capR = (i64)((double)(WS - TL) * (1.0 + eps * 0.5));
   // shared memory when the local CSR and the trials' state fit
-  const size_t need = sizeof(i32) * ((size_t)4 * s + 2 * (size_t)ES + (size_t)4 * s * trials);
+  const i32 stw = gggp_state_words(s);
+  const size_t need = sizeof(i32) * ((size_t)4 * s + 2 * (size_t)ES + (size_t)stw * trials);
   const bool in_smem = need <= kGggpSmem;   // block-uniform
   LocalTopo T;
   i32 *rb, *rn, *deg, *vw, *nb, *nw, *state;
@@ -400,53 +397,32 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   T.nw = nw;
   T.degS = deg;
   T.vw = vw;
-  // large sub-problems: members in (degS, index) order for empty-frontier steps
-  const i32* order = nullptr;
-  if (s > kGggpOrderMin) {   // block-uniform
-    i64 P = 1;
-    while (P < s) P <<= 1;
-    u64* a = g_okeys + 2 * (i64)base_off;   // P <= 2s keys; sub-problems' ranges are disjoint
-    for (i64 i = threadIdx.x; i < P; i += blockDim.x)
-      a[i] = i < s ? (((u64)(u32)deg[i] << 32) | (u32)i) : ~0ull;
-    __syncthreads();
-    for (i64 kk = 2; kk <= P; kk <<= 1)
-      for (i64 j = kk >> 1; j > 0; j >>= 1) {
-        for (i64 i = threadIdx.x; i < P; i += blockDim.x) {
-          const i64 l = i ^ j;
-          if (l > i) {
-            const u64 x = a[i], y = a[l];
-            const bool up = (i & kk) == 0;
-            if (up ? (x > y) : (x < y)) { a[i] = y; a[l] = x; }
-          }
-        }
-        __syncthreads();
-      }
-    i32* o = g_order + base_off;
-    for (i32 i = threadIdx.x; i < s; i += blockDim.x) o[i] = (i32)(u32)a[i];
-    __syncthreads();
-    order = o;
-  }
   const i32 t = wid;
   if (t < trials) {
     TrialState S;
     if (in_smem) {
-      i32* q = state + (size_t)t * 4 * s;
+      i32* q = state + (size_t)t * stw;   // [C | R | K | B1 | B2]
       S.C = q;
       S.R = q + s;
-      S.F = q + 2 * s;
-      S.posF = q + 3 * s;
+      S.K = reinterpret_cast<u64*>(q + 2 * s);
+      S.B1 = S.K + s;
+      S.B2 = S.B1 + gggp_nb1(s);
     } else {
-      i32* q = g_state + (size_t)t * 4 * n;   // [C | R | F | posF] of n each, this sub-problem at base_off
+      // [C | R] of n each per trial, this sub-problem at base_off; key blocks
+      // at base_off / 32 + p0 and base_off / 1024 + p0 (disjoint across the
+      // sub-problems, which lie in part order)
+      i32* q = g_state + (size_t)t * 2 * n;
       S.C = q + base_off;
       S.R = q + n + base_off;
-      S.F = q + 2 * (size_t)n + base_off;
-      S.posF = q + 3 * (size_t)n + base_off;
+      S.K = g_keys + (size_t)t * n + base_off;
+      S.B1 = g_b1 + (size_t)t * b1_stride + (base_off >> 5) + p0;
+      S.B2 = g_b2 + (size_t)t * b2_stride + (base_off >> 10) + p0;
     }
     // the seed names the part by its own graph's id (batched levels: parts are global)
     const i32 p0_local = part_base ? p0 - part_base[p0] : p0;
     const i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0_local * 1315423911ull + (u64)t) % (u32)s);
     i64 cut, dev;
-    gggp_trial(T, S, s, pick, TL, WS, capL, capR, order, cut, dev);
+    gggp_trial(T, S, s, pick, TL, WS, capL, capR, cut, dev);
     if (lane == 0) {
       s_cut[t] = cut;
       s_dev[t] = dev;
@@ -460,7 +436,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     s_best = b;
   }
   __syncthreads();
-  const i32* Rb = in_smem ? state + (size_t)s_best * 4 * s + s : g_state + (size_t)s_best * 4 * n + n + base_off;
+  const i32* Rb = in_smem ? state + (size_t)s_best * stw + s : g_state + (size_t)s_best * 2 * n + n + base_off;
   for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
     const i32 v = M[i];
     if (Rb[i]) { lo_out[v] = p0; hi_out[v] = pm; }
@@ -501,9 +477,12 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   i32* g_vw = h.scratch.alloc_n<i32>(n);
   i32* g_nb = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
   i32* g_nw = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
-  i32* g_state = h.scratch.alloc_n<i32>((size_t)kInitTrials * 4 * n);
-  i32* g_order = h.scratch.alloc_n<i32>(n);
-  u64* g_okeys = h.scratch.alloc_n<u64>(2 * (size_t)n);
+  i32* g_state = h.scratch.alloc_n<i32>((size_t)kInitTrials * 2 * n);
+  u64* g_keys = h.scratch.alloc_n<u64>((size_t)kInitTrials * n);
+  // key blocks: sub-problem p0 at offset base_off uses [base_off/32 + p0, + ceil(s/32))
+  const size_t b1_stride = (size_t)n / 32 + (size_t)k + 2, b2_stride = (size_t)n / 1024 + (size_t)k + 2;
+  u64* g_b1 = h.scratch.alloc_n<u64>((size_t)kInitTrials * b1_stride);
+  u64* g_b2 = h.scratch.alloc_n<u64>((size_t)kInitTrials * b2_stride);
   GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
   const u32 nb = ceil_div(n, 256);
   i32 depth = 0;
@@ -530,7 +509,7 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     exclusive_scan_i32(h, cnt, off, k, nullptr);
     launch(k_gggp_depth, k, kInitTrials * 32, kGggpSmem, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a],
            hi[a], cnt, off, mlist, loc, lo[b], hi[b], seed, eps, trials, g_rb, g_rn, g_deg, g_vw, g_nb, g_nw,
-           g_state, g_order, g_okeys, batch ? batch->part_base : (const i32*)nullptr,
+           g_state, g_keys, g_b1, g_b2, b1_stride, b2_stride, batch ? batch->part_base : (const i32*)nullptr,
            batch ? batch->part_v0 : (const i32*)nullptr, batch ? batch->part_v1 : (const i32*)nullptr);
     GKW_CHECK_LAUNCH();
     if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));

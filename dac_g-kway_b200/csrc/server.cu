@@ -23,7 +23,7 @@
 // A job that does not fit an empty device runs anyway and fails with
 // GKW_E_NOMEM if the memory really is not there.
 //
-// Dynamic batching: a slot that takes a small job (up to narrow_max_n
+// Dynamic batching: a slot that takes a small job (up to batch_graph_max_n
 // vertices, device initial partition) also drains the queued small jobs with
 // the same options, up to batch_max_n vertices together, and partitions them
 // as one disjoint union (batch.cu).  Each graph's result is still exactly its
@@ -135,7 +135,7 @@ struct gkw_server {
   void run_union(Slot& s, std::vector<JobPtr>& jobs);
   bool batchable(const Job& j) const {
     return cfg.batch_union && cfg.batch_max_n > 0 && j.opt.init_method == GKW_INIT_DEVICE &&
-           j.host.n <= cfg.narrow_max_n;
+           j.host.n <= cfg.batch_graph_max_n;
   }
 };
 
@@ -444,13 +444,14 @@ extern "C" {
 void gkw_server_default_config(gkw_server_config* c) {
   if (!c) return;
   memset(c, 0, sizeof(*c));
-  c->slots = 8;
+  c->slots = 2;
   c->pool_bytes = (int64_t)64 << 30;
-  c->slot_keep_bytes = (int64_t)256 << 20;
+  c->slot_keep_bytes = (int64_t)4 << 30;
   c->max_bypass = 0;   // 0: 4 x slots
   c->narrow_max_n = 262144;
   c->batch_union = 1;
   c->batch_max_n = 1 << 22;
+  c->batch_graph_max_n = 262144;
 }
 
 int64_t gkw_predict_footprint(int32_t n, int64_t nnz, int32_t k) {

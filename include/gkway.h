@@ -237,23 +237,25 @@ float gkw_max_part_weight(int64_t total_vwgt, int32_t k, double eps);
 typedef struct gkw_server gkw_server;
 
 typedef struct gkw_server_config {
-  int32_t slots;             /* concurrent partitions (default 8) */
+  int32_t slots;             /* concurrent partitions (default 2) */
   int32_t narrow_max_n;      /* jobs up to this many vertices run their barrier kernels as
                                 one thread-block cluster each, so any number of them can
                                 share the device; larger jobs take turns for their wide
                                 grids (default 262144) */
   int64_t pool_bytes;        /* device-memory budget of all slots together (default 64 GiB,
                                 capped at 90% of the free memory at creation) */
-  int64_t slot_keep_bytes;   /* memory a slot keeps between jobs (default 256 MiB) */
+  int64_t slot_keep_bytes;   /* memory a slot keeps between jobs (default 4 GiB) */
   int32_t max_bypass;        /* times the oldest waiting job may be overtaken by smaller
                                 jobs that fit when it does not (default 4 x slots) */
   int32_t batch_union;       /* 1 (default): graphs that share the options run as one disjoint
                                 union -- a whole gkw_partition_batch call, and queued served
-                                requests of up to narrow_max_n vertices drained together;
+                                requests of up to batch_graph_max_n vertices drained together;
                                 0: one job per graph on the slots */
   int32_t batch_max_n;       /* served requests drained into one union: at most this many
                                 vertices together (default 4194304) */
-  int32_t reserved[5];
+  int32_t batch_graph_max_n; /* served requests of up to this many vertices join unions
+                                (default 262144) */
+  int32_t reserved[4];
 } gkw_server_config;
 
 void gkw_server_default_config(gkw_server_config* cfg);
