@@ -110,10 +110,84 @@ __host__ __device__ __forceinline__ i32 gggp_state_words(i32 s) {
 // whole sub-problem).
 __host__ __device__ __forceinline__ i32 gggp_max_moves(i32 s) { return s / 4 + 32 < 256 ? s / 4 + 32 : 256; }
 
-// One GGGP trial by one warp (growth then positive-gain refinement); see the
-// file comment for the rules.  Returns the trial's cut and |W(R) - TL|.
-__device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL, i64 WS, i64 capL,
-                           i64 capR, i64& cut_out, i64& dev_out) {
+// Growth of small sub-problems: F = members outside R with conn > 0; a
+// frontier member always outranks a non-frontier one, so the argmax over F
+// equals the argmax over all unassigned members, and the full scan is only
+// needed when F is empty.  F and posF use the trial's key array.  Returns W(R).
+__device__ i64 grow_scan(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL) {
+  const int lane = threadIdx.x & 31;
+  i32* C = S.C;
+  i32* R = S.R;
+  i32* F = reinterpret_cast<i32*>(S.K);
+  i32* posF = F + s;
+  i64 wR = 0;
+  i32 nF = 0;
+  for (i32 step = 0; step < s; ++step) {
+    if (step > 0) {
+      u64 best = 0;
+      if (nF > 0) {
+        for (i32 f = lane; f < nF; f += 32) {
+          const i32 i = F[f];
+          const i32 c = C[i];
+          const u64 key = grow_key(true, 2 * c - T.degS[i], i);
+          best = best > key ? best : key;
+        }
+      } else {
+        for (i32 i = lane; i < s; i += 32) {
+          if (!R[i]) {
+            const i32 c = C[i];
+            const u64 key = grow_key(c > 0, 2 * c - T.degS[i], i);
+            best = best > key ? best : key;
+          }
+        }
+      }
+      best = warp_max_u64(best);
+      if (best == 0) break;
+      pick = key_idx(best);
+      const i64 vw = (u32)T.vw[pick];
+      if (wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
+    }
+    const i32 cp = C[pick];
+    if (lane == 0) {
+      R[pick] = 1;
+      if (cp > 0) {   // leave the frontier (swap-remove)
+        const i32 at = posF[pick];
+        const i32 last = F[nF - 1];
+        F[at] = last;
+        posF[last] = at;
+      }
+    }
+    if (cp > 0) --nF;
+    wR += (u32)T.vw[pick];
+    __syncwarp();
+    const i32 rb = T.rb[pick], rn = T.rn[pick];
+    for (i32 j0 = 0; j0 < rn; j0 += 32) {
+      const i32 j = j0 + lane;
+      bool join = false;
+      i32 u = 0;
+      if (j < rn) {
+        u = T.nb[rb + j];
+        const i32 w = T.nw[rb + j];
+        const i32 old = atomicAdd(&C[u], w);   // a row may list a neighbour twice
+        join = !R[u] && old <= 0 && old + w > 0;
+      }
+      const u32 m = __ballot_sync(kFull32, join);
+      if (join) {
+        const i32 at = nF + __popc(m & ((1u << lane) - 1));
+        F[at] = u;
+        posF[u] = at;
+      }
+      nF += __popc(m);
+    }
+    __syncwarp();
+    if (wR >= TL) break;
+  }
+  return wR;
+}
+
+// Growth of large sub-problems over the block maxima of the growth keys
+// (TrialState); the same picks as grow_scan.  Returns W(R).
+__device__ i64 grow_blocks(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL) {
   const int lane = threadIdx.x & 31;
   i32* C = S.C;
   i32* R = S.R;
@@ -121,11 +195,7 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
   u64* B1 = S.B1;
   u64* B2 = S.B2;
   const i32 nb1 = gggp_nb1(s), nb2 = gggp_nb2(s);
-  for (i32 i = lane; i < s; i += 32) {
-    R[i] = 0;
-    C[i] = 0;
-    K[i] = grow_key(false, -T.degS[i], i);
-  }
+  for (i32 i = lane; i < s; i += 32) K[i] = grow_key(false, -T.degS[i], i);
   __syncwarp();
   for (i32 b = lane; b < nb1; b += 32) {
     u64 m = 0;
@@ -140,8 +210,6 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
   }
   __syncwarp();
   i64 wR = 0;
-  // ---- growth: the unassigned member with the largest key (a member joined
-  // to the region outranks every other; then gain, then smaller index)
   for (i32 step = 0; step < s; ++step) {
     if (step > 0) {
       u64 best = 0;
@@ -184,6 +252,26 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
     }
     if (wR >= TL) break;
   }
+  return wR;
+}
+
+// Sub-problems above this size grow over block maxima; smaller ones scan
+// their (small) frontier, which is cheaper per step.
+constexpr i32 kGggpBlockMin = 2048;
+
+// One GGGP trial by one warp (growth then positive-gain refinement); see the
+// file comment for the rules.  Returns the trial's cut and |W(R) - TL|.
+__device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL, i64 WS, i64 capL,
+                           i64 capR, i64& cut_out, i64& dev_out) {
+  const int lane = threadIdx.x & 31;
+  i32* C = S.C;
+  i32* R = S.R;
+  for (i32 i = lane; i < s; i += 32) {
+    R[i] = 0;
+    C[i] = 0;
+  }
+  __syncwarp();
+  i64 wR = s > kGggpBlockMin ? grow_blocks(T, S, s, pick, TL) : grow_scan(T, S, s, pick, TL);
   // ---- refinement: positive-gain moves within the side caps ----
   const i32 max_moves = gggp_max_moves(s);
   for (i32 mv = 0; mv < max_moves; ++mv) {

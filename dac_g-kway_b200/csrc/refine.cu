@@ -28,6 +28,12 @@ static constexpr u32 kFullMask = 0xffffffffu;
 constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pass
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
 constexpr int kLevelThreads = 512;
+// Level-kernel CTAs: one per kLevelVertsPerCta vertices of the level, at
+// least kLevelMinCtas.  Every phase of a round is a chain of dependent loads
+// per vertex, so even small levels run faster spread over many warps than
+// on the cheaper barrier of a few CTAs.
+constexpr i32 kLevelVertsPerCta = 512;
+constexpr i32 kLevelMinCtas = 32;
 constexpr i32 kGreedySmemParts = 4096;   // balance greedy pass: part weights in smem up to this k
 constexpr i32 kGreedyWords = 3 * kMaxMoveCap + kGreedySmemParts;
 static_assert((size_t)kGreedyWords * 4 >= (size_t)kSortMax * 8, "the sort's second buffer aliases the greedy region");
@@ -1447,10 +1453,8 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
     a.trace_cap = kTraceCap;
     a.trace_n = c->trace_n + slot;
   }
-  // small levels use fewer CTAs: the barrier gets cheaper and the work fits;
-  // at least enough CTAs for the per-part checks to run in few passes
-  i32 grid = (i32)ceil_div(std::max(g.n, 1), 512);
-  grid = std::max(grid, std::max(32, c->kacc / 4));
+  i32 grid = (i32)ceil_div(std::max(g.n, 1), kLevelVertsPerCta);
+  grid = std::max(grid, std::max(kLevelMinCtas, c->kacc / 4));   // large k: few gain-update warps per CTA
   grid = std::min(grid, c->grid);
   grid = coop_grid(h, (const void*)k_level, grid, kLevelThreads, c->smem);
   void* args[] = {&a};
