@@ -26,6 +26,7 @@ namespace gkw {
 
 static constexpr u32 kFullMask = 0xffffffffu;
 constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pass
+constexpr i32 kSelBins = 2048;      // histogram bins of the threshold search above kSortMax
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
 constexpr int kLevelThreads = 512;
 // Level-kernel CTAs: one per kLevelVertsPerCta vertices of the level, at
@@ -59,6 +60,7 @@ struct RoundState {
   i32 light;
   u32 epoch;
   u64 rows;   // adjacency entries read by the gain updates of the rounds
+  i64 cand_sum;   // refinement candidates over the rounds (diagnostic)
 };
 
 
@@ -68,6 +70,7 @@ struct LevelStatsDev {
   i64 rows;
   i32 err;
   i32 pad;
+  i64 cand_sum;
 };
 
 struct RefineCtx {
@@ -666,26 +669,6 @@ __device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u3
 __device__ i32 select_sort(const LevelArgs& a, const u64* cands, i32 cnt, u64* s, i32* greedy) {
   const i32 cap = a.move_cap;
   const i32 B = cnt < cap ? cnt : cap;
-  // Element i is owned by thread i mod blockDim; for strides j < 32 both
-  // elements of a pair belong to one warp.
-  auto bitonic = [&](i32 P) {
-    for (i32 kk = 2; kk <= P; kk <<= 1)
-      for (i32 j = kk >> 1; j > 0; j >>= 1) {
-        for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
-          const i32 l = i ^ j;
-          if (l > i) {
-            const u64 x = s[i], y = s[l];
-            const bool up = (i & kk) == 0;
-            if (up ? (x > y) : (x < y)) { s[i] = y; s[l] = x; }
-          }
-        }
-        // a block barrier is needed when this stage or the next one pairs
-        // elements of different warps: j >= 32 now, or the next stage is
-        // (2kk, kk) with kk >= 32
-        if (j >= 32 || (j == 1 && kk >= 32)) __syncthreads();
-        else __syncwarp();
-      }
-  };
   if (cnt <= kSortMax) {
     i32 P = 32;
     while (P < cnt) P <<= 1;
@@ -698,18 +681,131 @@ __device__ i32 select_sort(const LevelArgs& a, const u64* cands, i32 cnt, u64* s
       __syncthreads();
     }
   } else {
-    i32 next = 0;
-    bool first = true;
-    while (next < cnt) {
-      const i32 lo = first ? 0 : cap;
-      for (i32 i = lo + threadIdx.x; i < kSortMax; i += blockDim.x) {
-        const i32 src = next + (i - lo);
-        s[i] = src < cnt ? ldc(cands + src) : ~0ull;
+    // More than kSortMax candidates: narrow a key threshold T with
+    // B <= #(keys <= T) <= kSortMax by histogram passes over the keys, then
+    // sort the keys <= T.  Keys are distinct (one per vertex), so the first B
+    // of that sort are the first B of all.
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    u32* hist = reinterpret_cast<u32*>(greedy);   // kSelBins counters (free until the sort below)
+    __shared__ u64 s_mn[32], s_mx[32];
+    __shared__ u64 s_lo, s_hi, s_T;
+    __shared__ u32 s_warp[33];
+    __shared__ i32 s_below, s_cum, s_bin, s_fill;
+    u64 mn = ~0ull, mx = 0;
+    for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const u64 k = ldc(cands + i);
+      mn = k < mn ? k : mn;
+      mx = k > mx ? k : mx;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const u64 y = __shfl_xor_sync(kFullMask, mn, o), z = __shfl_xor_sync(kFullMask, mx, o);
+      mn = y < mn ? y : mn;
+      mx = z > mx ? z : mx;
+    }
+    if (lane == 0) {
+      s_mn[wid] = mn;
+      s_mx[wid] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < nw; ++w) {
+        mn = s_mn[w] < mn ? s_mn[w] : mn;
+        mx = s_mx[w] > mx ? s_mx[w] : mx;
       }
-      next += kSortMax - lo;
-      first = false;
+      s_lo = mn;
+      s_hi = mx;
+      s_below = 0;
+      s_T = mx;
+    }
+    __syncthreads();
+    // every pass leaves one bin of the last: at least 11 bits fewer to
+    // resolve, so 6 passes reach single keys
+    for (i32 pass = 0; pass < 8; ++pass) {
+      const u64 lo = s_lo, hi = s_hi;
+      const i32 below = s_below;
+      if (threadIdx.x == 0) {
+        s_bin = 0;
+        s_cum = below;
+      }
+      i32 sft = 0;
+      while (((hi - lo) >> sft) >= (u64)kSelBins) ++sft;
+      for (i32 b = threadIdx.x; b < kSelBins; b += blockDim.x) hist[b] = 0;
       __syncthreads();
-      bitonic(kSortMax);
+      for (i32 base = 0; base < cnt; base += blockDim.x) {   // warp-uniform trip count
+        const i32 i = base + threadIdx.x;
+        u32 bin = 0xffffffffu;
+        if (i < cnt) {
+          const u64 k = ldc(cands + i);
+          if (k >= lo && k <= hi) bin = (u32)((k - lo) >> sft);
+        }
+        const u32 same = __match_any_sync(kFullMask, bin);   // lanes of one bin add once
+        if (bin != 0xffffffffu && lane == __ffs(same) - 1) atomicAdd(&hist[bin], (u32)__popc(same));
+      }
+      __syncthreads();
+      // first bin where below + (inclusive count) reaches B
+      constexpr i32 kPer = kSelBins / kLevelThreads;
+      const i32 b0 = threadIdx.x * kPer;
+      u32 loc = 0;
+      for (i32 j = 0; j < kPer; ++j) loc += hist[b0 + j];
+      u32 tot;
+      u32 run = (u32)below + block_exscan_u32(loc, s_warp, tot);
+      for (i32 j = 0; j < kPer; ++j) {
+        const u32 h = hist[b0 + j];
+        if (run < (u32)B && run + h >= (u32)B) {   // exactly one bin
+          s_bin = b0 + j;
+          s_cum = (i32)run;
+        }
+        run += h;
+      }
+      __syncthreads();
+      const i32 b = s_bin, cum = s_cum;
+      const u32 hb = hist[b];
+      const bool last = (u64)b == ((hi - lo) >> sft);
+      const u64 top = last ? hi : lo + ((u64)(b + 1) << sft) - 1;   // no overflow below the last bin
+      __syncthreads();
+      if ((i64)cum + hb <= (i64)kSortMax) {
+        if (threadIdx.x == 0) s_T = top;
+        __syncthreads();
+        break;
+      }
+      if (threadIdx.x == 0) {
+        s_lo = lo + ((u64)b << sft);
+        s_hi = top;
+        s_below = cum;
+        s_T = top;
+      }
+      __syncthreads();
+    }
+    // keep the keys <= T
+    if (threadIdx.x == 0) s_fill = 0;
+    __syncthreads();
+    const u64 T = s_T;
+    for (i32 base = 0; base < cnt; base += blockDim.x) {
+      const i32 i = base + threadIdx.x;
+      u64 k = 0;
+      bool keep = false;
+      if (i < cnt) {
+        k = ldc(cands + i);
+        keep = k <= T;
+      }
+      const u32 m = __ballot_sync(kFullMask, keep);
+      i32 at = 0;
+      if (lane == 0 && m) at = atomicAdd(&s_fill, __popc(m));
+      at = __shfl_sync(kFullMask, at, 0);
+      const i32 pos = at + __popc(m & ((1u << lane) - 1));
+      if (keep && pos < kSortMax) s[pos] = k;   // the threshold keeps at most kSortMax keys
+    }
+    __syncthreads();
+    const i32 nk = s_fill < kSortMax ? s_fill : kSortMax;
+    i32 P = 32;
+    while (P < nk) P <<= 1;
+    for (i32 i = nk + threadIdx.x; i < P; i += blockDim.x) s[i] = ~0ull;
+    __syncthreads();
+    u64* t = reinterpret_cast<u64*>(greedy);
+    if (block_merge_sort(s, t, P) == t) {
+      for (i32 i = threadIdx.x; i < B; i += blockDim.x) s[i] = t[i];
+      __syncthreads();
     }
   }
   return B;
@@ -769,8 +865,11 @@ __device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, 
   }
   const i32 B = select_sort(a, a.cands, cnt, s, greedy);
   if (!balance_mode) {
+    trace_mark(a, 25);
+    if (threadIdx.x == 0) st->cand_sum += cnt;
     for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
     const i32 pos = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp);
+    trace_mark(a, 26);
     if (threadIdx.x == 0) st->pos = pos;
   } else {
     const i32 nsel = select_greedy(a, s, greedy, B, 0, a.k);
@@ -1219,6 +1318,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
     o->brounds = ldc(&st->brounds);
     o->bmoves = ldc(&st->bmoves);
     o->rows = (i64)ldc(&st->rows);
+    o->cand_sum = ldc(&st->cand_sum);
     o->err = *(volatile i32*)a.err;
   }
 }
@@ -1494,7 +1594,8 @@ std::vector<RefineLevelStats> level_stats(Handle& h, RefineCtx* c, i32 nslots) {
         if (ph < 32) { acc[ph] += dt; cnt[ph] += 1; }
       }
       const double tot = (double)((t[tn[s] - 1] & 0x00ffffffffffffffull) - (t[0] & 0x00ffffffffffffffull));
-      fprintf(stderr, "[gkw trace] level slot %d: %.1f us total;", s, tot / 1e3);
+      fprintf(stderr, "[gkw trace] level slot %d: %.1f us total; candidates/round %.0f;", s, tot / 1e3,
+              d[s].rounds ? (double)d[s].cand_sum / d[s].rounds : 0.0);
       for (i32 p = 0; p < 32; ++p)
         if (cnt[p]) fprintf(stderr, " ph%d x%d %.2fus", p, cnt[p], acc[p] / cnt[p] / 1e3);
       fprintf(stderr, "\n");
