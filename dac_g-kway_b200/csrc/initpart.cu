@@ -230,9 +230,12 @@ __device__ i64 grow_blocks(const LocalTopo& T, const TrialState& S, i32 s, i32 p
     for (i32 j = lane; j < rn; j += 32) {
       const i32 u = T.nb[rb + j];
       const i32 w = T.nw[rb + j];
+      // R[u] and degS[u] do not change in this step (u != pick): load them
+      // beside the connection update
+      const i32 ru = R[u], du = T.degS[u];
       const i32 c = atomicAdd(&C[u], w) + w;
-      if (!R[u]) {
-        const unsigned long long key = grow_key(c > 0, 2 * c - T.degS[u], u);
+      if (!ru) {
+        const unsigned long long key = grow_key(c > 0, 2 * c - du, u);
         atomicMax(reinterpret_cast<unsigned long long*>(&K[u]), key);
         atomicMax(reinterpret_cast<unsigned long long*>(&B1[u >> 5]), key);
         atomicMax(reinterpret_cast<unsigned long long*>(&B2[u >> 10]), key);
@@ -276,16 +279,29 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
   const i32 max_moves = gggp_max_moves(s);
   for (i32 mv = 0; mv < max_moves; ++mv) {
     u64 best = 0;
-    for (i32 i = lane; i < s; i += 32) {
-      const i32 r = R[i];
-      const i32 c = C[i], d = T.degS[i];
-      const i32 g = r ? (d - 2 * c) : (2 * c - d);
-      if (g <= 0) continue;
-      const i64 vw = (u32)T.vw[i];
-      const bool ok = r ? ((WS - wR) + vw <= capR) : (wR + vw <= capL);
-      if (!ok) continue;
-      const u64 key = move_key2(g, i);
-      best = best > key ? best : key;
+    // four members per lane per pass, their loads issued together
+    constexpr i32 kU = 4;
+    for (i32 i0 = lane; i0 < s; i0 += 32 * kU) {
+      i32 r[kU], c[kU], d[kU], w[kU];
+#pragma unroll
+      for (i32 u = 0; u < kU; ++u) {
+        const i32 i = i0 + 32 * u;
+        const bool in = i < s;
+        r[u] = in ? R[i] : 0;
+        c[u] = in ? C[i] : 0;
+        d[u] = in ? T.degS[i] : 0;
+        w[u] = in ? T.vw[i] : 0;
+      }
+#pragma unroll
+      for (i32 u = 0; u < kU; ++u) {
+        const i32 g = r[u] ? (d[u] - 2 * c[u]) : (2 * c[u] - d[u]);
+        const i64 vw = (u32)w[u];
+        const bool ok = r[u] ? ((WS - wR) + vw <= capR) : (wR + vw <= capL);
+        if (g > 0 && ok) {   // out-of-range lanes have g = 0
+          const u64 key = move_key2(g, i0 + 32 * u);
+          best = best > key ? best : key;
+        }
+      }
     }
     best = warp_max_u64(best);
     if (best == 0) break;
@@ -296,7 +312,7 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
     wR += r ? -(i64)(u32)T.vw[i] : (i64)(u32)T.vw[i];
     const i32 sign = r ? -1 : 1;
     const i32 rb = T.rb[i], rn = T.rn[i];
-    for (i32 j = lane; j < rn; j += 32) C[T.nb[rb + j]] += sign * T.nw[rb + j];
+    for (i32 j = lane; j < rn; j += 32) atomicAdd(&C[T.nb[rb + j]], sign * T.nw[rb + j]);
     __syncwarp();
   }
   i64 cut = 0;
@@ -503,8 +519,16 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
       S.C = q + base_off;
       S.R = q + n + base_off;
       S.K = g_keys + (size_t)t * n + base_off;
-      S.B1 = g_b1 + (size_t)t * b1_stride + (base_off >> 5) + p0;
-      S.B2 = g_b2 + (size_t)t * b2_stride + (base_off >> 10) + p0;
+      const size_t nbw = (size_t)gggp_nb1(s) + gggp_nb2(s);
+      if (nbw * sizeof(u64) * trials <= kGggpSmem) {
+        // the block maxima fit in shared memory (the topology and the rest
+        // of the state did not): every scan and block update stays on chip
+        S.B1 = reinterpret_cast<u64*>(smem_raw) + (size_t)t * nbw;
+        S.B2 = S.B1 + gggp_nb1(s);
+      } else {
+        S.B1 = g_b1 + (size_t)t * b1_stride + (base_off >> 5) + p0;
+        S.B2 = g_b2 + (size_t)t * b2_stride + (base_off >> 10) + p0;
+      }
     }
     // the seed names the part by its own graph's id (batched levels: parts are global)
     const i32 p0_local = part_base ? p0 - part_base[p0] : p0;
