@@ -217,28 +217,45 @@ __device__ i64 grow_blocks(const LocalTopo& T, const TrialState& S, i32 s, i32 p
       best = warp_max_u64(best);
       if (best == 0) break;
       pick = key_idx(best);
-      const i64 vw = (u32)T.vw[pick];
-      if (wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
     }
+    // the picked member's weight and row, loaded together
+    const i64 vw = (u32)T.vw[pick];
+    const i32 rb = T.rb[pick], rn = T.rn[pick];
+    if (step > 0 && wR + vw > TL && (wR + vw - TL) > (TL - wR)) break;
     if (lane == 0) {
       R[pick] = 1;
       K[pick] = 0;
     }
-    wR += (u32)T.vw[pick];
+    wR += vw;
     __syncwarp();
-    const i32 rb = T.rb[pick], rn = T.rn[pick];
-    for (i32 j = lane; j < rn; j += 32) {
-      const i32 u = T.nb[rb + j];
-      const i32 w = T.nw[rb + j];
-      // R[u] and degS[u] do not change in this step (u != pick): load them
-      // beside the connection update
-      const i32 ru = R[u], du = T.degS[u];
-      const i32 c = atomicAdd(&C[u], w) + w;
-      if (!ru) {
-        const unsigned long long key = grow_key(c > 0, 2 * c - du, u);
-        atomicMax(reinterpret_cast<unsigned long long*>(&K[u]), key);
-        atomicMax(reinterpret_cast<unsigned long long*>(&B1[u >> 5]), key);
-        atomicMax(reinterpret_cast<unsigned long long*>(&B2[u >> 10]), key);
+    // neighbours, four per lane per pass: the row loads, then the state loads
+    // and connection updates of all four are issued together.  R[u] and
+    // degS[u] do not change in this step (u != pick).
+    constexpr i32 kU = 4;
+    for (i32 j0 = lane; j0 < rn; j0 += 32 * kU) {
+      i32 u[kU], w[kU], ru[kU], du[kU], c[kU];
+#pragma unroll
+      for (i32 q = 0; q < kU; ++q) {
+        const i32 j = j0 + 32 * q;
+        u[q] = j < rn ? T.nb[rb + j] : -1;
+        w[q] = j < rn ? T.nw[rb + j] : 0;
+      }
+#pragma unroll
+      for (i32 q = 0; q < kU; ++q) {
+        if (u[q] >= 0) {
+          ru[q] = R[u[q]];
+          du[q] = T.degS[u[q]];
+          c[q] = atomicAdd(&C[u[q]], w[q]) + w[q];
+        }
+      }
+#pragma unroll
+      for (i32 q = 0; q < kU; ++q) {
+        if (u[q] >= 0 && !ru[q]) {
+          const unsigned long long key = grow_key(c[q] > 0, 2 * c[q] - du[q], u[q]);
+          atomicMax(reinterpret_cast<unsigned long long*>(&K[u[q]]), key);
+          atomicMax(reinterpret_cast<unsigned long long*>(&B1[u[q] >> 5]), key);
+          atomicMax(reinterpret_cast<unsigned long long*>(&B2[u[q] >> 10]), key);
+        }
       }
     }
     __syncwarp();
@@ -265,7 +282,7 @@ constexpr i32 kGggpBlockMin = 2048;
 // One GGGP trial by one warp (growth then positive-gain refinement); see the
 // file comment for the rules.  Returns the trial's cut and |W(R) - TL|.
 __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 pick, i64 TL, i64 WS, i64 capL,
-                           i64 capR, i64& cut_out, i64& dev_out) {
+                           i64 capR, i64& cut_out, i64& dev_out, unsigned long long* prof) {
   const int lane = threadIdx.x & 31;
   i32* C = S.C;
   i32* R = S.R;
@@ -274,7 +291,9 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
     C[i] = 0;
   }
   __syncwarp();
+  const long long c0 = clock64();
   i64 wR = s > kGggpBlockMin ? grow_blocks(T, S, s, pick, TL) : grow_scan(T, S, s, pick, TL);
+  const long long c1 = clock64();
   // ---- refinement: positive-gain moves within the side caps ----
   const i32 max_moves = gggp_max_moves(s);
   for (i32 mv = 0; mv < max_moves; ++mv) {
@@ -321,6 +340,11 @@ __device__ void gggp_trial(const LocalTopo& T, const TrialState& S, i32 s, i32 p
   cut = warp_sum_i64(cut);
   cut_out = cut;
   dev_out = wR > TL ? wR - TL : TL - wR;
+  if (prof && lane == 0) {   // diagnostic timeline: slowest trial's growth and refinement cycles
+    const long long c2 = clock64();
+    atomicMax(prof, (unsigned long long)(c1 - c0));
+    atomicMax(prof + 1, (unsigned long long)(c2 - c1));
+  }
 }
 
 // Exclusive scan of a[0..s) in shared memory by the whole block (total out).
@@ -367,7 +391,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     i32* __restrict__ lo_out, i32* __restrict__ hi_out, u64 seed, double eps, i32 trials,
     i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state, u64* g_keys,
     u64* g_b1, u64* g_b2, size_t b1_stride, size_t b2_stride, const i32* __restrict__ part_base, const i32* __restrict__ part_v0,
-    const i32* __restrict__ part_v1) {
+    const i32* __restrict__ part_v1, unsigned long long* prof) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_cnt;
   __shared__ i32 s_warp[33];
@@ -534,7 +558,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     const i32 p0_local = part_base ? p0 - part_base[p0] : p0;
     const i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0_local * 1315423911ull + (u64)t) % (u32)s);
     i64 cut, dev;
-    gggp_trial(T, S, s, pick, TL, WS, capL, capR, cut, dev);
+    gggp_trial(T, S, s, pick, TL, WS, capL, capR, cut, dev, prof);
     if (lane == 0) {
       s_cut[t] = cut;
       s_dev[t] = dev;
@@ -608,7 +632,10 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   GKW_CHECK_LAUNCH();
   const bool trace = getenv("GKW_TRACE") && *getenv("GKW_TRACE") == '1';
   std::vector<cudaEvent_t> ev;
+  unsigned long long* prof = nullptr;   // per depth: slowest trial's growth / refinement cycles
   if (trace) {
+    prof = reinterpret_cast<unsigned long long*>(h.scratch.alloc_n<u64>(2 * (size_t)std::max(depth, 1)));
+    GKW_CUDA(cudaMemsetAsync(prof, 0, sizeof(u64) * 2 * std::max(depth, 1), h.stream));
     ev.resize(depth + 1);
     for (auto& e : ev) GKW_CUDA(cudaEventCreate(&e));
     GKW_CUDA(cudaEventRecord(ev[0], h.stream));
@@ -622,17 +649,21 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     launch(k_gggp_depth, k, kInitTrials * 32, kGggpSmem, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a],
            hi[a], cnt, off, mlist, loc, lo[b], hi[b], seed, eps, trials, g_rb, g_rn, g_deg, g_vw, g_nb, g_nw,
            g_state, g_keys, g_b1, g_b2, b1_stride, b2_stride, batch ? batch->part_base : (const i32*)nullptr,
-           batch ? batch->part_v0 : (const i32*)nullptr, batch ? batch->part_v1 : (const i32*)nullptr);
+           batch ? batch->part_v0 : (const i32*)nullptr, batch ? batch->part_v1 : (const i32*)nullptr,
+           prof ? prof + 2 * d : nullptr);
     GKW_CHECK_LAUNCH();
     if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));
   }
   if (trace) {
     GKW_CUDA(cudaEventSynchronize(ev[depth]));
+    std::vector<unsigned long long> hp(2 * (size_t)std::max(depth, 1));
+    if (depth) GKW_CUDA(cudaMemcpy(hp.data(), prof, sizeof(u64) * 2 * depth, cudaMemcpyDeviceToHost));
     fprintf(stderr, "[gkw trace] init n=%d k=%d:", n, k);
     for (i32 d = 0; d < depth; ++d) {
       float ms = 0;
       cudaEventElapsedTime(&ms, ev[d], ev[d + 1]);
-      fprintf(stderr, " d%d %.1fus", d, ms * 1e3);
+      fprintf(stderr, " d%d %.1fus (growth %.2f, refinement %.2f Mcycles)", d, ms * 1e3, hp[2 * d] / 1e6,
+              hp[2 * d + 1] / 1e6);
     }
     fprintf(stderr, "\n");
     for (auto& e : ev) cudaEventDestroy(e);
