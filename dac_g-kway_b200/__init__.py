@@ -188,6 +188,8 @@ _SIGS = [
                                      _i64p, ctypes.POINTER(Stats)]),
     ("gkw_partition_device", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.POINTER(Options),
                                             _VP, _i64p, ctypes.POINTER(Stats)]),
+    ("gkw_partition_multi_k", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, _VP, ctypes.POINTER(Options),
+                                             _VP, _VP]),
     ("gkw_match", ctypes.c_int, [_VP, ctypes.POINTER(Csr), _VP]),
     ("gkw_union_find", ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, _VP, _i32p]),
     ("gkw_group_map", ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, ctypes.c_int32, _VP, _i32p]),
@@ -371,6 +373,21 @@ class Handle:
         del keep, cb_keep
         check(rc)
         return part, int(cut.value), st.as_dict()
+
+    def partition_multi_k(self, xadj, adjncy, adjwgt, vwgt, ks, opts: Options | None = None):
+        """One graph for several k, coarsened once -> (parts [len(ks), n], cuts [len(ks)]);
+        row q equals ``partition(..., ks[q])``."""
+        c, keep = _csr_host(xadj, adjncy, adjwgt, vwgt)
+        kk = np.ascontiguousarray(ks, dtype=np.int32)
+        o = opts if opts is not None else default_options()
+        parts = np.empty((kk.shape[0], c.n), np.int32)
+        cuts = np.zeros(max(kk.shape[0], 1), np.int64)
+        rc = lib().gkw_partition_multi_k(self._h, ctypes.byref(c), int(kk.shape[0]),
+                                         kk.ctypes.data if kk.shape[0] else None, ctypes.byref(o),
+                                         parts.ctypes.data if parts.size else None, cuts.ctypes.data)
+        del keep
+        check(rc)
+        return parts, cuts[:kk.shape[0]]
 
     def partition_device(self, xadj, adjncy, adjwgt, vwgt, k: int, part_out, opts: Options | None = None,
                          stats: bool = True):

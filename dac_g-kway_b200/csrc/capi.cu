@@ -211,6 +211,17 @@ gkw_status gkw_partition(gkw_handle* h, const gkw_csr* graph, int32_t k, const g
   });
 }
 
+gkw_status gkw_partition_multi_k(gkw_handle* h, const gkw_csr* graph, int32_t n_k, const int32_t* ks,
+                                 const gkw_options* opt, int32_t* parts_out, int64_t* cuts_out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph hg = dev_view(graph);
+    gkw_options o;
+    if (opt) o = *opt; else gkw_default_options(&o);
+    partition_multi_host(hh, hg, n_k, ks, o, parts_out, cuts_out);
+  });
+}
+
 gkw_status gkw_match(gkw_handle* h, const gkw_csr* d_graph, int32_t* d_cand) {
   return guard([&] {
     Handle& hh = H(h);

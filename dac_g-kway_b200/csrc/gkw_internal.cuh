@@ -334,6 +334,11 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
 // by xadj[0], neighbour ids by vbase); part_out is host memory.
 void partition_host(Handle& h, const DevGraph& host_graph, i64 vbase, i32 k, const gkw_options& opt,
                     i32* part_out, i64* cut_out, gkw_stats* stats);
+// One graph for several k over one hierarchy (each k's result as alone).
+void partition_multi_impl(Handle& h, const DevGraph& g0, i32 nk, const i32* ks, const gkw_options& opt,
+                          i32* d_parts, i64* cuts_out);
+void partition_multi_host(Handle& h, const DevGraph& host_graph, i32 nk, const i32* ks, const gkw_options& opt,
+                          i32* parts_out, i64* cuts_out);
 Handle& handle_of(gkw_handle* h);   // the handle behind a C-ABI handle (capi.cu)
 // Many independent graphs partitioned as one disjoint union (batch.cu): host
 // arrays with global ids, graph g = vertices [graph_ptr[g], graph_ptr[g+1]).

@@ -123,15 +123,43 @@ void ensure_timer_events(Handle& h) {
   h.tev_ready = true;
 }
 
+// Initial partition of the coarsest graph cg into cpart: the device GGGP, or
+// the caller's callback (the reference calls host METIS here,
+// metis_partition.hpp:46-47).
+static void initial_partition(Handle& h, const DevGraph& cg, i32 k, const gkw_options& opt, i32* cpart) {
+  if (opt.init_method == GKW_INIT_CALLBACK) {
+    std::vector<i32> hx(cg.n + 1), ha(cg.m), hw(cg.m), hv(cg.n), hp(cg.n);
+    GKW_CUDA(cudaMemcpyAsync(hx.data(), cg.xadj, sizeof(i32) * (cg.n + 1), cudaMemcpyDeviceToHost, h.stream));
+    if (cg.m) {
+      GKW_CUDA(cudaMemcpyAsync(ha.data(), cg.adjncy, sizeof(i32) * cg.m, cudaMemcpyDeviceToHost, h.stream));
+      GKW_CUDA(cudaMemcpyAsync(hw.data(), cg.adjwgt, sizeof(i32) * cg.m, cudaMemcpyDeviceToHost, h.stream));
+    }
+    if (cg.n) GKW_CUDA(cudaMemcpyAsync(hv.data(), cg.vwgt, sizeof(i32) * cg.n, cudaMemcpyDeviceToHost, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+    const i32 rcb = opt.init_fn(opt.init_user, cg.n, hx.data(), ha.data(), hw.data(), hv.data(), k, hp.data());
+    if (rcb != 0) throw Error{GKW_E_INIT, "initial-partition callback returned " + std::to_string(rcb)};
+    for (i32 v = 0; v < cg.n; ++v)
+      if (hp[v] < 0 || hp[v] >= k) throw Error{GKW_E_INIT, "initial-partition callback gave a part out of range"};
+    if (cg.n) GKW_CUDA(cudaMemcpyAsync(cpart, hp.data(), sizeof(i32) * cg.n, cudaMemcpyHostToDevice, h.stream));
+    GKW_CUDA(cudaStreamSynchronize(h.stream));
+  } else {
+    device_init_partition(h, cg, k, opt.eps, opt.seed, std::max(1, std::min(8, opt.init_trials)), cpart);
+  }
+}
+
+static void check_options(const gkw_options& opt) {
+  GKW_REQUIRE(opt.group_cap >= 1, GKW_E_INVALID, "group_cap must be >= 1");
+  GKW_REQUIRE(opt.threshold_factor >= 0, GKW_E_INVALID, "threshold_factor must be >= 0");
+  GKW_REQUIRE(opt.init_method == GKW_INIT_DEVICE || (opt.init_method == GKW_INIT_CALLBACK && opt.init_fn),
+              GKW_E_INVALID, "init_method CALLBACK needs init_fn");
+}
+
 void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
                            i64* cut_out, gkw_stats* stats) {
   GKW_REQUIRE(k >= 1, GKW_E_INVALID, "k must be >= 1");
   GKW_REQUIRE(g0.n >= 0 && g0.m >= 0 && g0.m < ((i64)1 << 31), GKW_E_UNSUPPORTED,
               "graphs need n >= 0 and nnz < 2^31");
-  GKW_REQUIRE(opt.group_cap >= 1, GKW_E_INVALID, "group_cap must be >= 1");
-  GKW_REQUIRE(opt.threshold_factor >= 0, GKW_E_INVALID, "threshold_factor must be >= 0");
-  GKW_REQUIRE(opt.init_method == GKW_INIT_DEVICE || (opt.init_method == GKW_INIT_CALLBACK && opt.init_fn),
-              GKW_E_INVALID, "init_method CALLBACK needs init_fn");
+  check_options(opt);
   ensure_timer_events(h);
   cudaEvent_t* ev = h.tev;              // phase marks
   cudaEvent_t* lev = h.tev + 5;         // level kernel of slot s: lev[2s], lev[2s+1]
@@ -187,24 +215,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     ~CtxGuard() { refine_destroy(c); }
   } cguard{rc};
   i32* cpart = refine_part(rc);
-  if (opt.init_method == GKW_INIT_CALLBACK) {
-    std::vector<i32> hx(cg.n + 1), ha(cg.m), hw(cg.m), hv(cg.n), hp(cg.n);
-    GKW_CUDA(cudaMemcpyAsync(hx.data(), cg.xadj, sizeof(i32) * (cg.n + 1), cudaMemcpyDeviceToHost, h.stream));
-    if (cg.m) {
-      GKW_CUDA(cudaMemcpyAsync(ha.data(), cg.adjncy, sizeof(i32) * cg.m, cudaMemcpyDeviceToHost, h.stream));
-      GKW_CUDA(cudaMemcpyAsync(hw.data(), cg.adjwgt, sizeof(i32) * cg.m, cudaMemcpyDeviceToHost, h.stream));
-    }
-    if (cg.n) GKW_CUDA(cudaMemcpyAsync(hv.data(), cg.vwgt, sizeof(i32) * cg.n, cudaMemcpyDeviceToHost, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-    const i32 rcb = opt.init_fn(opt.init_user, cg.n, hx.data(), ha.data(), hw.data(), hv.data(), k, hp.data());
-    if (rcb != 0) throw Error{GKW_E_INIT, "initial-partition callback returned " + std::to_string(rcb)};
-    for (i32 v = 0; v < cg.n; ++v)
-      if (hp[v] < 0 || hp[v] >= k) throw Error{GKW_E_INIT, "initial-partition callback gave a part out of range"};
-    if (cg.n) GKW_CUDA(cudaMemcpyAsync(cpart, hp.data(), sizeof(i32) * cg.n, cudaMemcpyHostToDevice, h.stream));
-    GKW_CUDA(cudaStreamSynchronize(h.stream));
-  } else {
-    device_init_partition(h, cg, k, opt.eps, opt.seed, std::max(1, std::min(8, opt.init_trials)), cpart);
-  }
+  initial_partition(h, cg, k, opt, cpart);
   if (stage_checks()) check_stage("initial partition", (i32)lv.size() - 1, [&] { check_parts(h, cg.n, cpart, k); });
   refine_init_coarsest(h, rc, cg, cpart);
   i64* d_metrics = h.hier.alloc_n<i64>(k + 2);   // [0] cut, [1] bad-part flag, [2..k+2) part weights
@@ -291,23 +302,118 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   }
 }
 
-// Partition of a graph held in host memory: copy it into the handle's pool,
-// partition, copy the part ids back.  The host arrays may be a slice of a
-// larger concatenated CSR: `xadj` values are then offset by xadj[0] and
-// neighbour ids by `vbase`, and both are rebased on the device.
-void partition_host(Handle& hh, const DevGraph& hg, i64 vbase, i32 k, const gkw_options& o, i32* part_out,
-                    i64* cut_out, gkw_stats* stats) {
+// One graph partitioned for several k over one hierarchy.  Matching,
+// union-find, grouping and contraction do not depend on k; only where the
+// coarsening stops does (the threshold threshold_factor * k,
+// graph_partitioner.hpp:22; the discard rule nc < k + 1, :93-96; the default
+// mode's coarse-vertex cap).  The levels are built while some k still
+// coarsens, and each k runs the initial partition and the uncoarsening of
+// partition_impl on its own prefix of them, so its result is the one
+// partition_impl gives alone.  d_parts holds nk rows of g0.n part ids.
+void partition_multi_impl(Handle& h, const DevGraph& g0, i32 nk, const i32* ks, const gkw_options& opt,
+                          i32* d_parts, i64* cuts_out) {
+  GKW_REQUIRE(nk >= 0 && (nk == 0 || ks != nullptr), GKW_E_INVALID, "ks is NULL");
+  for (i32 q = 0; q < nk; ++q) GKW_REQUIRE(ks[q] >= 1, GKW_E_INVALID, "k must be >= 1");
+  GKW_REQUIRE(g0.n >= 0 && g0.m >= 0 && g0.m < ((i64)1 << 31), GKW_E_UNSUPPORTED,
+              "graphs need n >= 0 and nnz < 2^31");
+  check_options(opt);
+  const i64 W = validate(h, g0);
+  std::vector<Level> lv(1);
+  lv[0].g = g0;
+  std::vector<i32> Lk(nk, -1);   // coarsest level of each k
+  for (;;) {
+    const i32 l = (i32)lv.size() - 1;
+    const i64 nl = lv.back().g.n;
+    bool any = false;
+    for (i32 q = 0; q < nk; ++q) {
+      if (Lk[q] < 0 && (nl <= (i64)opt.threshold_factor * ks[q] || (i32)lv.size() >= kMaxLevels)) Lk[q] = l;
+      any |= Lk[q] < 0;
+    }
+    if (!any) break;
+    CoarsenOut co;
+    coarsen_level(h, lv.back().g, opt.group_cap, co);
+    bool cont = false;
+    for (i32 q = 0; q < nk; ++q) {
+      if (Lk[q] >= 0) continue;
+      bool stop = co.nc == nl || co.nc < ks[q] + 1;   // level discarded for this k
+      if (opt.enforce_balance && opt.coarse_vertex_frac > 0 &&
+          (double)co.max_cvw > opt.coarse_vertex_frac * (double)W / (double)ks[q])
+        stop = true;
+      if (stop) Lk[q] = l;
+      else cont = true;
+    }
+    if (!cont) break;
+    lv.back().cmap = co.cmap;
+    Level nx;
+    nx.g.n = co.nc;
+    nx.g.m = co.mc;
+    nx.g.xadj = co.cxadj;
+    nx.g.adjncy = co.cadjncy;
+    nx.g.adjwgt = co.cadjwgt;
+    nx.g.vwgt = co.cvwgt;
+    lv.push_back(nx);
+  }
+  for (i32 q = 0; q < nk; ++q) {
+    const i32 k = ks[q];
+    const float maxw = opt.enforce_balance ? balance_cap(W, k, opt.eps) : max_part_weight(W, k, opt.eps);
+    const i32 nl = Lk[q] + 1;
+    const DevGraph& cg = lv[nl - 1].g;
+    const Pool::Mark mk = h.hier.mark();   // this k's state, released before the next k
+    RefineCtx* rc = refine_create(h, std::max(g0.n, 1), k, opt.move_cap);
+    struct CtxGuard {
+      RefineCtx* c;
+      ~CtxGuard() { refine_destroy(c); }
+    } cguard{rc};
+    i32* cpart = refine_part(rc);
+    initial_partition(h, cg, k, opt, cpart);
+    refine_init_coarsest(h, rc, cg, cpart);
+    auto balances = [&](i32 L) {
+      return opt.enforce_balance && (L == 0 || L < nl - std::max(0, opt.balance_skip_levels));
+    };
+    if (balances(nl - 1)) {
+      LevelJob j;
+      j.balance = true;
+      j.bcap = maxw;
+      j.move_cap = opt.move_cap;
+      level_run(h, rc, cg, j, nl - 1);
+    }
+    for (i32 L = nl - 2; L >= 0; --L) {
+      LevelJob j;
+      j.cmap = lv[L].cmap;
+      j.balance = balances(L);
+      j.bcap = maxw;
+      j.refine = true;
+      j.maxw = maxw;
+      j.move_cap = opt.move_cap;
+      level_run(h, rc, lv[L].g, j, L);
+    }
+    i32* out = d_parts + (size_t)q * g0.n;
+    if (g0.n) {
+      GKW_CUDA(cudaMemcpyAsync(out, refine_part(rc), sizeof(i32) * g0.n, cudaMemcpyDeviceToDevice, h.stream));
+    }
+    i64* d_metrics = h.hier.alloc_n<i64>(k + 2);
+    compute_cut_pw(h, g0, out, k, d_metrics, d_metrics + 2);
+    i64 hm[2] = {0, 0};
+    GKW_CUDA(cudaMemcpyAsync(hm, d_metrics, sizeof(i64) * 2, cudaMemcpyDeviceToHost, h.stream));
+    level_stats(h, rc, nl);   // one sync; error words of the level kernels
+    GKW_REQUIRE(hm[1] == 0, GKW_E_INTERNAL, "partition produced a part id out of range");
+    if (cuts_out) cuts_out[q] = hm[0];
+    h.hier.release(mk);
+  }
+}
+
+// Copies a host CSR into the handle's hierarchy pool (unit weights where the
+// arrays are NULL).  The host arrays may be a slice of a larger concatenated
+// CSR: xadj values are then offset by xadj[0] and neighbour ids by vbase, and
+// both are rebased on the device.
+DevGraph upload_host_graph(Handle& hh, const DevGraph& hg, i64 vbase) {
   GKW_REQUIRE(hg.n >= 0 && hg.m >= 0, GKW_E_INVALID, "negative size");
-  GKW_REQUIRE(hg.n == 0 || part_out != nullptr, GKW_E_INVALID, "part_out is NULL");
   GKW_REQUIRE(vbase >= 0 && vbase < ((i64)1 << 31), GKW_E_UNSUPPORTED, "vertex offset out of range");
-  hh.hier.reset();
-  hh.scratch.reset();
   const i64 n = hg.n, m = hg.m;
   i32* x = hh.hier.alloc_n<i32>(n + 1);
   i32* a = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
   i32* w = hh.hier.alloc_n<i32>(std::max<i64>(m, 1));
   i32* vw = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
-  i32* part = hh.hier.alloc_n<i32>(std::max<i64>(n, 1));
   GKW_CUDA(cudaMemcpyAsync(x, hg.xadj, sizeof(i32) * (n + 1), cudaMemcpyHostToDevice, hh.stream));
   const i32 ebase = hg.xadj[0];
   if (ebase != 0) {
@@ -335,8 +441,36 @@ void partition_host(Handle& hh, const DevGraph& hg, i64 vbase, i32 k, const gkw_
   g.adjncy = a;
   g.adjwgt = w;
   g.vwgt = vw;
+  return g;
+}
+
+// Partition of a graph held in host memory: copy it into the handle's pool,
+// partition, copy the part ids back.  The host arrays may be a slice of a
+// larger concatenated CSR: `xadj` values are then offset by xadj[0] and
+// neighbour ids by `vbase`, and both are rebased on the device.
+void partition_host(Handle& hh, const DevGraph& hg, i64 vbase, i32 k, const gkw_options& o, i32* part_out,
+                    i64* cut_out, gkw_stats* stats) {
+  GKW_REQUIRE(hg.n == 0 || part_out != nullptr, GKW_E_INVALID, "part_out is NULL");
+  hh.hier.reset();
+  hh.scratch.reset();
+  const DevGraph g = upload_host_graph(hh, hg, vbase);
+  i32* part = hh.hier.alloc_n<i32>(std::max<i64>(hg.n, 1));
   partition_impl(hh, g, k, o, part, cut_out, stats);
-  if (n) GKW_CUDA(cudaMemcpyAsync(part_out, part, sizeof(i32) * n, cudaMemcpyDeviceToHost, hh.stream));
+  if (hg.n) GKW_CUDA(cudaMemcpyAsync(part_out, part, sizeof(i32) * hg.n, cudaMemcpyDeviceToHost, hh.stream));
+  GKW_CUDA(cudaStreamSynchronize(hh.stream));
+}
+
+// Several k over one hierarchy, host arrays in and out (nk rows of n ids).
+void partition_multi_host(Handle& hh, const DevGraph& hg, i32 nk, const i32* ks, const gkw_options& o,
+                          i32* parts_out, i64* cuts_out) {
+  GKW_REQUIRE(hg.n == 0 || nk == 0 || parts_out != nullptr, GKW_E_INVALID, "parts_out is NULL");
+  hh.hier.reset();
+  hh.scratch.reset();
+  const DevGraph g = upload_host_graph(hh, hg, 0);
+  i32* parts = hh.hier.alloc_n<i32>(std::max<i64>((i64)hg.n * std::max(nk, 1), 1));
+  partition_multi_impl(hh, g, nk, ks, o, parts, cuts_out);
+  if (hg.n && nk)
+    GKW_CUDA(cudaMemcpyAsync(parts_out, parts, sizeof(i32) * (size_t)hg.n * nk, cudaMemcpyDeviceToHost, hh.stream));
   GKW_CUDA(cudaStreamSynchronize(hh.stream));
 }
 

@@ -127,6 +127,14 @@ gkw_status gkw_partition(gkw_handle* h, const gkw_csr* graph, int32_t k, const g
 gkw_status gkw_partition_device(gkw_handle* h, const gkw_csr* d_graph, int32_t k,
                                 const gkw_options* opt, int32_t* d_part_out, int64_t* cut_out,
                                 gkw_stats* stats);
+/* One host graph partitioned for n_k values of k, coarsened once.  The levels
+ * do not depend on k except where the coarsening stops (threshold 20k,
+ * gkway/graph_partitioner.hpp:22; the discard rule, :93-96), so every k runs
+ * on a prefix of one hierarchy.  No counterpart in the reference, where each
+ * run coarsens again.  parts_out holds n_k rows of n part ids; row q and
+ * cuts_out[q] equal gkw_partition's result for ks[q]. */
+gkw_status gkw_partition_multi_k(gkw_handle* h, const gkw_csr* graph, int32_t n_k, const int32_t* ks,
+                                 const gkw_options* opt, int32_t* parts_out, int64_t* cuts_out);
 
 /* ---- per-phase entry points (device pointers) --------------------------
  * Heavy-edge candidate per vertex.  Replaces gk::matching_with_score
