@@ -215,6 +215,22 @@ PartitionResult GraphPartitioner::partition_with_stats(const Graph& g, int k) {
 
 std::vector<int> GraphPartitioner::partition(const Graph& g, int k) { return partition_with_stats(g, k).part; }
 
+std::vector<PartitionResult> GraphPartitioner::partition_multi_k(const Graph& g, const std::vector<int>& ks) {
+  gkw_csr c = g.csr();
+  const size_t n = (size_t)c.n, nk = ks.size();
+  std::vector<int32_t> kk(ks.begin(), ks.end()), parts(std::max<size_t>(n * nk, 1));
+  std::vector<int64_t> cuts(std::max<size_t>(nk, 1));
+  gkw_status st = gkw_partition_multi_k(h_, &c, (int32_t)nk, kk.data(), &opt_, parts.data(), cuts.data());
+  if (st != GKW_OK) throw std::runtime_error(std::string("gkw_partition_multi_k: ") + gkw_last_error());
+  std::vector<PartitionResult> out(nk);
+  for (size_t q = 0; q < nk; ++q) {
+    out[q].part.assign(parts.begin() + q * n, parts.begin() + (q + 1) * n);
+    out[q].cut = cuts[q];
+    std::memset(&out[q].stats, 0, sizeof(out[q].stats));
+  }
+  return out;
+}
+
 // ---------------------------------------------------------------------------
 // METIS as the initial partitioner (the reference's behaviour), loaded at run
 // time.  idx_t is 64-bit in the reference's bundled METIS (metis.h:33).

@@ -74,6 +74,9 @@ class GraphPartitioner {
 
   std::vector<int> partition(const Graph& g, int k);
   PartitionResult partition_with_stats(const Graph& g, int k);
+  // One graph for several k, coarsened once (gkw_partition_multi_k): result q
+  // equals partition_with_stats(g, ks[q]) without its statistics.
+  std::vector<PartitionResult> partition_multi_k(const Graph& g, const std::vector<int>& ks);
   gkw_options& options() { return opt_; }
 
  private:
