@@ -13,6 +13,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gkway.hpp"
@@ -67,6 +68,125 @@ inline bool next_int(const char*& b, const char* e, long long& out) {
   return true;
 }
 
+// Layout of a vertex line: [size] [weight] (neighbour [edge weight])*.
+struct LineFormat {
+  bool vsize, vw, ew;
+  long long n;
+};
+
+inline bool comment_line(const char* b, const char* e) {
+  while (b < e && (*b == ' ' || *b == '\t')) ++b;
+  return b < e && *b == '%';
+}
+
+// One vertex line: its weight into vw, its neighbours (0-based) and edge
+// weights appended to adj / w.
+void parse_vertex_line(const char* b, const char* e, const LineFormat& lf, int32_t& vw, std::vector<int32_t>& adj,
+                       std::vector<int32_t>& w) {
+  long long x;
+  if (lf.vsize && !next_int(b, e, x)) throw std::runtime_error("graph file: missing vertex size");
+  if (lf.vw) {
+    if (!next_int(b, e, x)) throw std::runtime_error("graph file: missing vertex weight");
+    vw = (int32_t)x;
+  }
+  while (next_int(b, e, x)) {
+    if (x < 1 || x > lf.n) throw std::runtime_error("graph file: neighbour id out of range");
+    adj.push_back((int32_t)(x - 1));
+    long long ew = 1;
+    if (lf.ew && !next_int(b, e, ew)) throw std::runtime_error("graph file: missing edge weight");
+    w.push_back((int32_t)ew);
+  }
+}
+
+// Files above this size are parsed by several threads.
+constexpr size_t kParallelParseBytes = (size_t)8 << 20;
+
+// The body [p, end) split at line starts into T chunks.  Pass 1 counts each
+// chunk's vertex lines, so every chunk knows the global index of its first
+// vertex; pass 2 parses the lines of vertices 0..n-1 (lines beyond them are
+// never read, as in the sequential reading); the chunks are then placed
+// one after the other.  An error is reported for the first failing vertex in
+// file order, the one the sequential reading would stop at.  Returns the
+// number of vertex lines read (<= n).
+long long parse_parallel(const char* p, const char* end, int T, const LineFormat& lf, std::vector<int32_t>& xadj,
+                         std::vector<int32_t>& vwgt, std::vector<int32_t>& adjncy, std::vector<int32_t>& adjwgt) {
+  std::vector<const char*> cut(T + 1);
+  cut[0] = p;
+  cut[T] = end;
+  for (int t = 1; t < T; ++t) {
+    const char* q = p + (size_t)(end - p) * t / T;
+    if (q < cut[t - 1]) q = cut[t - 1];
+    if (q > p && q < end && q[-1] != '\n') {
+      const char* nl = (const char*)memchr(q, '\n', (size_t)(end - q));
+      q = nl ? nl + 1 : end;
+    }
+    cut[t] = q;
+  }
+  std::vector<long long> lines(T, 0);
+  auto run = [&](auto&& body) {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(body, t);
+    for (auto& x : th) x.join();
+  };
+  run([&](int t) {
+    Cursor cc{cut[t], cut[t + 1]};
+    const char *b, *e;
+    long long k = 0;
+    while (cc.line(b, e))
+      if (!comment_line(b, e)) ++k;
+    lines[t] = k;
+  });
+  std::vector<long long> first(T + 1, 0);
+  for (int t = 0; t < T; ++t) first[t + 1] = first[t] + lines[t];
+  struct Part {
+    std::vector<int32_t> deg, adj, w;
+    long long err_v = -1;
+    std::string err;
+  };
+  std::vector<Part> part(T);
+  run([&](int t) {
+    Part& P = part[t];
+    Cursor cc{cut[t], cut[t + 1]};
+    const char *b, *e;
+    long long v = first[t];
+    while (v < lf.n && cc.line(b, e)) {
+      if (comment_line(b, e)) continue;
+      const size_t before = P.adj.size();
+      try {
+        parse_vertex_line(b, e, lf, vwgt[(size_t)v], P.adj, P.w);
+      } catch (const std::exception& ex) {
+        P.err_v = v;
+        P.err = ex.what();
+        return;
+      }
+      P.deg.push_back((int32_t)(P.adj.size() - before));
+      ++v;
+    }
+  });
+  for (int t = 0; t < T; ++t)
+    if (part[t].err_v >= 0) throw std::runtime_error(part[t].err);   // chunks are in file order
+  size_t total = 0;
+  for (const Part& P : part) total += P.adj.size();
+  if (total >= ((size_t)1 << 31)) throw std::runtime_error("graph file: too many adjacency entries");
+  adjncy.resize(total);
+  adjwgt.resize(total);
+  long long v = 0;
+  size_t at = 0;
+  for (const Part& P : part) {
+    for (int32_t d : P.deg) {
+      at += (size_t)d;
+      xadj[(size_t)++v] = (int32_t)at;
+    }
+  }
+  std::vector<size_t> eoff(T + 1, 0);
+  for (int t = 0; t < T; ++t) eoff[t + 1] = eoff[t] + part[t].adj.size();
+  run([&](int t) {
+    std::copy(part[t].adj.begin(), part[t].adj.end(), adjncy.begin() + eoff[t]);
+    std::copy(part[t].w.begin(), part[t].w.end(), adjwgt.begin() + eoff[t]);
+  });
+  return v;
+}
+
 }  // namespace
 
 Graph::Graph(const std::string& input_path, bool reference_quirks) {
@@ -109,33 +229,27 @@ Graph::Graph(const std::string& input_path, bool reference_quirks) {
     has_vsize = has_vw = false;
     has_ew = pairs_only;
   }
+  const LineFormat lf{has_vsize, has_vw, has_ew, n};
   xadj_.assign((size_t)n + 1, 0);
   vwgt_.assign((size_t)n, 1);
   adjncy_.clear();
   adjwgt_.clear();
-  adjncy_.reserve((size_t)(2 * m));
-  adjwgt_.reserve((size_t)(2 * m));
+  const size_t body = (size_t)(c.end - c.p);
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int T = body < kParallelParseBytes ? 1 : (int)std::min<unsigned>(std::max(hw, 1u), 32u);
   long long v = 0;
-  while (v < n) {
-    if (!c.line(b, e)) break;
-    const char* t = b;
-    while (t < e && (*t == ' ' || *t == '\t')) ++t;
-    if (t < e && *t == '%') continue;
-    long long x;
-    if (has_vsize && !next_int(b, e, x)) throw std::runtime_error("graph file: missing vertex size");
-    if (has_vw) {
-      if (!next_int(b, e, x)) throw std::runtime_error("graph file: missing vertex weight");
-      vwgt_[(size_t)v] = (int32_t)x;
+  if (T == 1) {
+    adjncy_.reserve((size_t)(2 * m));
+    adjwgt_.reserve((size_t)(2 * m));
+    while (v < n) {
+      if (!c.line(b, e)) break;
+      if (comment_line(b, e)) continue;
+      parse_vertex_line(b, e, lf, vwgt_[(size_t)v], adjncy_, adjwgt_);
+      ++v;
+      xadj_[(size_t)v] = (int32_t)adjncy_.size();
     }
-    while (next_int(b, e, x)) {
-      if (x < 1 || x > n) throw std::runtime_error("graph file: neighbour id out of range");
-      adjncy_.push_back((int32_t)(x - 1));
-      long long w = 1;
-      if (has_ew && !next_int(b, e, w)) throw std::runtime_error("graph file: missing edge weight");
-      adjwgt_.push_back((int32_t)w);
-    }
-    ++v;
-    xadj_[(size_t)v] = (int32_t)adjncy_.size();
+  } else {
+    v = parse_parallel(c.p, c.end, T, lf, xadj_, vwgt_, adjncy_, adjwgt_);
   }
   for (; v < n; ++v) xadj_[(size_t)v + 1] = (int32_t)adjncy_.size();   // missing trailing lines: isolated
   if (!reference_quirks && (long long)adjncy_.size() != 2 * m)

@@ -130,3 +130,37 @@ def test_write_metis_round_trip(pkg, gen, tmp_path, kind):
     x, a, w, vw = pkg.read_metis(p)
     assert np.array_equal(x, g.xadj) and np.array_equal(a, g.adjncy)
     assert np.array_equal(w, g.adjwgt) and np.array_equal(vw, g.vwgt)
+
+
+def test_reader_large_files_parallel(pkg, gen, tmp_path):
+    """Files above 8 MB are parsed by several threads; the result and the
+    errors are those of the sequential reading (small files)."""
+    from graphs import weighted
+    g = weighted(gen, gen.delaunay(250000, 3), seed=5)
+    p = str(tmp_path / "big.graph")
+    gen.write_metis(g, p)
+    import os
+    assert os.path.getsize(p) > (8 << 20)
+    x, a, w, vw = pkg.read_metis(p)
+    assert np.array_equal(x, g.xadj) and np.array_equal(a, g.adjncy)
+    assert np.array_equal(w, g.adjwgt) and np.array_equal(vw, g.vwgt)
+    # comment lines between vertex lines, and lines after the n-th vertex
+    # (never read) that would not parse
+    lines = open(p).read().split("\n")
+    body = lines[1:1 + g.n]
+    out = [lines[0]]
+    for i, ln in enumerate(body):
+        if i % 5000 == 0:
+            out.append("% a comment line")
+        out.append(ln)
+    out.append("not a vertex line")
+    q = str(tmp_path / "big2.graph")
+    open(q, "w").write("\n".join(out) + "\n")
+    x2, a2, w2, vw2 = pkg.read_metis(q)
+    assert np.array_equal(x2, g.xadj) and np.array_equal(a2, g.adjncy) and np.array_equal(w2, g.adjwgt)
+    assert np.array_equal(vw2, g.vwgt)
+    # a bad token late in the file is reported
+    out[-2] = out[-2] + " x"
+    open(q, "w").write("\n".join(out) + "\n")
+    with pytest.raises(pkg.GkwError, match="bad token"):
+        pkg.read_metis(q)
