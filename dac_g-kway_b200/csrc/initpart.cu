@@ -383,6 +383,8 @@ __device__ i32 block_exscan_smem(i32* a, i32 s, i32* s_warp) {
 }
 
 constexpr size_t kGggpSmem = 200 * 1024;   // dynamic shared memory of the depth kernel
+constexpr i32 kGggpLongRow = 64;            // rows longer than this are read by a whole warp
+constexpr i32 kGggpLongMax = 1024;          // long-row members listed in shared memory
 
 __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     i32 n, const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
@@ -439,21 +441,58 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     return;
   }
   const i32 pm = p0 + (p1 - p0) / 2;
-  // per member: neighbours inside the sub-problem, weight to them, W(S)
+  // per member: neighbours inside the sub-problem, weight to them, W(S).
+  // Rows longer than kGggpLongRow are read by a whole warp (hubs would stall
+  // one thread for thousands of dependent loads).  Their members are listed
+  // in s_long; when there are more than it holds, the warps find them by
+  // scanning all members instead.
+  __shared__ i32 s_long[kGggpLongMax];
+  __shared__ i32 s_nlong;
+  if (threadIdx.x == 0) s_nlong = 0;
+  __syncthreads();
   i64 wpart = 0, epart = 0;
   for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
     const i32 v = M[i];
+    const i32 b = xadj[v], e1 = xadj[v + 1];
+    g_vw[base_off + i] = vwgt[v];
+    wpart += (u32)vwgt[v];
+    if (e1 - b > kGggpLongRow) {
+      const i32 at = atomicAdd(&s_nlong, 1);
+      if (at < kGggpLongMax) s_long[at] = i;
+      continue;
+    }
     i32 d = 0, c = 0;
-    for (i32 e = xadj[v]; e < xadj[v + 1]; ++e)
+    for (i32 e = b; e < e1; ++e)
       if (lo[adjncy[e]] == p0) {
         d += adjwgt[e];
         ++c;
       }
     g_rn[base_off + i] = c;
     g_deg[base_off + i] = d;
-    g_vw[base_off + i] = vwgt[v];
-    wpart += (u32)vwgt[v];
     epart += c;
+  }
+  __syncthreads();
+  const bool listed = s_nlong <= kGggpLongMax;   // block-uniform
+  const i32 nq = listed ? s_nlong : s;
+  for (i32 q = wid; q < nq; q += (i32)(blockDim.x >> 5)) {
+    const i32 i = listed ? s_long[q] : q;
+    const i32 v = M[i];
+    const i32 b = xadj[v], e1 = xadj[v + 1];
+    if (e1 - b <= kGggpLongRow) continue;   // warp-uniform (scan mode only)
+    i64 d = 0;
+    i32 c = 0;
+    for (i32 e = b + lane; e < e1; e += 32)
+      if (lo[adjncy[e]] == p0) {
+        d += adjwgt[e];
+        ++c;
+      }
+    d = warp_sum_i64(d);
+    c = (i32)warp_sum_i64(c);
+    if (lane == 0) {
+      g_rn[base_off + i] = c;
+      g_deg[base_off + i] = (i32)d;
+      epart += c;
+    }
   }
   wpart = warp_sum_i64(wpart);
   epart = warp_sum_i64(epart);
@@ -508,14 +547,40 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   }
   for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
     const i32 v = M[i];
+    const i32 b = xadj[v], e1 = xadj[v + 1];
+    if (e1 - b > kGggpLongRow) continue;   // a warp fills it below
     i32 j = rb[i];
-    for (i32 e = xadj[v]; e < xadj[v + 1]; ++e) {
+    for (i32 e = b; e < e1; ++e) {
       const i32 u = adjncy[e];
       if (lo[u] == p0) {
         nb[j] = loc[u];
         nw[j] = adjwgt[e];
         ++j;
       }
+    }
+  }
+  // long rows: one warp each, kept neighbours in row order
+  for (i32 q = wid; q < nq; q += (i32)(blockDim.x >> 5)) {
+    const i32 i = listed ? s_long[q] : q;
+    const i32 v = M[i];
+    const i32 b = xadj[v], e1 = xadj[v + 1];
+    if (e1 - b <= kGggpLongRow) continue;   // warp-uniform (scan mode only)
+    i32 j = rb[i];
+    for (i32 e0 = b; e0 < e1; e0 += 32) {
+      const i32 e = e0 + lane;
+      i32 u = 0;
+      bool keep = false;
+      if (e < e1) {
+        u = adjncy[e];
+        keep = lo[u] == p0;
+      }
+      const u32 m = __ballot_sync(kFull32, keep);
+      if (keep) {
+        const i32 at = j + __popc(m & ((1u << lane) - 1));
+        nb[at] = loc[u];
+        nw[at] = adjwgt[e];
+      }
+      j += __popc(m);
     }
   }
   __syncthreads();
