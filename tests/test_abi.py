@@ -164,3 +164,14 @@ def test_reader_large_files_parallel(pkg, gen, tmp_path):
     open(q, "w").write("\n".join(out) + "\n")
     with pytest.raises(pkg.GkwError, match="bad token"):
         pkg.read_metis(q)
+
+
+def test_server_config_defaults(pkg):
+    """The documented defaults of gkw_server_config (no device needed)."""
+    c = pkg.server_config()
+    assert c.slots == 2 and c.pool_bytes == 64 << 30 and c.slot_keep_bytes == 4 << 30
+    assert c.narrow_max_n == 262144 and c.batch_union == 1
+    assert c.batch_max_n == 1 << 22 and c.batch_graph_max_n == 262144
+    assert all(r == 0 for r in c.reserved)
+    c2 = pkg.server_config(slots=5, batch_union=0)
+    assert c2.slots == 5 and c2.batch_union == 0 and c2.batch_max_n == 1 << 22
