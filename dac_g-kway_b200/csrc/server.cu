@@ -295,7 +295,7 @@ void gkw_server::run_union(Slot& s, std::vector<JobPtr>& jobs) {
       fallback = true;
     }
   } catch (const Error& e) {
-    if (e.st == GKW_E_INVALID) {
+    if (e.st == GKW_E_INVALID || e.st == GKW_E_UNSUPPORTED) {   // a bad graph, or too many parts together
       fallback = true;
     } else {
       for (JobPtr& j : jobs) {
@@ -685,7 +685,9 @@ gkw_status gkw_partition_batch(gkw_server* s, const gkw_csr_batch* b, const gkw_
       try {
         ok = partition_batch_union(bh, hg, b->n_graphs, b->graph_ptr, b->k, uo, part_out, cuts.data());
       } catch (const Error& e) {
-        if (e.st != GKW_E_INVALID) throw;   // a bad graph: the per-graph path reports which one
+        // a bad graph, or more parts than one union holds: the per-graph path
+        // reports each graph's own status
+        if (e.st != GKW_E_INVALID && e.st != GKW_E_UNSUPPORTED) throw;
       }
       if (ok) {
         const auto t1 = Clock::now();
