@@ -370,10 +370,11 @@ int32_t metis_init_cb(void* user, int32_t n, const int32_t* xadj, const int32_t*
 }
 }  // namespace
 
-bool use_metis_init(gkw_options* opt, const std::string& path) {
+bool use_metis_init(gkw_options* opt, const std::string& path, bool recursive) {
   void* h = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL);
   if (!h) return false;
-  void* fn = dlsym(h, "METIS_PartGraphKway");
+  // METIS_PartGraphRecursive takes the same arguments (metis.h:185)
+  void* fn = dlsym(h, recursive ? "METIS_PartGraphRecursive" : "METIS_PartGraphKway");
   if (!fn) return false;
   opt->init_method = GKW_INIT_CALLBACK;
   opt->init_fn = metis_init_cb;
@@ -442,6 +443,8 @@ void gkw_free(void* p) { std::free(p); }
 // timers and the cut, write <cwd>/<out>.out.  Environment:
 //   GKW_METIS_LIB=<path to libmetis.so>  initial partition by METIS, as the
 //                                        reference does (default: on device)
+//   GKW_METIS_RECURSIVE=1                with GKW_METIS_LIB: METIS's recursive
+//                                        bisection instead of its k-way call
 //   GKW_SEED=<n>                         seed of the device initial partition
 void graph_partitioner(const std::string& GRAPH_FILE, const std::string& OUT_FILE, const int NUM_PARTITIONS) {
   gk::Graph graph(GRAPH_FILE);
@@ -449,7 +452,9 @@ void graph_partitioner(const std::string& GRAPH_FILE, const std::string& OUT_FIL
   gkw_default_options(&opt);
   if (const char* s = std::getenv("GKW_SEED")) opt.seed = std::strtoull(s, nullptr, 10);
   if (const char* lib = std::getenv("GKW_METIS_LIB")) {
-    if (!gk::use_metis_init(&opt, lib)) throw std::runtime_error(std::string("cannot load METIS from ") + lib);
+    const char* rb = std::getenv("GKW_METIS_RECURSIVE");
+    if (!gk::use_metis_init(&opt, lib, rb && *rb == '1'))
+      throw std::runtime_error(std::string("cannot load METIS from ") + lib);
   }
   gk::GraphPartitioner gp(&opt);
   gk::PartitionResult r = gp.partition_with_stats(graph, NUM_PARTITIONS);

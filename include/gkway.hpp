@@ -87,7 +87,8 @@ class GraphPartitioner {
 // Loads METIS from a shared library (the reference's initial partitioner,
 // gkway/metis_partition.hpp:46-47) and installs it as the initial-partition
 // callback in `opt`.  Returns false if the library or its symbol is missing.
-bool use_metis_init(gkw_options* opt, const std::string& libmetis_path);
+// recursive: METIS_PartGraphRecursive (metis.h:185) instead of METIS_PartGraphKway.
+bool use_metis_init(gkw_options* opt, const std::string& libmetis_path, bool recursive = false);
 
 }  // namespace gk
 

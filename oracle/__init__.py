@@ -81,6 +81,7 @@ def lib():
         L.orc_set_metis.argtypes = [ctypes.c_char_p]
         L.orc_has_metis.restype = ctypes.c_int
         L.orc_metis_kway.restype = ctypes.c_int
+        L.orc_metis_recursive.restype = ctypes.c_int
         L.orc_cut.restype = ctypes.c_int64
         L.orc_max_part_weight.restype = ctypes.c_float
         L.orc_max_part_weight.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]
@@ -158,6 +159,18 @@ def metis_kway(g, k: int):
     obj = ctypes.c_int64(0)
     rc = lib().orc_metis_kway(ctypes.c_int32(g.n), _p(g.xadj), _p(g.adjncy), _p(g.adjwgt), _p(g.vwgt),
                               ctypes.c_int32(k), _p(part), ctypes.byref(obj))
+    if rc != 1:
+        raise RuntimeError(f"METIS failed: {rc}")
+    return part, int(obj.value)
+
+
+def metis_recursive(g, k: int):
+    """METIS_PartGraphRecursive (the recursive-bisection alternative to the
+    k-way call of metis_partition.hpp:46-47, metis.h:185) -> (part, cut)."""
+    part = np.empty(g.n, np.int32)
+    obj = ctypes.c_int64(0)
+    rc = lib().orc_metis_recursive(ctypes.c_int32(g.n), _p(g.xadj), _p(g.adjncy), _p(g.adjwgt), _p(g.vwgt),
+                                   ctypes.c_int32(k), _p(part), ctypes.byref(obj))
     if rc != 1:
         raise RuntimeError(f"METIS failed: {rc}")
     return part, int(obj.value)

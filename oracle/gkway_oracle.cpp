@@ -206,20 +206,41 @@ i64 orc_contract(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, c
 typedef int (*metis_kway_fn)(i64*, i64*, i64*, i64*, i64*, i64*, i64*, i64*, double*, double*,
                              i64*, i64*, i64*);
 static metis_kway_fn g_metis = nullptr;
+// METIS_PartGraphRecursive (metis.h:185), same arguments: the recursive-
+// bisection alternative to the k-way initial partition.
+static metis_kway_fn g_metis_rb = nullptr;
 
 int orc_set_metis(const char* path) {
   void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
   if (!h) return -1;
   g_metis = (metis_kway_fn)dlsym(h, "METIS_PartGraphKway");
+  g_metis_rb = (metis_kway_fn)dlsym(h, "METIS_PartGraphRecursive");
   return g_metis ? 0 : -2;
 }
 
 int orc_has_metis() { return g_metis != nullptr; }
 
+// One METIS partitioning call (k-way or recursive bisection) on 64-bit
+// copies of the arrays.  Returns METIS's status (1 = METIS_OK).
+static int metis_call(metis_kway_fn fn, i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt,
+                      const i32* vwgt, i32 k, i32* part, i64* objval);
+
 // Returns METIS's status (1 = METIS_OK) or -1 if METIS is not loaded.
 int orc_metis_kway(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, const i32* vwgt,
                    i32 k, i32* part, i64* objval) {
   if (!g_metis) return -1;
+  return metis_call(g_metis, n, xadj, adjncy, adjwgt, vwgt, k, part, objval);
+}
+
+// The same through METIS_PartGraphRecursive; -1 if it is not loaded.
+int orc_metis_recursive(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt, const i32* vwgt,
+                        i32 k, i32* part, i64* objval) {
+  if (!g_metis_rb) return -1;
+  return metis_call(g_metis_rb, n, xadj, adjncy, adjwgt, vwgt, k, part, objval);
+}
+
+static int metis_call(metis_kway_fn fn, i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt,
+                      const i32* vwgt, i32 k, i32* part, i64* objval) {
   i64 nv = n, ncon = 1, nparts = k, cut = 0;
   i64 m = xadj[n];
   std::vector<i64> x(n + 1), a(std::max<i64>(m, 1)), w(std::max<i64>(m, 1)), vw(std::max(n, 1)),
@@ -227,8 +248,8 @@ int orc_metis_kway(i32 n, const i32* xadj, const i32* adjncy, const i32* adjwgt,
   for (i32 i = 0; i <= n; ++i) x[i] = xadj[i];
   for (i64 e = 0; e < m; ++e) { a[e] = adjncy[e]; w[e] = adjwgt[e]; }
   for (i32 i = 0; i < n; ++i) vw[i] = vwgt[i];
-  int rc = g_metis(&nv, &ncon, x.data(), a.data(), vw.data(), nullptr, w.data(), &nparts, nullptr,
-                   nullptr, nullptr, &cut, p.data());
+  int rc = fn(&nv, &ncon, x.data(), a.data(), vw.data(), nullptr, w.data(), &nparts, nullptr,
+              nullptr, nullptr, &cut, p.data());
   for (i32 i = 0; i < n; ++i) part[i] = (i32)p[i];
   if (objval) *objval = cut;
   return rc;

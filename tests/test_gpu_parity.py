@@ -188,6 +188,24 @@ def test_partition_reference_mode_matches_oracle(handle, orc, gen, pkg, cases):
 
 
 @pytest.mark.skipif("not __import__('oracle').has_metis()")
+def test_partition_metis_recursive_init_matches_oracle(handle, orc, gen, cases, pkg):
+    """METIS's recursive bisection (metis.h:185) on the coarsest graph through
+    the initial-partition callback, in both modes."""
+    def init(x, a, w, vw, kk):
+        return orc.metis_recursive(gen.Csr(x, a, w, vw), kk)[0]
+    for name, g in cases[:4]:
+        if g.m and g.adjwgt.min() <= 0:
+            continue   # METIS requires positive edge weights
+        for k in (8, 64):
+            for enforce in (0, 1):
+                o = pkg.default_options(enforce_balance=enforce)
+                part, cut, st = handle.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k, o, init=init)
+                ref, info = orc.partition(g, k, init=init, enforce_balance=bool(enforce))
+                assert np.array_equal(part, ref), (name, k, enforce)
+                assert cut == info["cut"], (name, k, enforce)
+
+
+@pytest.mark.skipif("not __import__('oracle').has_metis()")
 def test_partition_metis_init_matches_oracle(handle, orc, gen, cases, pkg):
     """The reference's own configuration: METIS on the coarsest graph."""
     def metis_init(x, a, w, vw, kk):

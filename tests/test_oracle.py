@@ -31,6 +31,32 @@ def test_metis_known_answers_n11(k, cut, maxpw):
     assert oracle.part_weights(g, part, k).max() == maxpw
 
 
+@needs_n11
+@pytest.mark.parametrize("k,cut,maxpw", [(8, 355, 257), (64, 1254, 33)])
+def test_metis_recursive_known_answers_n11(k, cut, maxpw):
+    # METIS_PartGraphRecursive, the recursive-bisection alternative init
+    # (metis.h:185); answers measured here with the bundled METIS 5.2.1
+    g = oracle.read_metis_graph(oracle.N11_PATH)
+    part, obj = oracle.metis_recursive(g, k)
+    assert obj == cut == oracle.cut(g, part)
+    assert oracle.part_weights(g, part, k).max() == maxpw
+    assert len(np.unique(part)) == k
+
+
+@needs_n11
+def test_partition_with_recursive_metis_init(gen):
+    g = oracle.read_metis_graph(oracle.N11_PATH)
+
+    def init(x, a, w, vw, kk):
+        return oracle.metis_recursive(gen.Csr(x, a, w, vw), kk)[0]
+    for k in (8, 64):
+        part, info = oracle.partition(g, k, init=init)
+        assert info["cut"] == oracle.cut(g, part)
+        assert part.min() >= 0 and part.max() < k
+        bal, binfo = oracle.partition(g, k, init=init, enforce_balance=True)
+        assert oracle.part_weights(g, bal, k).max() <= oracle.balance_cap(int(g.vwgt.sum()), k)
+
+
 # ---------------------------------------------------------------------------
 # A3 heavy-edge candidate (coarsen.hpp:39-78)
 # ---------------------------------------------------------------------------
