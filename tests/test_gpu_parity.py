@@ -193,7 +193,11 @@ def test_partition_metis_recursive_init_matches_oracle(handle, orc, gen, cases, 
     the initial-partition callback, in both modes."""
     def init(x, a, w, vw, kk):
         return orc.metis_recursive(gen.Csr(x, a, w, vw), kk)[0]
-    for name, g in cases[:4]:
+    # Delaunay and grid cases: on the skewed circuit case in reference mode the
+    # coarsest graph has vertices heavier than a bisection target, and METIS's
+    # recursive bisection reports "Cannot bisect a graph with 0 vertices" and
+    # leaves the part vector unspecified
+    for name, g in cases[:3]:
         if g.m and g.adjwgt.min() <= 0:
             continue   # METIS requires positive edge weights
         for k in (8, 64):
