@@ -175,3 +175,27 @@ def test_server_config_defaults(pkg):
     assert all(r == 0 for r in c.reserved)
     c2 = pkg.server_config(slots=5, batch_union=0)
     assert c2.slots == 5 and c2.batch_union == 0 and c2.batch_max_n == 1 << 22
+
+
+def test_server_argument_errors_without_device(pkg):
+    """Argument checks of the server entry points answer before any device
+    work (so they hold on a machine without a GPU too)."""
+    with pytest.raises(pkg.GkwError):
+        pkg.Server(0, slots=0)
+    with pytest.raises(pkg.GkwError):
+        pkg.Server(0, batch_max_n=-1)
+    with pytest.raises(pkg.GkwError):
+        pkg.Server(0, narrow_max_n=-5)
+
+
+def test_concat_graphs_layout(pkg, gen):
+    gs = [gen.delaunay(300, 1), gen.from_edges(0, np.zeros(0, np.int64), np.zeros(0, np.int64)),
+          gen.grid27(3, 3, 3)]
+    x, a, w, vw, gp = pkg.concat_graphs(gs)
+    assert list(gp) == [0, gs[0].n, gs[0].n, gs[0].n + gs[2].n]
+    assert x[-1] == a.shape[0] == sum(g.m for g in gs)
+    for i, g in enumerate(gs):
+        v0, v1 = gp[i], gp[i + 1]
+        assert np.array_equal(x[v0:v1 + 1] - x[v0], g.xadj)
+        assert np.array_equal(a[x[v0]:x[v1]] - v0, g.adjncy)
+        assert np.array_equal(w[x[v0]:x[v1]], g.adjwgt) and np.array_equal(vw[v0:v1], g.vwgt)
