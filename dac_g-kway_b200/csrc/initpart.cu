@@ -722,7 +722,10 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   if (trace) {
     GKW_CUDA(cudaEventSynchronize(ev[depth]));
     std::vector<unsigned long long> hp(2 * (size_t)std::max(depth, 1));
-    if (depth) GKW_CUDA(cudaMemcpy(hp.data(), prof, sizeof(u64) * 2 * depth, cudaMemcpyDeviceToHost));
+    if (depth) {
+      GKW_CUDA(cudaMemcpyAsync(hp.data(), prof, sizeof(u64) * 2 * depth, cudaMemcpyDeviceToHost, h.stream));
+      GKW_CUDA(cudaStreamSynchronize(h.stream));
+    }
     fprintf(stderr, "[gkw trace] init n=%d k=%d:", n, k);
     for (i32 d = 0; d < depth; ++d) {
       float ms = 0;
