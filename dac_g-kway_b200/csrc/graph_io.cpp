@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <charconv>
 #include <fstream>
 #include <iostream>
 #include <numeric>
@@ -280,6 +281,19 @@ size_t Graph::get_num_vertex() { return xadj_.empty() ? 0 : xadj_.size() - 1; }
 size_t Graph::get_num_edge() { return adjncy_.size(); }
 int Graph::get_total_vertex_weight() { return std::accumulate(vwgt_.begin(), vwgt_.end(), 0); }
 
+// One part id per line (graph.hpp:227-240), formatted into one buffer.
+static std::string format_parts(const int32_t* part, size_t n) {
+  std::string buf(n * 12 + 1, '\0');
+  char* p = &buf[0];
+  char* const end = p + buf.size();
+  for (size_t i = 0; i < n; ++i) {
+    p = std::to_chars(p, end, part[i]).ptr;
+    *p++ = '\n';
+  }
+  buf.resize((size_t)(p - buf.data()));
+  return buf;
+}
+
 void Graph::dump_result(const std::vector<int>& vertex_partition, const std::string& file_name) {
   char cwd[4096];
   std::string dir = getcwd(cwd, sizeof(cwd)) ? std::string(cwd) : std::string(".");
@@ -287,13 +301,9 @@ void Graph::dump_result(const std::vector<int>& vertex_partition, const std::str
   std::cout << "out_path:" << out_path << "\n";
   FILE* f = fopen(out_path.c_str(), "wb");
   if (!f) throw std::runtime_error("cannot open output file " + out_path);
-  std::string buf;
-  buf.reserve(vertex_partition.size() * 4);
-  char tmp[16];
-  for (int p : vertex_partition) {
-    int len = snprintf(tmp, sizeof(tmp), "%d\n", p);
-    buf.append(tmp, (size_t)len);
-  }
+  static_assert(sizeof(int) == sizeof(int32_t), "part ids are 32-bit");
+  const std::string buf = format_parts(reinterpret_cast<const int32_t*>(vertex_partition.data()),
+                                       vertex_partition.size());
   fwrite(buf.data(), 1, buf.size(), f);
   fclose(f);
 }
@@ -422,13 +432,7 @@ gkw_status gkw_write_partition(const char* path, int32_t n, const int32_t* part)
     gkw_io_set_error(std::string("cannot open ") + path);
     return GKW_E_INVALID;
   }
-  std::string buf;
-  buf.reserve((size_t)n * 4);
-  char tmp[16];
-  for (int32_t i = 0; i < n; ++i) {
-    int len = snprintf(tmp, sizeof(tmp), "%d\n", part[i]);
-    buf.append(tmp, (size_t)len);
-  }
+  const std::string buf = gk::format_parts(part, (size_t)n);
   size_t wr = fwrite(buf.data(), 1, buf.size(), f);
   fclose(f);
   return wr == buf.size() ? GKW_OK : GKW_E_INVALID;

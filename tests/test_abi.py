@@ -199,3 +199,13 @@ def test_concat_graphs_layout(pkg, gen):
         assert np.array_equal(x[v0:v1 + 1] - x[v0], g.xadj)
         assert np.array_equal(a[x[v0]:x[v1]] - v0, g.adjncy)
         assert np.array_equal(w[x[v0]:x[v1]], g.adjwgt) and np.array_equal(vw[v0:v1], g.vwgt)
+
+
+def test_write_partition_many_ids(pkg, tmp_path):
+    rng = np.random.default_rng(0)
+    part = np.concatenate([rng.integers(0, 40000, 50000), [0, 2 ** 31 - 1, -7]]).astype(np.int32)
+    p = str(tmp_path / "many.out")
+    pkg.write_partition(p, part)
+    assert open(p).read() == "".join(f"{v}\n" for v in part.tolist())
+    pkg.write_partition(p, np.zeros(0, np.int32))
+    assert open(p).read() == ""
