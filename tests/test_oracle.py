@@ -244,3 +244,27 @@ def test_star_and_path_hierarchies(gen):
         init = lambda x, a, w, vw, kk: oracle.init_partition(gen.Csr(x, a, w, vw), kk)
         part, info = oracle.partition(g, 4, init=init)
         assert info["cut"] == oracle.cut(g, part)
+
+
+# ---------------------------------------------------------------------------
+# hierarchy reuse across k: the levels do not depend on k except where the
+# coarsening stops, so the hierarchies of two k share their common prefix
+# (the premise of gkw_partition_multi_k)
+# ---------------------------------------------------------------------------
+def test_hierarchies_of_different_k_share_a_prefix(gen):
+    from graphs import weighted
+    init = lambda x, a, w, vw, kk: oracle.init_partition(gen.Csr(x, a, w, vw), kk)
+    for g in (gen.delaunay(20000, 5), weighted(gen, gen.delaunay(8000, 9), seed=4),
+              gen.circuit(30000, seed=2, levels=60, hub_max=3000)):
+        for enforce in (False, True):
+            levels = []
+            for k in (2, 8, 64, 256):
+                _, info = oracle.partition(g, k, init=init, enforce_balance=enforce)
+                levels.append((info["level_n"], info["level_m"]))
+            for (n1, m1) in levels:
+                for (n2, m2) in levels:
+                    L = min(len(n1), len(n2))
+                    assert n1[:L] == n2[:L] and m1[:L] == m2[:L]
+            # a larger k never coarsens deeper
+            depths = [len(n) for n, _ in levels]
+            assert depths == sorted(depths, reverse=True)
