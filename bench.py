@@ -180,6 +180,17 @@ def metis_cpu_baseline(g, budget_s: float = 12.0) -> dict:
             "cut": int(cut)}
 
 
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The largest x over all ranks: the whole job's step time is that of its
+    slowest replica."""
+    import torch
+    if world <= 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def bench_ours(args):
     import torch
     import __graft_entry__ as ge
@@ -238,10 +249,7 @@ def bench_ours(args):
     barrier()
     clocks = sampler.stop() if sampler else None
     ms = sum(step_ms) / len(step_ms)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, world, dev)
 
     # ---- e2e: host API, pinned host buffers, copies inside ----
     hx, ha, hw, hv = (torch.from_numpy(a).pin_memory() for a in (g.xadj, g.adjncy, g.adjwgt, g.vwgt))
@@ -263,10 +271,7 @@ def bench_ours(args):
         e2e_ms.append(e0.elapsed_time(e1))
     barrier()
     e2e = sum(e2e_ms) / len(e2e_ms)
-    e2e_t = torch.tensor([e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_max = float(e2e_t.item())
+    e2e_max = max_over_ranks(e2e, world, dev)
     assert int(cut_e) == int(cut), "host and device paths disagree"
 
     # ---- roofline of the dominant kernel, from the timed steps ----
