@@ -276,6 +276,18 @@ def bench_ours(args):
 
     # ---- roofline of the dominant kernel, from the timed steps ----
     roof, phase_roof = roofline_report(steps_stats)
+    h.close()
+
+    # ---- the batched and served forms (one GPU, rank 0 of a lone run) ----
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        del xadj, adjncy, adjwgt, vwgt, flush
+        torch.cuda.empty_cache()
+        for name, fn in (("batched", batched_summary), ("served", served_summary)):
+            try:
+                extras[name] = fn(args)
+            except Exception as e:   # reported in the line, not fatal to the headline
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         part_np = part.cpu().numpy()
@@ -305,8 +317,8 @@ def bench_ours(args):
                          "total": st["ms_total"]} if st else None,
             "clocks": clocks,
         }
+        line.update(extras)
         print(json.dumps(line))
-    h.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
@@ -528,10 +540,11 @@ def mixed_graphs(count, n_lo, n_hi, seed, tag):
     return graphs, specs
 
 
-def bench_batched(args):
+def batched_summary(args, sample_clocks=True):
     """Config: many independent small graphs in one call (gkw_partition_batch)
     against the plain path partitioning them one after another on the same
-    GPU.  Both sides go host arrays -> host parts; wall-clock time."""
+    GPU.  Both sides go host arrays -> host parts; wall-clock time.  Returns
+    the result object (clocks sampled over both timed parts)."""
     import torch
     import __graft_entry__ as ge
     torch.cuda.set_device(0)
@@ -547,6 +560,9 @@ def bench_batched(args):
     for g, k in list(zip(graphs, ks))[:8]:
         h.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k)
     torch.cuda.synchronize()
+    sampler = ClockSampler(0) if sample_clocks else None
+    if sampler:
+        sampler.start()
     t0 = time.perf_counter()
     plain = [h.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k) for g, k in zip(graphs, ks)]
     t_plain = time.perf_counter() - t0
@@ -555,27 +571,34 @@ def bench_batched(args):
     srv.partition_batch(x[: gp[8] + 1], a[: x[gp[8]]], w[: x[gp[8]]], vw[: gp[8]], gp[:9], ks[:8])   # warm
     times = []
     part = cuts = None
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, min(args.steps, 5))):
         t0 = time.perf_counter()
         part, cuts, sts = srv.partition_batch(x, a, w, vw, gp, ks)
         times.append(time.perf_counter() - t0)
+    clocks = sampler.stop() if sampler else None
     srv.close()
     same = all(np.array_equal(part[gp[i]:gp[i + 1]], plain[i][0]) and int(cuts[i]) == plain[i][1]
                for i in range(count))
     t_b = statistics.median(times)
-    print(json.dumps({
+    return {
         "workload": "batched", "metric": "graphs/s partitioned (batched form)", "value": count / t_b,
         "unit": "graphs/s", "edges_per_s": edges / t_b, "plain_graphs_per_s": count / t_plain,
         "plain_edges_per_s": edges / t_plain, "speedup_vs_plain": t_plain / t_b, "identical_to_plain": bool(same),
         "slots": args.slots, "steps": len(times), "timing": "wall clock, host arrays in, host parts out",
         "config": {"graphs": count, "n": "log-uniform 1k-64k", "generators": "Delaunay / 27-point grid / circuit",
-                   "k": list(BATCH_KS), "eps": EPS, "vertices": int(gp[-1]), "edges": edges}}))
+                   "k": list(BATCH_KS), "eps": EPS, "vertices": int(gp[-1]), "edges": edges},
+        "clocks": clocks}
 
 
-def bench_served(args):
+def bench_batched(args):
+    print(json.dumps(batched_summary(args)))
+
+
+def served_summary(args, sample_clocks=True):
     """Config: open-loop Poisson requests of mixed sizes at a sweep of offered
     loads, through the server (continuous batching) and through the plain
-    path (one handle serving requests first come, first served)."""
+    path (one handle serving requests first come, first served).  Returns the
+    result object (clocks sampled over every load)."""
     import threading
     import torch
     import __graft_entry__ as ge
@@ -585,6 +608,9 @@ def bench_served(args):
     rng = np.random.default_rng(3)
     ks_all = [2 ** int(rng.integers(1, 9)) for _ in range(4096)]
     out = []
+    sampler = ClockSampler(0) if sample_clocks else None
+    if sampler:
+        sampler.start()
     for rate in [float(r) for r in args.rates.split(",")]:
         nreq = int(max(20, min(args.requests, rate * args.duration)))
         arr = np.cumsum(rng.exponential(1.0 / rate, nreq))
@@ -637,11 +663,17 @@ def bench_served(args):
             if mode == "served":   # graphs partitioned together with a request, on average
                 res[mode]["mean_union_graphs"] = float(np.mean(together))
         out.append(res)
-    print(json.dumps({"workload": "served", "metric": "served graphs/s and p50/p99 latency vs plain",
-                      "unit": "graphs/s", "slots": args.slots, "loads": out,
-                      "config": {"pool_graphs": len(pool), "n": f"log-uniform 1k-{args.max_n}",
-                                 "k": "2..256 powers of two", "eps": EPS,
-                                 "timing": "wall clock, submit to result on the host"}}))
+    clocks = sampler.stop() if sampler else None
+    return {"workload": "served", "metric": "served graphs/s and p50/p99 latency vs plain",
+            "unit": "graphs/s", "slots": args.slots, "loads": out,
+            "config": {"pool_graphs": len(pool), "n": f"log-uniform 1k-{args.max_n}",
+                       "k": "2..256 powers of two", "eps": EPS, "requests_per_load": f"<= {args.requests}",
+                       "arrivals_s": args.duration, "timing": "wall clock, submit to result on the host"},
+            "clocks": clocks}
+
+
+def bench_served(args):
+    print(json.dumps(served_summary(args)))
 
 
 def bench_configs(args):
@@ -712,11 +744,13 @@ def main():
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "configs"])
     ap.add_argument("--graphs", type=int, default=4096, help="batched: number of graphs")
     ap.add_argument("--slots", type=int, default=2, help="batched/served: concurrent partitions")
-    ap.add_argument("--pool", type=int, default=48, help="served: distinct graphs requests draw from")
+    ap.add_argument("--pool", type=int, default=96, help="served: distinct graphs requests draw from")
     ap.add_argument("--max-n", type=int, default=2000000, help="served: largest graph")
-    ap.add_argument("--rates", default="10,100,500,2000", help="served: offered loads (requests/s)")
-    ap.add_argument("--requests", type=int, default=200, help="served: most requests per load")
-    ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals per load")
+    ap.add_argument("--rates", default="20,1000", help="served: offered loads (requests/s)")
+    ap.add_argument("--requests", type=int, default=400, help="served: most requests per load")
+    ap.add_argument("--duration", type=float, default=10.0, help="served: seconds of arrivals per load")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain workload: leave the batched and served objects out of the line")
     args = ap.parse_args()
     if args.workload == "configs":
         bench_configs(args)

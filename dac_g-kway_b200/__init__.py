@@ -616,6 +616,8 @@ def cut_noalloc(g, part, k: int, stream: int = 0):
     """gkw_cut_noalloc over torch CUDA tensors: (cut, part weights).  Allocates
     no device memory and needs no handle; runs on `stream` (a cudaStream_t as
     an int, 0 = the default stream) of the current device."""
+    if int(k) < 1:
+        raise GkwError(GKW_E_UNSUPPORTED, "gkw_cut_noalloc: k must be in [1, 8190]")
     c = _csr_dev(*g)
     cut = ctypes.c_int64()
     pw = np.zeros(k, np.int64)

@@ -19,23 +19,39 @@ static constexpr u32 kFull = 0xffffffffu;
 // the reference: the first position with minimum degree among the maximum
 // weight entries, or the vertex itself when no entry has positive weight.
 // ===========================================================================
+// Rows longer than kMatchLong are left to k_match_long (one CTA per row), so
+// a hub row never holds its group's lanes for thousands of dependent loads.
+constexpr i32 kMatchLong = 512;
+
+// the candidate rule's order: weight desc, neighbour degree asc, position asc
+__device__ __forceinline__ bool match_better(u32 w, u32 d, i32 pos, u32 bw, u32 bd, i32 bpos) {
+  return w > bw || (w == bw && (d < bd || (d == bd && pos < bpos)));
+}
+
 template <int G>
 __global__ void __launch_bounds__(256) k_match(i32 n, const i32* __restrict__ xadj,
                                                const i32* __restrict__ adjncy,
-                                               const i32* __restrict__ adjwgt, i32* __restrict__ cand) {
+                                               const i32* __restrict__ adjwgt, i32* __restrict__ cand,
+                                               i32* __restrict__ longlist, i32* __restrict__ longcnt) {
   const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   const i32 v = (i32)(t / G);
   const int sub = threadIdx.x & (G - 1);
   u32 bw = 0, bd = kFull;
   i32 bpos = INT_MAX, bu = -1;
+  bool skip = false;
   if (v < n) {
     const i32 beg = __ldg(xadj + v), end = __ldg(xadj + v + 1);
-    for (i32 e = beg + sub; e < end; e += G) {
-      const u32 w = (u32)__ldg(adjwgt + e);
-      if (w == 0 || w < bw) continue;
-      const i32 u = __ldg(adjncy + e);
-      const u32 d = (u32)(__ldg(xadj + u + 1) - __ldg(xadj + u));
-      if (w > bw || d < bd) { bw = w; bd = d; bpos = e; bu = u; }
+    skip = longlist != nullptr && end - beg > kMatchLong;   // uniform within the group
+    if (skip) {
+      if (sub == 0) longlist[atomicAdd(longcnt, 1)] = v;
+    } else {
+      for (i32 e = beg + sub; e < end; e += G) {
+        const u32 w = (u32)__ldg(adjwgt + e);
+        if (w == 0 || w < bw) continue;
+        const i32 u = __ldg(adjncy + e);
+        const u32 d = (u32)(__ldg(xadj + u + 1) - __ldg(xadj + u));
+        if (w > bw || d < bd) { bw = w; bd = d; bpos = e; bu = u; }
+      }
     }
   }
 #pragma unroll
@@ -44,26 +60,102 @@ __global__ void __launch_bounds__(256) k_match(i32 n, const i32* __restrict__ xa
     const u32 od = __shfl_xor_sync(kFull, bd, o, G);
     const i32 op = __shfl_xor_sync(kFull, bpos, o, G);
     const i32 ou = __shfl_xor_sync(kFull, bu, o, G);
-    const bool better = ow > bw || (ow == bw && (od < bd || (od == bd && op < bpos)));
-    if (better) { bw = ow; bd = od; bpos = op; bu = ou; }
+    if (match_better(ow, od, op, bw, bd, bpos)) { bw = ow; bd = od; bpos = op; bu = ou; }
   }
-  if (v < n && sub == 0) cand[v] = bw > 0 ? bu : v;
+  if (v < n && sub == 0 && !skip) cand[v] = bw > 0 ? bu : v;
 }
 
-void run_match(Handle& h, const DevGraph& g, i32* cand) {
+// One CTA per long row (listed by k_match): the threads stride the row --
+// its 16-byte-aligned body four entries per load when both arrays are
+// 16-byte aligned -- and the per-thread bests are reduced by the same rule.
+constexpr int kMatchLongThreads = 256;
+__global__ void __launch_bounds__(kMatchLongThreads) k_match_long(const i32* __restrict__ xadj,
+                                                                  const i32* __restrict__ adjncy,
+                                                                  const i32* __restrict__ adjwgt,
+                                                                  i32* __restrict__ cand,
+                                                                  const i32* __restrict__ longlist,
+                                                                  const i32* __restrict__ longcnt) {
+  __shared__ u32 s_w[kMatchLongThreads / 32], s_d[kMatchLongThreads / 32];
+  __shared__ i32 s_p[kMatchLongThreads / 32], s_u[kMatchLongThreads / 32];
+  const i32 nlong = *longcnt;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool vec = ((reinterpret_cast<uintptr_t>(adjncy) | reinterpret_cast<uintptr_t>(adjwgt)) & 15) == 0;
+  for (i32 r = blockIdx.x; r < nlong; r += gridDim.x) {
+    const i32 v = longlist[r];
+    const i32 beg = xadj[v], end = xadj[v + 1];
+    u32 bw = 0, bd = kFull;
+    i32 bpos = INT_MAX, bu = -1;
+    auto visit = [&](u32 w, i32 u, i32 e) {
+      if (w == 0 || w < bw) return;
+      const u32 d = (u32)(__ldg(xadj + u + 1) - __ldg(xadj + u));
+      if (match_better(w, d, e, bw, bd, bpos)) { bw = w; bd = d; bpos = e; bu = u; }
+    };
+    i32 body = beg, tail = end;
+    if (vec) {
+      body = (beg + 3) & ~3;
+      tail = body + ((end - body) & ~3);
+      if (tail < body) tail = body;
+      for (i32 e = beg + threadIdx.x; e < body && e < end; e += blockDim.x) visit((u32)adjwgt[e], adjncy[e], e);
+      for (i32 c = body / 4 + threadIdx.x; c < tail / 4; c += blockDim.x) {
+        const int4 w4 = __ldg(reinterpret_cast<const int4*>(adjwgt) + c);
+        const int4 u4 = __ldg(reinterpret_cast<const int4*>(adjncy) + c);
+        visit((u32)w4.x, u4.x, 4 * c);
+        visit((u32)w4.y, u4.y, 4 * c + 1);
+        visit((u32)w4.z, u4.z, 4 * c + 2);
+        visit((u32)w4.w, u4.w, 4 * c + 3);
+      }
+      for (i32 e = (tail > body ? tail : body) + threadIdx.x; e < end; e += blockDim.x)
+        visit((u32)adjwgt[e], adjncy[e], e);
+    } else {
+      for (i32 e = beg + threadIdx.x; e < end; e += blockDim.x) visit((u32)adjwgt[e], adjncy[e], e);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const u32 ow = __shfl_xor_sync(kFull, bw, o);
+      const u32 od = __shfl_xor_sync(kFull, bd, o);
+      const i32 op = __shfl_xor_sync(kFull, bpos, o);
+      const i32 ou = __shfl_xor_sync(kFull, bu, o);
+      if (match_better(ow, od, op, bw, bd, bpos)) { bw = ow; bd = od; bpos = op; bu = ou; }
+    }
+    if (lane == 0) {
+      s_w[wid] = bw;
+      s_d[wid] = bd;
+      s_p[wid] = bpos;
+      s_u[wid] = bu;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+        if (match_better(s_w[w], s_d[w], s_p[w], bw, bd, bpos)) { bw = s_w[w]; bd = s_d[w]; bpos = s_p[w]; bu = s_u[w]; }
+      cand[v] = bw > 0 ? bu : v;
+    }
+    __syncthreads();
+  }
+}
+
+void run_match(Handle& h, const DevGraph& g, i32* cand, i64 maxdeg) {
   if (g.n == 0) return;
   const double avg = g.n ? (double)g.m / g.n : 0.0;
   const int threads = 256;
+  const bool split = maxdeg < 0 || maxdeg > kMatchLong;
+  Pool::Mark mk = h.scratch.mark();
+  i32* longlist = split ? h.scratch.alloc_n<i32>(g.n) : nullptr;
+  i32* longcnt = split ? h.scratch.alloc_n<i32>(1) : nullptr;
+  if (split) GKW_CUDA(cudaMemsetAsync(longcnt, 0, sizeof(i32), h.stream));
   auto go = [&](auto kern, int G) {
     const i64 tot = (i64)g.n * G;
     launch(kern, (u32)((tot + threads - 1) / threads), threads, 0, h.stream, g.n, g.xadj, g.adjncy,
-           g.adjwgt, cand);
+           g.adjwgt, cand, longlist, longcnt);
   };
   if (avg <= 6.5) go(k_match<4>, 4);
   else if (avg <= 14) go(k_match<8>, 8);
   else if (avg <= 28) go(k_match<16>, 16);
   else go(k_match<32>, 32);
+  if (split)
+    launch(k_match_long, (u32)h.sm_count * 2, kMatchLongThreads, 0, h.stream, g.xadj, g.adjncy, g.adjwgt, cand,
+           (const i32*)longlist, (const i32*)longcnt);
   GKW_CHECK_LAUNCH();
+  h.scratch.release(mk);
 }
 
 // ===========================================================================
@@ -707,19 +799,55 @@ __global__ void __launch_bounds__(512) k_contract_cta(
   }
 }
 
-// one thread per coarse row (rows are short; consecutive threads touch
-// consecutive rows)
+// One warp per 32 consecutive coarse rows: the lanes scan the rows' lengths
+// and copy the 32 rows' entries as one flat range, each lane finding its
+// entry's row by a binary search over the lanes' prefix sums.  A hub row of
+// thousands of entries is then copied by all 32 lanes, not by one thread.
 __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__ ub, const i32* __restrict__ cnt,
                             const i32* __restrict__ cx, const i32* __restrict__ sadj,
-                            const i32* __restrict__ swgt, i32* __restrict__ cadj, i32* __restrict__ cwgt) {
+                            const i32* __restrict__ swgt, i32* __restrict__ cadj, i32* __restrict__ cwgt,
+                            i32* __restrict__ maxdeg) {
   const i32 nc = *ncp;
-  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
-    const i32 src = ub[c], dst = cx[c], len = cnt[c];
-    for (i32 i = 0; i < len; ++i) {
-      cadj[dst + i] = sadj[src + i];
-      cwgt[dst + i] = swgt[src + i];
+  const int lane = threadIdx.x & 31;
+  const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  i32 mx = 0;
+  for (i64 c0 = warp * 32; c0 < nc; c0 += nwarps * 32) {
+    const i64 c = c0 + lane;
+    i32 src = 0, dst = 0, len = 0;
+    if (c < nc) {
+      src = ub[c];
+      dst = cx[c];
+      len = cnt[c];
+    }
+    mx = len > mx ? len : mx;
+    i32 inc = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const i32 y = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const i32 total = __shfl_sync(kFull, inc, 31);
+    const i32 exc = inc - len;
+    for (i32 idx = lane; idx < total; idx += 32) {
+      // the row r with exc_r <= idx < inc_r: the first lane whose inclusive sum exceeds idx
+      i32 r = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const i32 probe = __shfl_sync(kFull, inc, r + step - 1);
+        if (probe <= idx) r += step;
+      }
+      const i32 rs = __shfl_sync(kFull, src, r), rd = __shfl_sync(kFull, dst, r), re = __shfl_sync(kFull, exc, r);
+      cadj[rd + (idx - re)] = sadj[rs + (idx - re)];
+      cwgt[rd + (idx - re)] = swgt[rs + (idx - re)];
     }
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const i32 y = __shfl_xor_sync(kFull, mx, o);
+    mx = mx > y ? mx : y;
+  }
+  if (lane == 0 && mx > 0) atomicMax(maxdeg, mx);
 }
 
 void ensure_arena(Handle& h, u64 words) {
@@ -789,7 +917,7 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc
   exclusive_scan_i32(h, cnt, cxadj, nu, d_mc);   // cxadj[n_c] = m_c (rows beyond n_c are empty)
   if (nc_ub > 0)
     launch(k_copy_rows, ceil_div(nc_ub, 256), 256, 0, h.stream, d_nc, ub, cnt, cxadj, sadj, swgt, cadjncy,
-           cadjwgt);
+           cadjwgt, &h.coop->maxdeg);
   GKW_CHECK_LAUNCH();
   h.scratch.release(mk);
 }
@@ -836,12 +964,13 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   Pool::Mark mk = h.scratch.mark();
   i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
   u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
-  run_match(h, g, cand);
+  run_match(h, g, cand, g.maxdeg);
   run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
   out.cmap = h.hier.alloc_n<i32>(std::max(g.n, 1));
   run_group_map(h, g.n, keys, cap, out.cmap, &h.coop->nc);
   h.scratch.release(mk);
   // coarse arrays at upper bounds (n_c <= n, m_c <= m); one host sync per level
+  GKW_CUDA(cudaMemsetAsync(&h.coop->maxdeg, 0, sizeof(i32), h.stream));
   out.cxadj = h.hier.alloc_n<i32>((i64)g.n + 1);
   out.cvwgt = h.hier.alloc_n<i32>(std::max(g.n, 1));
   out.cadjncy = h.hier.alloc_n<i32>(std::max<i64>(g.m, 1));
@@ -857,6 +986,7 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   CoopState c = read_coop(h);
   if (c.arena_overflow) {   // very long coarse rows: grow the arena and redo the step
     ensure_arena(h, (u64)((double)(h.arena_words + (u64)c.arena_need) * 1.25) + 1024);
+    GKW_CUDA(cudaMemsetAsync(&h.coop->maxdeg, 0, sizeof(i32), h.stream));
     run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
                  &h.coop->mc);
     c = read_coop(h);
@@ -866,6 +996,7 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   out.mc = c.mc;
   out.uf_rounds = c.uf_rounds;
   out.max_cvw = c.max_cvw;
+  out.maxdeg = c.maxdeg;
 }
 
 }  // namespace gkw

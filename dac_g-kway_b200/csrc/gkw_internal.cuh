@@ -88,6 +88,7 @@ struct DevGraph {
   const i32* adjncy = nullptr;
   const i32* adjwgt = nullptr;
   const i32* vwgt = nullptr;
+  i64 maxdeg = -1;   // longest row, when known (-1: unknown)
 };
 
 struct Level {
@@ -106,6 +107,7 @@ struct CoarsenOut {
   i32* cvwgt = nullptr;
   i32 uf_rounds = 0;
   i32 max_cvw = 0;   // heaviest coarse vertex
+  i32 maxdeg = 0;    // longest coarse row
 };
 
 // Grid barrier word of a cooperative launch (see device_util.cuh); zero
@@ -127,7 +129,7 @@ struct CoopState {
   i32 arena_overflow;
   i64 arena_need;
   i32 max_cvw;    // heaviest coarse vertex of the last coarsening step
-  i32 pad2;
+  i32 maxdeg;     // longest coarse row of the last coarsening step
 };
 
 // Bump arena for the hash tables of very long coarse rows (handle-owned,
@@ -214,7 +216,9 @@ inline void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, c
 void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total);
 
 // ---- coarsening (coarsen.cu) ----
-void run_match(Handle& h, const DevGraph& g, i32* cand);
+// maxdeg: the longest row if known (< 0: unknown); rows above the sub-warp
+// limit go to one CTA each.
+void run_match(Handle& h, const DevGraph& g, i32* cand, i64 maxdeg = -1);
 // returns the number of round launches the reference's loop would make
 // These run without host synchronisation; results that the host needs are
 // left in device memory (see CoopState) and read once per level.
@@ -327,7 +331,8 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
                            i32* d_part, const GggpBatch* batch = nullptr);
 
 // ---- driver (partitioner.cu) ----
-i64 validate(Handle& h, const DevGraph& g);   // total vertex weight; throws on malformed input
+// total vertex weight (and the longest row in *maxdeg); throws on malformed input
+i64 validate(Handle& h, const DevGraph& g, i64* maxdeg = nullptr);
 void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt, i32* d_part_out,
                     i64* cut_out, gkw_stats* stats);
 // The same from host arrays (a slice of a concatenated CSR: xadj values offset

@@ -73,6 +73,14 @@ __device__ __forceinline__ u64 move_key2(i32 g, i32 idx) {
 
 __device__ __forceinline__ i32 key_idx(u64 key) { return (i32)(0x3fffffffu - (u32)(key & 0x3fffffffu)); }
 
+typedef uint8_t u8;
+
+// A large sub-problem handed from the depth kernel to the per-trial kernel.
+struct BigParams {
+  i64 TL, WS, capL, capR;
+  i32 pm, p1;
+};
+
 // Topology of one sub-problem in local (member) indices: row i holds the
 // member's neighbours inside the sub-problem.
 struct LocalTopo {
@@ -393,7 +401,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     i32* __restrict__ lo_out, i32* __restrict__ hi_out, u64 seed, double eps, i32 trials,
     i32* g_rb, i32* g_rn, i32* g_deg, i32* g_vw, i32* g_nb, i32* g_nw, i32* g_state, u64* g_keys,
     u64* g_b1, u64* g_b2, size_t b1_stride, size_t b2_stride, const i32* __restrict__ part_base, const i32* __restrict__ part_v0,
-    const i32* __restrict__ part_v1, unsigned long long* prof) {
+    const i32* __restrict__ part_v1, unsigned long long* prof, i32* bigcount, i32* biglist, BigParams* bigp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ i32 s_cnt;
   __shared__ i32 s_warp[33];
@@ -510,10 +518,14 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   const i64 TL = WS * (pm - p0) / (p1 - p0);
   const i64 capL = (i64)((double)TL * (1.0 + eps * 0.5));
   const i64 capR = (i64)((double)(WS - TL) * (1.0 + eps * 0.5));
+  // Sub-problems above kGggpBlockMin members (when the caller passes the
+  // big-list): the local CSR goes to the global arrays and the trials run in
+  // k_gggp_big_trial, one CTA each.
+  const bool big = bigcount != nullptr && s > kGggpBlockMin;   // block-uniform
   // shared memory when the local CSR and the trials' state fit
   const i32 stw = gggp_state_words(s);
   const size_t need = sizeof(i32) * ((size_t)4 * s + 2 * (size_t)ES + (size_t)stw * trials);
-  const bool in_smem = need <= kGggpSmem;   // block-uniform
+  const bool in_smem = !big && need <= kGggpSmem;   // block-uniform
   LocalTopo T;
   i32 *rb, *rn, *deg, *vw, *nb, *nw, *state;
   if (in_smem) {
@@ -584,6 +596,20 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     }
   }
   __syncthreads();
+  if (big) {
+    if (threadIdx.x == 0) {
+      BigParams bp;
+      bp.TL = TL;
+      bp.WS = WS;
+      bp.capL = capL;
+      bp.capR = capR;
+      bp.pm = pm;
+      bp.p1 = p1;
+      bigp[p0] = bp;
+      biglist[atomicAdd(bigcount, 1)] = p0;
+    }
+    return;
+  }
   T.rb = rb;
   T.rn = rn;
   T.nb = nb;
@@ -645,6 +671,253 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Large sub-problems: one CTA per (sub-problem, trial).  The depth kernel has
+// built the local CSR in the global arrays (rows at the members' CSR
+// positions) and listed the sub-problem; here the trial's state -- C, R and
+// the block maxima of the growth keys, and, when they fit, the members'
+// weights to the sub-problem and vertex weights -- sits in the CTA's shared
+// memory, so a growth step is a chain of on-chip accesses instead of L2 round
+// trips, and the eight trials run on eight SMs.  A member's growth key is a
+// function of C, R and degS (it only rises while the member is unassigned),
+// so it is recomputed instead of stored.  Growth is one warp (the picks are
+// sequential); the refinement scans and the final cut use the whole CTA.
+// The picks, moves and results are those of gggp_trial.
+// ---------------------------------------------------------------------------
+constexpr int kBigThreads = 512;
+constexpr size_t kGggpBigSmem = 224 * 1024;
+
+__device__ __forceinline__ u64 member_key(const i32* C, const u8* R, const i32* deg, i32 i) {
+  if (R[i]) return 0ull;
+  const i32 c = C[i];
+  return grow_key(c > 0, 2 * c - deg[i], i);
+}
+
+__device__ __forceinline__ u64 block_max_u64(u64 x, u64* s_red) {
+  x = warp_max_u64(x);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  u64 r = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = r > s_red[w] ? r : s_red[w];
+  return r;
+}
+
+__device__ __forceinline__ i64 block_sum_i64(i64 x, i64* s_red) {
+  x = warp_sum_i64(x);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  i64 r = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += s_red[w];
+  return r;
+}
+
+__global__ void __launch_bounds__(kBigThreads, 1) k_gggp_big_trial(
+    i32 n, const i32* __restrict__ cnt, const i32* __restrict__ off, const i32* __restrict__ bigcount,
+    const i32* __restrict__ biglist, const BigParams* __restrict__ bigp, i32 trials, u64 seed,
+    const i32* __restrict__ part_base, const i32* __restrict__ g_rb, const i32* __restrict__ g_rn,
+    const i32* __restrict__ g_deg, const i32* __restrict__ g_vw, const i32* __restrict__ g_nb,
+    const i32* __restrict__ g_nw, i32* g_C, u8* g_R, i64* tcut, i64* tdev, unsigned long long* prof) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ u64 s_red[kBigThreads / 32];
+  __shared__ i64 s_red64[kBigThreads / 32];
+  __shared__ i64 s_wR;
+  const i32 j = blockIdx.x / trials, t = blockIdx.x % trials;
+  if (j >= *bigcount) return;
+  const i32 p0 = biglist[j];
+  const i32 s = cnt[p0], base = off[p0];
+  const BigParams P = bigp[p0];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const i32* rb = g_rb + base;
+  const i32* rn = g_rn + base;
+  const i32* nbr = g_nb;
+  const i32* nwt = g_nw;
+  const i32 nb1 = gggp_nb1(s), nb2 = gggp_nb2(s);
+  // shared layout: B1 | B2 | C | deg | vw | R, tiers by size (block-uniform)
+  u64* B1 = reinterpret_cast<u64*>(smem_raw);
+  u64* B2 = B1 + nb1;
+  unsigned char* q = reinterpret_cast<unsigned char*>(B2 + nb2);
+  const size_t fixed = sizeof(u64) * ((size_t)nb1 + nb2);
+  const size_t all = fixed + (size_t)13 * s, mid = fixed + (size_t)5 * s;
+  i32* C;
+  const i32 *deg, *vw;
+  u8* R;
+  if (all <= kGggpBigSmem) {
+    i32* sc = reinterpret_cast<i32*>(q);
+    i32* sd = sc + s;
+    i32* sv = sd + s;
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
+      sd[i] = g_deg[base + i];
+      sv[i] = g_vw[base + i];
+    }
+    C = sc;
+    deg = sd;
+    vw = sv;
+    R = reinterpret_cast<u8*>(sv + s);
+  } else if (mid <= kGggpBigSmem) {
+    C = reinterpret_cast<i32*>(q);
+    R = reinterpret_cast<u8*>(C + s);
+    deg = g_deg + base;
+    vw = g_vw + base;
+  } else {
+    C = g_C + (size_t)t * n + base;
+    R = g_R + (size_t)t * n + base;
+    deg = g_deg + base;
+    vw = g_vw + base;
+  }
+  for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
+    C[i] = 0;
+    R[i] = 0;
+  }
+  __syncthreads();
+  // block maxima of the initial keys (C = 0): one warp per block of 32 members
+  for (i32 b = wid; b < nb1; b += nw) {
+    const i32 i = (b << 5) + lane;
+    const u64 m = warp_max_u64(i < s ? grow_key(false, -deg[i], i) : 0ull);
+    if (lane == 0) B1[b] = m;
+  }
+  __syncthreads();
+  for (i32 c = wid; c < nb2; c += nw) {
+    const i32 b = (c << 5) + lane;
+    const u64 m = warp_max_u64(b < nb1 ? B1[b] : 0ull);
+    if (lane == 0) B2[c] = m;
+  }
+  __syncthreads();
+  const long long c0 = clock64();
+  if (wid == 0) {
+    // ---- growth: the picks of grow_blocks ----
+    const i32 p0_local = part_base ? p0 - part_base[p0] : p0;
+    i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0_local * 1315423911ull + (u64)t) % (u32)s);
+    i64 wR = 0;
+    for (i32 step = 0; step < s; ++step) {
+      if (step > 0) {
+        u64 best = 0;
+        for (i32 c = lane; c < nb2; c += 32) best = best > B2[c] ? best : B2[c];
+        best = warp_max_u64(best);
+        if (best == 0) break;
+        pick = key_idx(best);
+      }
+      const i64 w = (u32)vw[pick];
+      const i32 r0 = rb[pick], rc = rn[pick];
+      if (step > 0 && wR + w > P.TL && (wR + w - P.TL) > (P.TL - wR)) break;
+      if (lane == 0) R[pick] = 1;
+      wR += w;
+      __syncwarp();
+      constexpr i32 kU = 4;
+      for (i32 j0 = lane; j0 < rc; j0 += 32 * kU) {
+        i32 u[kU], ew[kU], ru[kU], du[kU], cu[kU];
+#pragma unroll
+        for (i32 x = 0; x < kU; ++x) {
+          const i32 jj = j0 + 32 * x;
+          u[x] = jj < rc ? nbr[r0 + jj] : -1;
+          ew[x] = jj < rc ? nwt[r0 + jj] : 0;
+        }
+#pragma unroll
+        for (i32 x = 0; x < kU; ++x) {
+          if (u[x] >= 0) {
+            ru[x] = R[u[x]];
+            du[x] = deg[u[x]];
+            cu[x] = atomicAdd(&C[u[x]], ew[x]) + ew[x];   // a row may list a neighbour twice
+          }
+        }
+#pragma unroll
+        for (i32 x = 0; x < kU; ++x) {
+          if (u[x] >= 0 && !ru[x]) {
+            const unsigned long long key = grow_key(cu[x] > 0, 2 * cu[x] - du[x], u[x]);
+            atomicMax(reinterpret_cast<unsigned long long*>(&B1[u[x] >> 5]), key);
+            atomicMax(reinterpret_cast<unsigned long long*>(&B2[u[x] >> 10]), key);
+          }
+        }
+      }
+      __syncwarp();
+      {   // the picked member leaves its blocks
+        const i32 b = pick >> 5, i = (b << 5) + lane;
+        const u64 m = warp_max_u64(i < s ? member_key(C, R, deg, i) : 0ull);
+        if (lane == 0) B1[b] = m;
+        __syncwarp();
+        const i32 c = pick >> 10, bb = (c << 5) + lane;
+        const u64 m2 = warp_max_u64(bb < nb1 ? B1[bb] : 0ull);
+        if (lane == 0) B2[c] = m2;
+        __syncwarp();
+      }
+      if (wR >= P.TL) break;
+    }
+    if (lane == 0) s_wR = wR;
+  }
+  __syncthreads();
+  const long long c1 = clock64();
+  i64 wR = s_wR;
+  // ---- refinement: positive-gain moves within the side caps (gggp_trial) ----
+  const i32 max_moves = gggp_max_moves(s);
+  for (i32 mv = 0; mv < max_moves; ++mv) {
+    u64 best = 0;
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
+      const i32 r = R[i], c = C[i], d = deg[i];
+      const i32 g = r ? (d - 2 * c) : (2 * c - d);
+      if (g > 0) {
+        const i64 w = (u32)vw[i];
+        const bool ok = r ? ((P.WS - wR) + w <= P.capR) : (wR + w <= P.capL);
+        if (ok) {
+          const u64 key = move_key2(g, i);
+          best = best > key ? best : key;
+        }
+      }
+    }
+    best = block_max_u64(best, s_red);
+    if (best == 0) break;
+    const i32 i = key_idx(best);
+    const i32 r = R[i];
+    __syncthreads();   // every thread has read R[i] before it flips
+    if (threadIdx.x == 0) R[i] = (u8)(r ^ 1);
+    wR += r ? -(i64)(u32)vw[i] : (i64)(u32)vw[i];
+    const i32 sign = r ? -1 : 1;
+    const i32 r0 = rb[i], rc = rn[i];
+    for (i32 jj = threadIdx.x; jj < rc; jj += blockDim.x) atomicAdd(&C[nbr[r0 + jj]], sign * nwt[r0 + jj]);
+    __syncthreads();
+  }
+  i64 cut = 0;
+  for (i32 i = threadIdx.x; i < s; i += blockDim.x)
+    if (R[i]) cut += deg[i] - C[i];
+  cut = block_sum_i64(cut, s_red64);
+  u8* Rout = g_R + (size_t)t * n + base;
+  if (Rout != R)
+    for (i32 i = threadIdx.x; i < s; i += blockDim.x) Rout[i] = R[i];
+  if (threadIdx.x == 0) {
+    tcut[(size_t)p0 * trials + t] = cut;
+    tdev[(size_t)p0 * trials + t] = wR > P.TL ? wR - P.TL : P.TL - wR;
+    if (prof) {
+      atomicMax(prof, (unsigned long long)(c1 - c0));
+      atomicMax(prof + 1, (unsigned long long)(clock64() - c1));
+    }
+  }
+}
+
+// The winning trial of each large sub-problem (smallest cut, then smallest
+// |W(R) - TL|, then the lower trial) splits it, as in k_gggp_depth.
+__global__ void k_gggp_big_pick(i32 n, const i32* __restrict__ cnt, const i32* __restrict__ off,
+                                const i32* __restrict__ bigcount, const i32* __restrict__ biglist,
+                                const BigParams* __restrict__ bigp, i32 trials, const i32* __restrict__ mlist,
+                                const u8* __restrict__ g_R, const i64* __restrict__ tcut,
+                                const i64* __restrict__ tdev, i32* __restrict__ lo_out, i32* __restrict__ hi_out) {
+  const i32 j = blockIdx.x;
+  if (j >= *bigcount) return;
+  const i32 p0 = biglist[j];
+  const i32 s = cnt[p0], base = off[p0];
+  const BigParams P = bigp[p0];
+  i32 b = 0;
+  for (i32 q = 1; q < trials; ++q) {
+    const i64 cq = tcut[(size_t)p0 * trials + q], cb = tcut[(size_t)p0 * trials + b];
+    if (cq < cb || (cq == cb && tdev[(size_t)p0 * trials + q] < tdev[(size_t)p0 * trials + b])) b = q;
+  }
+  const u8* R = g_R + (size_t)b * n + base;
+  for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
+    const i32 v = mlist[base + i];
+    if (R[i]) { lo_out[v] = p0; hi_out[v] = P.pm; }
+    else { lo_out[v] = P.pm; hi_out[v] = P.p1; }
+  }
+}
+
 __global__ void k_init_fill(i32 n, i32* lo, i32* hi, i32 k) {
   const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (v < n) { lo[v] = 0; hi[v] = k; }
@@ -684,6 +957,24 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
   const size_t b1_stride = (size_t)n / 32 + (size_t)k + 2, b2_stride = (size_t)n / 1024 + (size_t)k + 2;
   u64* g_b1 = h.scratch.alloc_n<u64>((size_t)kInitTrials * b1_stride);
   u64* g_b2 = h.scratch.alloc_n<u64>((size_t)kInitTrials * b2_stride);
+  // large sub-problems (more than kGggpBlockMin members; at most maxbig of
+  // them per depth) run their trials as separate CTAs
+  const i32 maxbig = n / (kGggpBlockMin + 1);
+  i32* bigcount = nullptr;
+  i32* biglist = nullptr;
+  BigParams* bigp = nullptr;
+  i64* tcut = nullptr;
+  i64* tdev = nullptr;
+  u8* g_R = nullptr;
+  if (maxbig > 0) {
+    bigcount = h.scratch.alloc_n<i32>(1);
+    biglist = h.scratch.alloc_n<i32>(maxbig);
+    bigp = h.scratch.alloc_n<BigParams>(k);
+    tcut = h.scratch.alloc_n<i64>((size_t)k * kInitTrials);
+    tdev = h.scratch.alloc_n<i64>((size_t)k * kInitTrials);
+    g_R = h.scratch.alloc_n<u8>((size_t)kInitTrials * n);
+    GKW_CUDA(cudaFuncSetAttribute(k_gggp_big_trial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpBigSmem));
+  }
   GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
   const u32 nb = ceil_div(n, 256);
   i32 depth = 0;
@@ -711,12 +1002,25 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     launch(k_init_count, nb, 256, 0, h.stream, n, lo[a], cnt);
     GKW_CHECK_LAUNCH();
     exclusive_scan_i32(h, cnt, off, k, nullptr);
+    if (maxbig > 0) GKW_CUDA(cudaMemsetAsync(bigcount, 0, sizeof(i32), h.stream));
+    const i32* pbase = batch ? batch->part_base : nullptr;
     launch(k_gggp_depth, k, kInitTrials * 32, kGggpSmem, h.stream, n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, lo[a],
            hi[a], cnt, off, mlist, loc, lo[b], hi[b], seed, eps, trials, g_rb, g_rn, g_deg, g_vw, g_nb, g_nw,
-           g_state, g_keys, g_b1, g_b2, b1_stride, b2_stride, batch ? batch->part_base : (const i32*)nullptr,
+           g_state, g_keys, g_b1, g_b2, b1_stride, b2_stride, pbase,
            batch ? batch->part_v0 : (const i32*)nullptr, batch ? batch->part_v1 : (const i32*)nullptr,
-           prof ? prof + 2 * d : nullptr);
+           prof ? prof + 2 * d : nullptr, bigcount, biglist, bigp);
     GKW_CHECK_LAUNCH();
+    if (maxbig > 0) {
+      launch(k_gggp_big_trial, (u32)maxbig * trials, kBigThreads, kGggpBigSmem, h.stream, n, (const i32*)cnt,
+             (const i32*)off, (const i32*)bigcount, (const i32*)biglist, (const BigParams*)bigp, trials, seed, pbase,
+             (const i32*)g_rb, (const i32*)g_rn, (const i32*)g_deg, (const i32*)g_vw, (const i32*)g_nb,
+             (const i32*)g_nw, g_state, g_R, tcut, tdev, prof ? prof + 2 * d : nullptr);
+      GKW_CHECK_LAUNCH();
+      launch(k_gggp_big_pick, (u32)maxbig, 256, 0, h.stream, n, (const i32*)cnt, (const i32*)off,
+             (const i32*)bigcount, (const i32*)biglist, (const BigParams*)bigp, trials, (const i32*)mlist,
+             (const u8*)g_R, (const i64*)tcut, (const i64*)tdev, lo[b], hi[b]);
+      GKW_CHECK_LAUNCH();
+    }
     if (trace) GKW_CUDA(cudaEventRecord(ev[d + 1], h.stream));
   }
   if (trace) {

@@ -65,9 +65,14 @@ extern "C" gkw_status gkw_cut_noalloc(const gkw_csr* d_graph, const int32_t* d_p
   cudaStream_t st = (cudaStream_t)stream;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (e != cudaSuccess) {
     set_error(std::string("gkw_cut_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
     return GKW_E_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("gkw_cut_noalloc: device index too large (the address table has " + std::to_string(kMaxDevices) +
+              " entries)");
+    return GKW_E_UNSUPPORTED;
   }
   i64* acc = nullptr;
   i32 sms = 0;

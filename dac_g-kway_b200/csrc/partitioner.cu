@@ -19,35 +19,74 @@ namespace gkw {
 // in range and not the vertex itself, weights >= 0.  Also sums vertex weights.
 // flags[0] bit0 bad xadj, bit1 bad id, bit2 self loop, bit3 negative weight.
 // ---------------------------------------------------------------------------
+// flags[1] receives the longest row.  Rows are checked by G lanes each (G
+// from the average row length); rows longer than kValidateLong are left to
+// k_validate_long, one CTA each, so that a hub row does not hold a lane for
+// thousands of loads.
+constexpr i32 kValidateLong = 512;
+
+__device__ __forceinline__ i32 validate_entries(i32 v, i32 n, i32 b, i32 e, i32 first, i32 step,
+                                                const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt) {
+  i32 f = 0;
+  for (i32 j = b + first; j < e; j += step) {
+    const i32 u = adjncy[j];
+    if (u < 0 || u >= n) f |= 2;
+    else if (u == v) f |= 4;
+    if (adjwgt[j] < 0) f |= 8;
+  }
+  return f;
+}
+
+template <int G>
 __global__ void k_validate(i32 n, i64 m, const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
                            const i32* __restrict__ adjwgt, const i32* __restrict__ vwgt,
-                           i32* __restrict__ flags, unsigned long long* __restrict__ wsum) {
-  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  i32 f = 0;
+                           i32* __restrict__ flags, unsigned long long* __restrict__ wsum, i32* __restrict__ longlist,
+                           i32* __restrict__ longcnt) {
+  const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const i64 v = t / G;
+  const int sub = threadIdx.x & (G - 1);
+  i32 f = 0, deg = 0;
   u64 w = 0;
   if (v < n) {
     const i32 b = xadj[v], e = xadj[v + 1];
     if (e < b || b < 0 || (i64)e > m) f |= 1;
     if (v == 0 && b != 0) f |= 1;
     if (v == n - 1 && (i64)e != m) f |= 1;
-    if (vwgt[v] < 0) f |= 8;
-    w = (u32)vwgt[v];
+    if (sub == 0) {
+      if (vwgt[v] < 0) f |= 8;
+      w = (u32)vwgt[v];
+    }
     if (!(f & 1)) {
-      for (i32 j = b; j < e; ++j) {
-        const i32 u = adjncy[j];
-        if (u < 0 || u >= n) f |= 2;
-        else if (u == v) f |= 4;
-        if (adjwgt[j] < 0) f |= 8;
+      deg = e - b;
+      if (deg > kValidateLong) {
+        if (sub == 0) longlist[atomicAdd(longcnt, 1)] = (i32)v;
+      } else {
+        f |= validate_entries((i32)v, n, b, e, sub, G, adjncy, adjwgt);
       }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
     f |= __shfl_xor_sync(0xffffffffu, f, o);
     w += __shfl_xor_sync(0xffffffffu, w, o);
+    const i32 d = __shfl_xor_sync(0xffffffffu, deg, o);
+    deg = d > deg ? d : deg;
   }
   if ((threadIdx.x & 31) == 0) {
     if (f) atomicOr(flags, f);
     if (w) atomicAdd(wsum, (unsigned long long)w);
+    if (deg) atomicMax(flags + 1, deg);
+  }
+}
+
+__global__ void k_validate_long(i32 n, const i32* __restrict__ xadj, const i32* __restrict__ adjncy,
+                                const i32* __restrict__ adjwgt, i32* __restrict__ flags,
+                                const i32* __restrict__ longlist, const i32* __restrict__ longcnt) {
+  const i32 nl = *longcnt;
+  for (i32 r = blockIdx.x; r < nl; r += gridDim.x) {
+    const i32 v = longlist[r];
+    i32 f = validate_entries(v, n, xadj[v], xadj[v + 1], threadIdx.x, blockDim.x, adjncy, adjwgt);
+    for (int o = 16; o > 0; o >>= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
+    if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
   }
 }
 
@@ -61,22 +100,32 @@ __global__ void k_sub_i32(i32* p, i64 n, i32 v) {
   if (i < n) p[i] -= v;
 }
 
-// returns total vertex weight; throws on malformed input
-i64 validate(Handle& h, const DevGraph& g) {
+// returns total vertex weight (the longest row in *maxdeg); throws on malformed input
+i64 validate(Handle& h, const DevGraph& g, i64* maxdeg) {
   Pool::Mark mk = h.scratch.mark();
-  i32* flags = h.scratch.alloc_n<i32>(4);
+  i32* flags = h.scratch.alloc_n<i32>(4);   // [0] error bits, [1] longest row, [2] long rows
   unsigned long long* ws = h.scratch.alloc_n<unsigned long long>(1);
+  i32* longlist = h.scratch.alloc_n<i32>(std::max(g.n, 1));
   GKW_CUDA(cudaMemsetAsync(flags, 0, sizeof(i32) * 4, h.stream));
   GKW_CUDA(cudaMemsetAsync(ws, 0, sizeof(u64), h.stream));
   if (g.n > 0) {
-    launch(k_validate, ceil_div(g.n, 256), 256, 0, h.stream, g.n, g.m, g.xadj, g.adjncy, g.adjwgt, g.vwgt,
-                                                         flags, ws);
+    const double avg = (double)g.m / g.n;
+    auto go = [&](auto kern, int G) {
+      launch(kern, ceil_div((u64)g.n * G, 256), 256, 0, h.stream, g.n, g.m, g.xadj, g.adjncy, g.adjwgt, g.vwgt,
+             flags, ws, longlist, flags + 2);
+    };
+    if (avg <= 6.5) go(k_validate<4>, 4);
+    else if (avg <= 14) go(k_validate<8>, 8);
+    else go(k_validate<16>, 16);
+    launch(k_validate_long, (u32)h.sm_count * 2, 256, 0, h.stream, g.n, g.xadj, g.adjncy, g.adjwgt, flags,
+           (const i32*)longlist, (const i32*)(flags + 2));
     GKW_CHECK_LAUNCH();
   }
-  GKW_CUDA(cudaMemcpyAsync(h.h_pinned, flags, sizeof(i32), cudaMemcpyDeviceToHost, h.stream));
+  GKW_CUDA(cudaMemcpyAsync(h.h_pinned, flags, sizeof(i32) * 2, cudaMemcpyDeviceToHost, h.stream));
   GKW_CUDA(cudaMemcpyAsync(h.h_pinned + 1, ws, sizeof(u64), cudaMemcpyDeviceToHost, h.stream));
   GKW_CUDA(cudaStreamSynchronize(h.stream));
   const i32 f = (i32)(h.h_pinned[0] & 0xffffffff);
+  if (maxdeg) *maxdeg = (i32)((u64)h.h_pinned[0] >> 32);
   const i64 W = h.h_pinned[1];
   h.scratch.release(mk);
   if (f & 1) throw Error{GKW_E_INVALID, "malformed xadj (must rise from 0 to nnz)"};
@@ -164,7 +213,8 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   cudaEvent_t* ev = h.tev;              // phase marks
   cudaEvent_t* lev = h.tev + 5;         // level kernel of slot s: lev[2s], lev[2s+1]
   GKW_CUDA(cudaEventRecord(ev[0], h.stream));
-  const i64 W = validate(h, g0);
+  i64 maxdeg0 = -1;
+  const i64 W = validate(h, g0, &maxdeg0);
   // the reference's MAX_PARTITION_WGT, or the default mode's strict cap
   const float maxw = opt.enforce_balance ? balance_cap(W, k, opt.eps) : max_part_weight(W, k, opt.eps);
   const i64 threshold = (i64)opt.threshold_factor * k;
@@ -172,6 +222,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
   // ---- coarsening (graph_partitioner.hpp:66-105) ----
   std::vector<Level> lv(1);
   lv[0].g = g0;
+  lv[0].g.maxdeg = maxdeg0;
   std::vector<i32> uf_rounds;
   while ((i64)lv.back().g.n > threshold && (i32)lv.size() < kMaxLevels) {
     CoarsenOut co;
@@ -202,6 +253,7 @@ void partition_impl(Handle& h, const DevGraph& g0, i32 k, const gkw_options& opt
     nl.g.adjncy = co.cadjncy;
     nl.g.adjwgt = co.cadjwgt;
     nl.g.vwgt = co.cvwgt;
+    nl.g.maxdeg = co.maxdeg;
     uf_rounds.push_back(co.uf_rounds);
     lv.push_back(nl);
   }
@@ -317,9 +369,11 @@ void partition_multi_impl(Handle& h, const DevGraph& g0, i32 nk, const i32* ks, 
   GKW_REQUIRE(g0.n >= 0 && g0.m >= 0 && g0.m < ((i64)1 << 31), GKW_E_UNSUPPORTED,
               "graphs need n >= 0 and nnz < 2^31");
   check_options(opt);
-  const i64 W = validate(h, g0);
+  i64 maxdeg0 = -1;
+  const i64 W = validate(h, g0, &maxdeg0);
   std::vector<Level> lv(1);
   lv[0].g = g0;
+  lv[0].g.maxdeg = maxdeg0;
   std::vector<i32> Lk(nk, -1);   // coarsest level of each k
   for (;;) {
     const i32 l = (i32)lv.size() - 1;
@@ -351,6 +405,7 @@ void partition_multi_impl(Handle& h, const DevGraph& g0, i32 nk, const i32* ks, 
     nx.g.adjncy = co.cadjncy;
     nx.g.adjwgt = co.cadjwgt;
     nx.g.vwgt = co.cvwgt;
+    nx.g.maxdeg = co.maxdeg;
     lv.push_back(nx);
   }
   for (i32 q = 0; q < nk; ++q) {

@@ -61,6 +61,8 @@ struct RoundState {
   u32 epoch;
   u64 rows;   // adjacency entries read by the gain updates of the rounds
   i64 cand_sum;   // refinement candidates over the rounds (diagnostic)
+  i32 needcheck;  // some part could exceed MAXW if every candidate moved (plain levels)
+  i32 nrisk;      // parts flagged in risk this round
 };
 
 
@@ -88,6 +90,11 @@ struct RefineCtx {
   u64* cands = nullptr;
   u64* top = nullptr;
   u32* pw = nullptr;
+  u32* pwd = nullptr;    // part-weight changes of a round's moves, folded into pw by the gain update
+  u32* pin = nullptr;    // weight the round's candidates would bring into each part
+  i32* msrc = nullptr;   // source part of each candidate, taken before any move is applied
+  u32* risk = nullptr;   // per part: 1 + its index among the round's at-risk parts, 0 if not at risk
+  i32* riskpart = nullptr;   // the at-risk parts by index
   RoundState* st = nullptr;
   u32* bmark = nullptr;
   i32* btarget = nullptr;
@@ -122,6 +129,11 @@ struct LevelArgs {
   i32 *part, *bnd, *gain, *target, *updflag, *inP, *U, *P0, *P1;
   u64 *cands, *top;
   u32* pw;
+  u32* pwd;           // plain levels: refinement moves add their weight changes here
+  u32* pin;           // plain levels: per-part inflow of the round's candidates
+  i32* msrc;          // plain levels: source part of each candidate
+  u32* risk;          // plain levels: 1 + index among the round's at-risk parts, or 0
+  i32* riskpart;      // plain levels: the at-risk parts by index
   RoundState* st;
   u32* bmark;
   i32 *btarget, *bgain, *blist;
@@ -333,15 +345,55 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
     u32* accb = acc - pb;
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
     rows += (unsigned long long)(end - beg);
+    u32 g = 0, q_best = (u32)p;
+    bool b;
+    if (end - beg <= 64) {   // warp-uniform: the row's part ids stay in registers (one load chain)
+      const i32 e0 = beg + lane, e1 = e0 + 32;
+      const bool h0 = e0 < end, h1 = e1 < end;
+      const i32 u0 = h0 ? a.adjncy[e0] : 0, u1 = h1 ? a.adjncy[e1] : 0;
+      const u32 w0 = h0 ? (u32)a.adjwgt[e0] : 0u, w1 = h1 ? (u32)a.adjwgt[e1] : 0u;
+      const i32 q0 = h0 ? ldc(a.part + u0) : p, q1 = h1 ? ldc(a.part + u1) : p;
+      if (h0) atomicAdd(&accb[q0], w0);
+      if (h1) atomicAdd(&accb[q1], w1);
+      b = __any_sync(kFullMask, q0 != p || q1 != p);
+      __syncwarp();
+      if (b) {
+        const u32 id = accb[p];
+        u64 best = 0;
+        if (q0 != p) best = ((u64)(accb[q0] - id) << 32) | (u32)(~(u32)q0);
+        if (q1 != p) {
+          const u64 key = ((u64)(accb[q1] - id) << 32) | (u32)(~(u32)q1);
+          best = best > key ? best : key;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const u64 ot = __shfl_xor_sync(kFullMask, best, o);
+          best = best > ot ? best : ot;
+        }
+        const u32 gb = (u32)(best >> 32);
+        if (gb > 0) { g = gb; q_best = ~(u32)best; }
+      }
+      if (lane == 0) {
+        a.updflag[v] = 0;
+        a.bnd[v] = b ? 1 : 0;
+        a.gain[v] = (i32)g;
+        a.target[v] = (i32)q_best;
+        if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) Pout[atomicAdd(pcount, 1)] = v;
+      }
+      __syncwarp();
+      if (h0) accb[q0] = 0;
+      if (h1) accb[q1] = 0;
+      __syncwarp();
+      continue;
+    }
     bool bl = false;
     for (i32 e = beg + lane; e < end; e += 32) {
       const i32 q = ldc(a.part + a.adjncy[e]);
       atomicAdd(&accb[q], (u32)a.adjwgt[e]);
       bl |= (q != p);
     }
-    const bool b = __any_sync(kFullMask, bl);
+    b = __any_sync(kFullMask, bl);
     __syncwarp();
-    u32 g = 0, q_best = (u32)p;
     if (b) {
       const u32 id = accb[p];
       u64 best = 0;
@@ -377,9 +429,17 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
 // Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
 // boundary, gain > 0, a valid destination by weight, and no neighbour with a
 // smaller id that is itself positive and valid.  P is compacted on the way.
+// Plain levels also keep each candidate's source part (msrc) and add its
+// weight to the inflow bound of its destination (pin): if no part could pass
+// MAXW even with every candidate moved in, every prefix of the sorted moves
+// is balanced and the select phase needs neither the sort nor the check;
+// otherwise the parts that could pass it are flagged in risk.
 __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
   RoundState* st = a.st;
-  if (a.batch && blockIdx.x == 0 && threadIdx.x == 0) *a.mcount = 0;   // the round's moves
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (a.batch) *a.mcount = 0;   // the round's moves
+    else st->ucount = 0;          // U was consumed by the last gain update
+  }
   const int lane = threadIdx.x & 31;
   const i32 nP = ldc(&st->pcount[0]);
   // entry r*32*W + lane*W + w goes to warp w, lane `lane`: the entries of a
@@ -389,13 +449,20 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
   for (i64 r0 = 0; r0 < nP; r0 += 32 * W) {
     const i64 i = r0 + lane * W + gw;
     bool check = false;
-    i32 v = 0, g = 0;
+    i32 v = 0, g = 0, t = 0, p = 0, xb = 0, xe = 0;
+    u32 pwt = 0, vw = 0;
     if (i < nP) {
       v = ldc(a.P0 + i);
       g = ldc(a.gain + v);
-      if (g > 0 && ldc(a.bnd + v) && graph_flag(a, v, 0)) {   // batched: graphs that refine here
-        const i32 t = ldc(a.target + v);
-        check = valid_move(ldc(a.pw + t), (u32)a.vwgt[v], maxw_of(a, t));
+      const i32 bv = ldc(a.bnd + v);
+      t = ldc(a.target + v);   // loads issued together; used only when v is positive
+      vw = (u32)a.vwgt[v];
+      xb = a.xadj[v];
+      xe = a.xadj[v + 1];
+      if (!a.batch) p = ldc(a.part + v);
+      if (g > 0 && bv && graph_flag(a, v, 0)) {   // batched: graphs that refine here
+        pwt = ldc(a.pw + t);
+        check = valid_move(pwt, vw, maxw_of(a, t));
       }
     }
     // independent-set test, one candidate at a time, neighbours across lanes
@@ -405,13 +472,14 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
       const int src = __ffs(pend) - 1;
       pend &= pend - 1;
       const i32 cv = __shfl_sync(kFullMask, v, src);
-      const i32 beg = a.xadj[cv], end = a.xadj[cv + 1];
+      const i32 beg = __shfl_sync(kFullMask, xb, src), end = __shfl_sync(kFullMask, xe, src);
       bool blocked = false;
       for (i32 e = beg + lane; e < end && !blocked; e += 32) {
         const i32 u = a.adjncy[e];
-        if (u < cv && ldc(a.gain + u) > 0) {
-          const i32 tu = ldc(a.target + u);
-          blocked = valid_move(ldc(a.pw + tu), (u32)a.vwgt[u], maxw_of(a, tu));
+        if (u < cv) {
+          const i32 gu = ldc(a.gain + u), tu = ldc(a.target + u);   // issued together
+          const u32 vu = (u32)a.vwgt[u];
+          if (gu > 0) blocked = valid_move(ldc(a.pw + tu), vu, maxw_of(a, tu));
         }
       }
       const bool any_blocked = __any_sync(kFullMask, blocked);
@@ -423,7 +491,27 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
         a.cands[__ldg(a.gvbase + gv) + atomicAdd(a.gcc + gv, 1)] = move_key(g, v);
       }
     } else {
+      u32 before = 0;
+      if (cand) {
+        a.msrc[v] = p;
+        before = atomicAdd(a.pin + t, vw);
+      }
       block_append64(cand, move_key(g, v), a.cands, &st->ccount, s_cnt, s_base);
+      // the final inflow of t is at least before + vw, and (float)(u32) is
+      // monotone, so one add that passes MAXW shows the final sum passes it
+      if (cand) {
+        const u64 in = (u64)pwt + before + vw;
+        if (in >> 32 || __uint2float_rn((u32)in) > a.maxw) {
+          // part t could pass MAXW: the select phase checks it.  The first
+          // thread to flag it gives it a dense index (read after the barrier).
+          if (atomicCAS(a.risk + t, 0u, 0xffffffffu) == 0u) {
+            const i32 id = atomicAdd(&st->nrisk, 1);
+            a.riskpart[id] = t;
+            atomicExch(a.risk + t, (u32)id + 1u);
+          }
+          st->needcheck = 1;
+        }
+      }
     }
   }
 }
@@ -524,15 +612,17 @@ __device__ u64* block_merge_sort(u64* s, u64* t, i32 P) {
 // that index range in a difference array.  The result is the largest
 // unmarked index, 0 if every index is marked (move 0 is applied regardless,
 // as in the reference: its -1 case is dead code, uncoarsen.hpp:481-488).
-// Block 0 only; t is a second buffer of kSortMax keys; s is overwritten.
-__device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u32* s_warp) {
+// Block-wide; t is a second buffer of kSortMax keys; s is overwritten.  The
+// moves' source parts are read from srcp (the level's parts, or the
+// candidates' parts taken before any move of the round was applied).
+__device__ i32 refine_balanced_pos(const LevelArgs& a, u64* s, u64* t, i32 B, u32* s_warp, const i32* srcp) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const i32 E = 2 * B;
   i32 P = 32;
   while (P < E) P <<= 1;
   for (i32 m = threadIdx.x; m < B; m += blockDim.x) {
     const i32 v = (i32)(u32)s[m];
-    const i32 src = ldc(a.part + v), dst = ldc(a.target + v);
+    const i32 src = ldc(srcp + v), dst = ldc(a.target + v);
     const u32 w = (u32)a.vwgt[v];
     t[2 * m] = ((u64)(u32)dst << 43) | ((u64)m << 32) | w;
     t[2 * m + 1] = ((u64)(u32)src << 43) | ((u64)m << 32) | (u32)(0u - w);
@@ -850,35 +940,22 @@ __device__ i32 select_greedy(const LevelArgs& a, u64* s, i32* greedy, i32 B, i32
   return nsel;
 }
 
-// Plain level: block 0 selects from all candidates.  Resets the per-round
-// counters.
-__device__ void ph_select(const LevelArgs& a, u64* s, i32* greedy, u32* s_warp, bool balance_mode) {
+// Plain level, balance rounds: block 0 sorts the candidates and keeps the
+// greedy selection.  Resets the per-round counters.
+__device__ void ph_bal_select(const LevelArgs& a, u64* s, i32* greedy) {
   if (blockIdx.x != 0) return;
   RoundState* st = a.st;
   const i32 cnt = ldc(&st->ccount);
   if (cnt == 0) {
-    if (threadIdx.x == 0) {
-      if (balance_mode) st->bdone = 1;
-      else st->done = 1;
-    }
+    if (threadIdx.x == 0) st->bdone = 1;
     return;
   }
   const i32 B = select_sort(a, a.cands, cnt, s, greedy);
-  if (!balance_mode) {
-    trace_mark(a, 25);
-    if (threadIdx.x == 0) st->cand_sum += cnt;
-    for (i32 i = threadIdx.x; i < B; i += blockDim.x) a.top[i] = s[i];
-    const i32 pos = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp);
-    trace_mark(a, 26);
-    if (threadIdx.x == 0) st->pos = pos;
-  } else {
-    const i32 nsel = select_greedy(a, s, greedy, B, 0, a.k);
-    for (i32 i = threadIdx.x; i < nsel; i += blockDim.x) a.top[i] = s[i];
-    if (threadIdx.x == 0) st->firstbad = nsel;   // moves 0..nsel-1 of top are applied
-  }
+  const i32 nsel = select_greedy(a, s, greedy, B, 0, a.k);
+  for (i32 i = threadIdx.x; i < nsel; i += blockDim.x) a.top[i] = s[i];
   __syncthreads();
   if (threadIdx.x == 0) {
-    st->B = B;
+    st->firstbad = nsel;   // moves 0..nsel-1 of top are applied
     st->ccount = 0;
     st->ucount = 0;
   }
@@ -911,7 +988,7 @@ __device__ void ph_select_batch(const LevelArgs& a, u64* s, i32* greedy, u32* s_
     if (!balance_mode) {
       // the check below overwrites s: park the sorted moves in the bucket
       for (i32 i = threadIdx.x; i < B; i += blockDim.x) cg[i] = s[i];
-      keep = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp) + 1;
+      keep = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp, a.part) + 1;
     } else {
       keep = select_greedy(a, s, greedy, B, __ldg(a.gpbase + g), __ldg(a.gk + g));
       for (i32 i = threadIdx.x; i < keep; i += blockDim.x) cg[i] = s[i];
@@ -944,15 +1021,35 @@ __device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
   for (i32 t = threadIdx.x; t < c; t += blockDim.x) U[S.base + t] = S.buf[t];
 }
 
-// Apply the moves 0..pos, pos = the largest balanced prefix index
-// (uncoarsen.hpp:284-286 keep the max balanced index; prefix 0 is always
-// balanced).  Part weights change by the same sums as pw[p] += D[p][pos]; moved
-// vertices and their neighbours are flagged and appended to U
-// (uncoarsen.hpp:290-323).  One warp per move.
+// One move, by one warp: v goes to its target; v and its neighbours are
+// flagged for the gain update and appended to U (uncoarsen.hpp:290-323).
+// The part-weight change goes to pwc: pw itself, or the round's delta array
+// when other CTAs may still read pw in the same phase.
+__device__ __forceinline__ void apply_move(const LevelArgs& a, UStage& S, u64 key, u32* pwc,
+                                           unsigned long long* s_gsum) {
+  const int lane = threadIdx.x & 31;
+  const i32 v = (i32)(u32)key;
+  const i32 s = ldc(a.part + v), d = ldc(a.target + v);
+  const i32 beg = a.xadj[v], end = a.xadj[v + 1];   // issued beside the loads above
+  if (lane == 0) {
+    const u32 w = (u32)a.vwgt[v];
+    atomicAdd(&pwc[d], w);
+    atomicSub(&pwc[s], w);
+    a.part[v] = d;
+    atomicAdd(s_gsum, (unsigned long long)(i64)key_gain(key));
+    if (atomicExch(&a.updflag[v], 1) == 0) ustage_push(S, v, a.U, &a.st->ucount);
+  }
+  for (i32 e = beg + lane; e < end; e += 32) {
+    const i32 u = a.adjncy[e];
+    if (atomicExch(&a.updflag[u], 1) == 0) ustage_push(S, u, a.U, &a.st->ucount);
+  }
+}
+
+// Batched level: apply every graph's kept moves, top[0..mcount).  One warp
+// per move.
 __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
   RoundState* st = a.st;
-  const i32 pos = a.batch ? ldc(a.mcount) - 1 : ldc(&st->pos);   // batched: every graph's kept moves
-  const int lane = threadIdx.x & 31;
+  const i32 pos = ldc(a.mcount) - 1;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
   __shared__ unsigned long long s_gsum;
@@ -961,30 +1058,258 @@ __device__ void ph_apply_refine(const LevelArgs& a, UStage& S) {
     S.cnt = 0;
   }
   __syncthreads();
-  if (warp == 0 && lane == 0) {
+  if (warp == 0 && (threadIdx.x & 31) == 0) {
     st->rounds += 1;
     st->moves += pos + 1;
   }
-  for (i64 j = warp; j <= pos; j += nwarps) {
-    const u64 key = ldc(a.top + j);
+  for (i64 j = warp; j <= pos; j += nwarps) apply_move(a, S, ldc(a.top + j), a.pw, &s_gsum);
+  ustage_flush(S, a.U, &st->ucount);
+  if (threadIdx.x == 0 && s_gsum) atomicAdd((unsigned long long*)&st->gain_sum, s_gsum);
+}
+
+// Block-wide min (or max) of one u64 per thread; every thread gets the result.
+template <bool kMax>
+__device__ __forceinline__ u64 block_reduce_u64(u64 x, u64* s_tmp) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const u64 y = __shfl_xor_sync(kFullMask, x, o);
+    x = kMax ? (y > x ? y : x) : (y < x ? y : x);
+  }
+  __syncthreads();
+  if (lane == 0) s_tmp[wid] = x;
+  __syncthreads();
+  u64 r = s_tmp[0];
+  for (int w = 1; w < nw; ++w) r = kMax ? (s_tmp[w] > r ? s_tmp[w] : r) : (s_tmp[w] < r ? s_tmp[w] : r);
+  return r;
+}
+
+constexpr i32 kRiskEvents = 1024;   // event limit of the at-risk balance check
+constexpr i32 kRiskParts = 1024;    // at-risk part limit of that check
+
+// The balance check of a round whose candidates are all kept (cnt <= cap),
+// without sorting them.  Only parts flagged in risk can be over MAXW at any
+// prefix (a part's running change D never exceeds its inflow bound), so only
+// the moves into or out of those parts matter.  Each such move is an event
+// (part, key, +-w), and the events are grouped by part (a counting sort over
+// the parts' dense indices).  A part's D after one of its events is the sum of
+// its events with keys up to that key, and it holds until the part's next
+// event.  An event with D > 0 and (float)(pw + D) > MAXW marks the key range
+// [key, next key of the part) -- the same index ranges the reference's table
+// marks (uncoarsen.hpp:239-288), in key order instead of index order.  The
+// applied moves are those with key <= K*, K* = the largest unmarked key, or
+// the smallest key if every key is marked (prefix 0 always counts as
+// balanced, :481-488).  Returns false (block-uniform) beyond kRiskEvents events
+// or kRiskParts parts; the caller then sorts.
+__device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greedy, u64* keep, u64* s_tmp,
+                                 u32* s_warp, u64* kstar, i32* napplied) {
+  __shared__ i32 s_ne;
+  const i32 nrisk = ldc(&a.st->nrisk);
+  if (nrisk > kRiskParts) return false;   // block-uniform
+  u64* ev_key = s + kMaxMoveCap;      // [kRiskEvents] events as found
+  u64* gk = ev_key + kRiskEvents;     // [kRiskEvents] grouped by part
+  u64* gnext = keep;                  // [kRiskEvents] next key of the same part
+  i32* ev_b = greedy;                 // [kRiskEvents] part index of each event
+  i32* ev_d = ev_b + kRiskEvents;     // [kRiskEvents] weight change
+  i32* gb = ev_d + kRiskEvents;       // grouped: part index
+  i32* gd = gb + kRiskEvents;         // grouped: weight change
+  i32* gbad = gd + kRiskEvents;       // grouped: marks its range
+  i32* bcnt = gbad + kRiskEvents;     // [kRiskParts] events per part
+  i32* boff = bcnt + kRiskParts;      // [kRiskParts] first grouped slot
+  i32* bfill = boff + kRiskParts;     // [kRiskParts]
+  if (threadIdx.x == 0) s_ne = 0;
+  for (i32 b = threadIdx.x; b < nrisk; b += blockDim.x) {
+    bcnt[b] = 0;
+    bfill[b] = 0;
+  }
+  __syncthreads();
+  u64 kmax = 0;
+  for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const u64 key = ldc(a.cands + i);
+    s[i] = key;
+    kmax = key > kmax ? key : kmax;
     const i32 v = (i32)(u32)key;
-    const i32 s = ldc(a.part + v), d = ldc(a.target + v);
-    const i32 beg = a.xadj[v], end = a.xadj[v + 1];   // issued beside the loads above
-    if (lane == 0) {
-      const u32 w = (u32)a.vwgt[v];
-      atomicAdd(&a.pw[d], w);
-      atomicSub(&a.pw[s], w);
-      a.part[v] = d;
-      atomicAdd(&s_gsum, (unsigned long long)(i64)key_gain(key));
-      if (atomicExch(&a.updflag[v], 1) == 0) ustage_push(S, v, a.U, &st->ucount);
+    const i32 src = ldc(a.msrc + v), dst = ldc(a.target + v);
+    const i32 w = a.vwgt[v];
+    const u32 rs = ldc(a.risk + src), rd = ldc(a.risk + dst);
+    if (rs) {
+      const i32 e = atomicAdd(&s_ne, 1);
+      if (e < kRiskEvents) {
+        ev_key[e] = key;
+        ev_b[e] = (i32)rs - 1;
+        ev_d[e] = -w;
+        atomicAdd(&bcnt[rs - 1], 1);
+      }
     }
-    for (i32 e = beg + lane; e < end; e += 32) {
-      const i32 u = a.adjncy[e];
-      if (atomicExch(&a.updflag[u], 1) == 0) ustage_push(S, u, a.U, &st->ucount);
+    if (rd) {
+      const i32 e = atomicAdd(&s_ne, 1);
+      if (e < kRiskEvents) {
+        ev_key[e] = key;
+        ev_b[e] = (i32)rd - 1;
+        ev_d[e] = w;
+        atomicAdd(&bcnt[rd - 1], 1);
+      }
+    }
+  }
+  __syncthreads();
+  const i32 ne = s_ne;
+  if (ne > kRiskEvents) return false;   // block-uniform
+  {   // first grouped slot of each part: exclusive scan, two parts per thread
+    const i32 b0 = 2 * threadIdx.x;
+    const u32 c0 = b0 < nrisk ? (u32)bcnt[b0] : 0u, c1 = b0 + 1 < nrisk ? (u32)bcnt[b0 + 1] : 0u;
+    u32 tot;
+    const u32 ex = block_exscan_u32(c0 + c1, s_warp, tot);
+    if (b0 < nrisk) boff[b0] = (i32)ex;
+    if (b0 + 1 < nrisk) boff[b0 + 1] = (i32)(ex + c0);
+  }
+  __syncthreads();
+  for (i32 e = threadIdx.x; e < ne; e += blockDim.x) {
+    const i32 b = ev_b[e];
+    const i32 at = boff[b] + atomicAdd(&bfill[b], 1);
+    gk[at] = ev_key[e];
+    gd[at] = ev_d[e];
+    gb[at] = b;
+  }
+  __syncthreads();
+  for (i32 j = threadIdx.x; j < ne; j += blockDim.x) {
+    const i32 b = gb[j];
+    const u64 kj = gk[j];
+    i32 D = 0;
+    u64 knext = ~0ull;
+    for (i32 f = boff[b], fe = boff[b] + bcnt[b]; f < fe; ++f) {
+      const u64 kf = gk[f];
+      if (kf <= kj) D += gd[f];
+      else knext = kf < knext ? kf : knext;
+    }
+    gnext[j] = knext;
+    gbad[j] = D > 0 && __uint2float_rn((u32)D + ldc(a.pw + ldc(a.riskpart + b))) > a.maxw;
+  }
+  u64 K = block_reduce_u64<true>(kmax, s_tmp);   // (its barriers publish the marks)
+  for (i32 guard = 0; guard <= ne; ++guard) {
+    // smallest start of a marked range that covers K
+    u64 lo = ~0ull;
+    for (i32 j = threadIdx.x; j < ne; j += blockDim.x)
+      if (gbad[j] && gk[j] <= K && K < gnext[j]) lo = gk[j] < lo ? gk[j] : lo;
+    lo = block_reduce_u64<false>(lo, s_tmp);
+    if (lo == ~0ull) break;   // K is unmarked
+    // the largest key below that start; none: every key is marked
+    u64 below = 0;
+    bool any = false;
+    for (i32 i = threadIdx.x; i < cnt; i += blockDim.x)
+      if (s[i] < lo) {
+        below = s[i] > below ? s[i] : below;
+        any = true;
+      }
+    const u64 pred = block_reduce_u64<true>(any ? below + 1 : 0, s_tmp);   // +1: 0 means none
+    if (pred == 0) {
+      K = lo;   // lo is the smallest key
+      break;
+    }
+    K = pred - 1;
+  }
+  __shared__ i32 s_c;
+  if (threadIdx.x == 0) s_c = 0;
+  __syncthreads();
+  i32 c = 0;
+  for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) c += s[i] <= K;
+  if (c) atomicAdd(&s_c, c);
+  __syncthreads();
+  *kstar = K;
+  *napplied = s_c;
+  return true;
+}
+
+// Plain level: select and apply in one phase.  The kept moves are the first
+// B = min(cnt, cap) candidates by (gain desc, id asc) (uncoarsen.hpp:471-476,
+// move_request.hpp:36-41), and moves 0..pos are applied, pos = the largest
+// balanced index (uncoarsen.hpp:239-288; prefix 0 always counts as
+// balanced, :481-488).
+//  * cnt <= cap and no part's inflow bound passes MAXW (see ph_candidates):
+//    every index is balanced, all candidates move, and their order does not
+//    matter: no sort, no check.
+//  * cnt <= cap otherwise: the check over the flagged parts alone, in key
+//    order (refine_threshold); the moves with key <= K* apply.
+//  * cnt > cap, or too many events for that check: every CTA that owns a
+//    move index below B sorts the candidates itself (all get the same order)
+//    and runs the check over all parts (refine_balanced_pos).
+// Every check reads the source parts from msrc and pw as it was before the
+// round: the moves of this phase add their weights to pwd, which the gain
+// update folds into pw.  Move j is applied by global warp j (mod the warp
+// count), so a CTA owns an index below B iff blockIdx.x * warps_per_cta < B.
+__device__ void ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* keep, u32* s_warp, u64* s_tmp,
+                                UStage& S) {
+  RoundState* st = a.st;
+  const i32 cnt = ldc(&st->ccount);
+  const i32 B = cnt < a.move_cap ? cnt : a.move_cap;
+  const bool check = ldc(&st->needcheck) != 0;
+  const i32 nw = blockDim.x >> 5;
+  const i64 warp = (i64)blockIdx.x * nw + (threadIdx.x >> 5);
+  const i64 nwarps = (i64)gridDim.x * nw;
+  if ((i64)blockIdx.x * nw >= B) return;   // block-uniform: no move index of this CTA is kept
+  __shared__ unsigned long long s_gsum;
+  if (threadIdx.x == 0) {
+    s_gsum = 0;
+    S.cnt = 0;
+  }
+  u64 kstar = ~0ull;   // cnt <= cap: the moves with key <= kstar apply
+  i32 napplied = B;
+  bool sorted = false;
+  i32 pos = B - 1;     // sorted: moves 0..pos of keep apply
+  if (check) {
+    bool done = false;
+    if (cnt <= a.move_cap) done = refine_threshold(a, cnt, s, greedy, keep, s_tmp, s_warp, &kstar, &napplied);
+    trace_mark(a, 25);
+    if (!done) {
+      select_sort(a, a.cands, cnt, s, greedy);   // s[0..B) sorted (ends with a block barrier)
+      for (i32 i = threadIdx.x; i < B; i += blockDim.x) keep[i] = s[i];
+      __syncthreads();
+      pos = refine_balanced_pos(a, s, reinterpret_cast<u64*>(greedy), B, s_warp, a.msrc);
+      napplied = pos + 1;
+      sorted = true;
+      trace_mark(a, 26);
+    }
+  } else if (cnt > a.move_cap) {
+    select_sort(a, a.cands, cnt, s, greedy);   // the first cap candidates, all balanced
+    for (i32 i = threadIdx.x; i < B; i += blockDim.x) keep[i] = s[i];
+    sorted = true;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->rounds += 1;
+    st->moves += napplied;
+    st->cand_sum += cnt;
+  }
+  if (sorted) {
+    for (i64 j = warp; j <= pos; j += nwarps) apply_move(a, S, keep[j], a.pwd, &s_gsum);
+  } else {
+    for (i64 j = warp; j < cnt; j += nwarps) {
+      const u64 key = ldc(a.cands + j);
+      if (key <= kstar) apply_move(a, S, key, a.pwd, &s_gsum);   // warp-uniform
     }
   }
   ustage_flush(S, a.U, &st->ucount);
   if (threadIdx.x == 0 && s_gsum) atomicAdd((unsigned long long*)&st->gain_sum, s_gsum);
+}
+
+// Plain level, after the moves of a round: their part-weight changes join pw,
+// the inflow bounds and the per-round counters start again from zero.  Runs
+// beside the gain update, which reads none of these.
+__device__ void ph_fold(const LevelArgs& a) {
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += stride) {
+    const u32 d = ldc(a.pwd + p);
+    if (d) {
+      a.pw[p] = ldc(a.pw + p) + d;
+      a.pwd[p] = 0;
+    }
+    if (ldc(a.pin + p)) a.pin[p] = 0;
+    if (ldc(a.risk + p)) a.risk[p] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.st->ccount = 0;
+    a.st->needcheck = 0;
+    a.st->nrisk = 0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1211,11 +1536,16 @@ __device__ void ph_apply_balance(const LevelArgs& a, UStage& S) {
 // ---------------------------------------------------------------------------
 // The level kernel.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
+// Resident level-kernel CTAs per SM the register budget is sized for.
+#ifndef GKW_LEVEL_MIN_BLOCKS
+#define GKW_LEVEL_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(LevelArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   u64* s_sort = reinterpret_cast<u64*>(smem_raw);                  // kSortMax u64
   i32* greedy = reinterpret_cast<i32*>(smem_raw + kSortMax * 8);   // kGreedyWords
-  u32* acc_all = reinterpret_cast<u32*>(greedy + kGreedyWords);    // acc_warps * k u32
+  u64* s_keep = reinterpret_cast<u64*>(greedy + kGreedyWords);    // kMaxMoveCap u64: sorted moves
+  u32* acc_all = reinterpret_cast<u32*>(s_keep + kMaxMoveCap);     // acc_warps * k u32
   __shared__ u32 s_warp[33];
   __shared__ u64 s_tmp[32];
   __shared__ i32 s_flag;
@@ -1269,7 +1599,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 11);
       if (a.batch) ph_select_batch(a, s_sort, greedy, s_warp, true, fr);
-      else ph_select(a, s_sort, greedy, s_warp, true);
+      else ph_bal_select(a, s_sort, greedy);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 12);
       if (a.batch ? ldc(a.anyf + fr % 3) == 0 : ldc(&st->bdone) != 0) break;
@@ -1296,16 +1626,18 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(LevelArgs a) {
       if (a.batch) {
         ++fr;
         ph_select_batch(a, s_sort, greedy, s_warp, false, fr);
+        if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        trace_mark(a, 21);
+        if (ldc(a.anyf + fr % 3) == 0) break;
+        ph_apply_refine(a, s_ustage);
       } else {
-        ph_select(a, s_sort, greedy, s_warp, false);
+        if (ldc(&st->ccount) == 0) break;   // every CTA reads the same count
+        ph_refine_apply(a, s_sort, greedy, s_keep, s_warp, s_tmp, s_ustage);
       }
-      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
-      trace_mark(a, 21);
-      if (a.batch ? ldc(a.anyf + fr % 3) == 0 : ldc(&st->done) != 0) break;
-      ph_apply_refine(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 23);
       ph_update(a, acc_all, true);
+      if (!a.batch) ph_fold(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 24);
     }
@@ -1360,6 +1692,11 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   const bool batched = c->kacc > 0 && c->kacc < c->k;
   c->top = P.alloc_n<u64>(batched ? std::max<size_t>(n, kMaxMoveCap) : kMaxMoveCap);
   c->pw = P.alloc_n<u32>(c->k);
+  c->pwd = P.alloc_n<u32>(c->k);
+  c->pin = P.alloc_n<u32>(c->k);
+  c->msrc = P.alloc_n<i32>(n);
+  c->risk = P.alloc_n<u32>(c->k);
+  c->riskpart = P.alloc_n<i32>(c->k);
   c->st = P.alloc_n<RoundState>(1);
   c->bmark = P.alloc_n<u32>(n);
   c->btarget = P.alloc_n<i32>(n);
@@ -1376,6 +1713,9 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
     GKW_CUDA(cudaMemsetAsync(c->trace_n, 0, sizeof(i32) * kStatSlots, h.stream));
   }
   GKW_CUDA(cudaMemsetAsync(c->bmark, 0, sizeof(u32) * n, h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->pwd, 0, sizeof(u32) * c->k, h.stream));   // kept at zero between rounds
+  GKW_CUDA(cudaMemsetAsync(c->pin, 0, sizeof(u32) * c->k, h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->risk, 0, sizeof(u32) * c->k, h.stream));
   GKW_CUDA(cudaMemsetAsync(c->epoch, 0, sizeof(u32), h.stream));
   GKW_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(GridBarrier), h.stream));
   GKW_CUDA(cudaMemsetAsync(c->err, 0, sizeof(i32), h.stream));
@@ -1385,7 +1725,8 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   if (c->kacc <= 0) c->kacc = c->k;
   const i32 w = (i32)std::min<size_t>(kLevelThreads / 32, budget / (4 * (size_t)c->kacc));
   c->acc_warps = std::max(1, w);
-  c->smem = (size_t)kSortMax * 8 + (size_t)kGreedyWords * 4 + (size_t)c->acc_warps * c->kacc * 4;
+  c->smem = (size_t)kSortMax * 8 + (size_t)kGreedyWords * 4 + (size_t)kMaxMoveCap * 8 +
+            (size_t)c->acc_warps * c->kacc * 4;
   // one value for every handle of the process (handles of a server launch
   // this kernel concurrently with different sizes): the device's opt-in limit
   // less the kernel's static shared memory
@@ -1519,6 +1860,11 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.cands = c->cands;
   a.top = c->top;
   a.pw = c->pw;
+  a.pwd = c->pwd;
+  a.pin = c->pin;
+  a.msrc = c->msrc;
+  a.risk = c->risk;
+  a.riskpart = c->riskpart;
   a.st = c->st;
   a.bmark = c->bmark;
   a.btarget = c->btarget;

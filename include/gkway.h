@@ -227,7 +227,9 @@ void gkw_free(void* p);
  * stream) of the current device and returns when that stream is idle; cut_out
  * and pw_out (k entries, may be NULL) are host memory.  The first call on a
  * device looks up the array's device address; make it outside stream capture.
- * All calls share the array: calls whose work overlaps on the GPU race. */
+ * That address is kept for the life of the process: it does not survive a
+ * cudaDeviceReset of the device.  All calls share the array: calls whose work
+ * overlaps on the GPU race. */
 gkw_status gkw_cut_noalloc(const gkw_csr* d_graph, const int32_t* d_part, int32_t k, void* stream,
                            int64_t* cut_out, int64_t* pw_out);
 

@@ -46,6 +46,23 @@ def two_components(gen, seed: int):
     return gen.from_edges(a.n + b.n, np.concatenate([sa, sb]), np.concatenate([a.adjncy, b.adjncy + a.n]))
 
 
+def with_hub(gen, seed: int, n: int = 20000, fan: int = 10000):
+    """A Delaunay graph whose vertex n/2 is also joined to `fan` random others:
+    one row of about 10k entries among rows of about 6 (the skew of the
+    circuit-like graphs' fan-out hubs)."""
+    rng = np.random.default_rng(seed)
+    base = gen.delaunay(n, seed)
+    src = np.repeat(np.arange(base.n), np.diff(base.xadj))
+    keep = src < base.adjncy
+    s, d = src[keep], base.adjncy[keep]
+    hub = n // 2
+    others = rng.choice(np.setdiff1d(np.arange(n), [hub]), fan, replace=False)
+    s = np.concatenate([s, np.full(fan, hub)])
+    d = np.concatenate([d, others])
+    w = rng.integers(1, 4, s.shape[0])
+    return gen.from_edges(n, s, d, w)
+
+
 def small_cases(gen):
     """(name, graph) pairs for per-phase parity; each runs in well under a second."""
     cases = [
@@ -58,5 +75,28 @@ def small_cases(gen):
         ("two_components", two_components(gen, 21)),
         ("path_1500", path_graph(gen, 1500)),
         ("star_6000", star_graph(gen, 6000)),
+        ("delaunay_hub10k", with_hub(gen, 13)),
     ]
     return cases
+
+
+def build_graph(spec):
+    """Generator call by spec, for a process pool: ("delaunay", n, seed),
+    ("grid27", nx, ny, nz), ("circuit", n, seed) or ("road", n, seed)."""
+    import os
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import __graft_entry__ as ge
+    gen = ge.load_generators()
+    kind, *args = spec
+    if kind == "delaunay":
+        return gen.delaunay(args[0], seed=args[1])
+    if kind == "grid27":
+        return gen.grid27(*args)
+    if kind == "circuit":
+        return gen.circuit(args[0], seed=args[1])
+    if kind == "road":
+        return gen.road(args[0], seed=args[1])
+    raise ValueError(spec)
