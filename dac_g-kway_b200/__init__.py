@@ -117,6 +117,15 @@ class Stats(ctypes.Structure):
         )
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("match_lanes", ctypes.c_int32 * 4), ("level_verts_per_cta", ctypes.c_int32),
+                ("level_min_ctas", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"match_lanes": list(self.match_lanes), "level_verts_per_cta": int(self.level_verts_per_cta),
+                "level_min_ctas": int(self.level_min_ctas)}
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [
         ("slots", ctypes.c_int32),
@@ -205,6 +214,13 @@ _SIGS = [
                                       ctypes.POINTER(_i32p), ctypes.POINTER(_i32p), ctypes.POINTER(_i32p)]),
     ("gkw_write_partition", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _i32p]),
     ("gkw_free", None, [_VP]),
+    ("gkw_get_tuning", ctypes.c_int, [_VP, ctypes.POINTER(Tuning)]),
+    ("gkw_set_tuning", ctypes.c_int, [_VP, ctypes.POINTER(Tuning)]),
+    ("gkw_autotune", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.POINTER(Options),
+                                    ctypes.POINTER(Tuning)]),
+    ("gkw_read_metis_device", ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(Csr)]),
+    ("gkw_free_device_graph", None, [ctypes.POINTER(Csr)]),
+    ("gkw_write_partition_device", ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int32, _VP]),
     ("gkw_max_part_weight", ctypes.c_float, [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]),
     ("gkw_balance_cap", ctypes.c_float, [ctypes.c_int64, ctypes.c_int32, ctypes.c_double]),
     ("gkw_balance", ctypes.c_int, [_VP, ctypes.POINTER(Csr), ctypes.c_int32, ctypes.c_float, ctypes.c_int32, _VP,
@@ -474,6 +490,50 @@ class Handle:
                                        part.data_ptr()))
         return part[: int(g[0].shape[0]) - 1]
 
+    # ---- launch shapes ----
+    def tuning(self) -> dict:
+        t = Tuning()
+        check(lib().gkw_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, match_lanes=(4, 8, 16, 32), level_verts_per_cta=512, level_min_ctas=32) -> None:
+        t = Tuning((ctypes.c_int32 * 4)(*match_lanes), int(level_verts_per_cta), int(level_min_ctas))
+        check(lib().gkw_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, xadj, adjncy, adjwgt, vwgt, k: int, opts: Options | None = None) -> dict:
+        """gkw_autotune on torch CUDA int32 tensors; returns the chosen shapes."""
+        c = _csr_dev(xadj, adjncy, adjwgt, vwgt)
+        o = opts if opts is not None else default_options()
+        t = Tuning()
+        check(lib().gkw_autotune(self._h, ctypes.byref(c), int(k), ctypes.byref(o), ctypes.byref(t)))
+        return t.as_dict()
+
+    # ---- METIS files parsed and written on the device ----
+    def read_metis_device(self, path: str, reference_quirks: bool = False):
+        """Parse a METIS .graph file on the device -> (xadj, adjncy, adjwgt, vwgt) as
+        torch CUDA int32 tensors (copies; the library's arrays are released)."""
+        import torch
+        c = Csr()
+        check(lib().gkw_read_metis_device(self._h, path.encode(), int(reference_quirks), ctypes.byref(c)))
+        try:
+            dev = torch.device("cuda", self.device)
+            out = []
+            for ptr, cnt in ((c.xadj, c.n + 1), (c.adjncy, c.nnz), (c.adjwgt, c.nnz), (c.vwgt, c.n)):
+                addr = ctypes.cast(ptr, ctypes.c_void_p).value
+                if cnt > 0 and addr:
+                    out.append(torch.as_tensor(_DeviceArray(addr, int(cnt)), device=dev).clone())
+                else:
+                    out.append(torch.empty(0, dtype=torch.int32, device=dev))
+            torch.cuda.synchronize(dev)
+        finally:
+            lib().gkw_free_device_graph(ctypes.byref(c))
+        return tuple(out)
+
+    def write_partition_device(self, path: str, part) -> None:
+        """Write part ids (a torch CUDA int32 tensor) one per line, formatted on the device."""
+        n = int(part.numel())
+        check(lib().gkw_write_partition_device(self._h, path.encode(), n, part.data_ptr() if n else None))
+
     def cut(self, g, part, k):
         c = _csr_dev(*g)
         cut = ctypes.c_int64()
@@ -481,6 +541,14 @@ class Handle:
         check(lib().gkw_cut(self._h, ctypes.byref(c), part.data_ptr(), int(k), ctypes.byref(cut),
                             pw.ctypes.data_as(_i64p)))
         return int(cut.value), pw
+
+
+class _DeviceArray:
+    """A view of device int32 memory for torch.as_tensor (CUDA array interface)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4", "data": (ptr, False),
+                                         "version": 2, "strides": None}
 
 
 def predict_footprint(n: int, nnz: int, k: int) -> int:

@@ -185,6 +185,42 @@ gkw_status gkw_set_stream(gkw_handle* h, void* stream) {
 
 void* gkw_get_stream(gkw_handle* h) { return h ? (void*)h->h.stream : nullptr; }
 
+static void check_tuning(const gkw_tuning& t) {
+  for (int b = 0; b < 4; ++b)
+    GKW_REQUIRE(t.match_lanes[b] == 4 || t.match_lanes[b] == 8 || t.match_lanes[b] == 16 || t.match_lanes[b] == 32,
+                GKW_E_INVALID, "match_lanes must be 4, 8, 16 or 32");
+  GKW_REQUIRE(t.level_verts_per_cta >= 32 && t.level_min_ctas >= 1, GKW_E_INVALID,
+              "level_verts_per_cta must be >= 32 and level_min_ctas >= 1");
+}
+
+gkw_status gkw_get_tuning(gkw_handle* h, gkw_tuning* out) {
+  return guard([&] {
+    GKW_REQUIRE(out != nullptr, GKW_E_INVALID, "out is NULL");
+    *out = H(h).tuning;
+  });
+}
+
+gkw_status gkw_set_tuning(gkw_handle* h, const gkw_tuning* t) {
+  return guard([&] {
+    GKW_REQUIRE(t != nullptr, GKW_E_INVALID, "tuning is NULL");
+    check_tuning(*t);
+    H(h).tuning = *t;
+  });
+}
+
+gkw_status gkw_autotune(gkw_handle* h, const gkw_csr* d_graph, int32_t k, const gkw_options* opt, gkw_tuning* out) {
+  return guard([&] {
+    Handle& hh = H(h);
+    DevGraph g = dev_view(d_graph);
+    need_weights(g);
+    gkw_options o;
+    if (opt) o = *opt; else gkw_default_options(&o);
+    GKW_REQUIRE(o.init_method == GKW_INIT_DEVICE, GKW_E_INVALID, "autotune runs the device initial partition");
+    autotune(hh, g, k, o);
+    if (out) *out = hh.tuning;
+  });
+}
+
 gkw_status gkw_partition_device(gkw_handle* h, const gkw_csr* d_graph, int32_t k, const gkw_options* opt,
                                 int32_t* d_part_out, int64_t* cut_out, gkw_stats* stats) {
   return guard([&] {
@@ -412,6 +448,49 @@ gkw_status gkw_cut(gkw_handle* h, const gkw_csr* d_graph, const int32_t* d_part,
     if (cut_out) *cut_out = hm[0];
     if (pw_out) memcpy(pw_out, hm.data() + 2, sizeof(i64) * k);
   });
+}
+
+gkw_status gkw_read_metis_device(gkw_handle* h, const char* path, int32_t reference_quirks, gkw_csr* d_graph) {
+  if (!path || !d_graph) {
+    set_error("gkw_read_metis_device: NULL argument");
+    return GKW_E_INVALID;
+  }
+  return guard([&] {
+    Handle& hh = H(h);
+    DeviceCsr g;
+    try {
+      read_metis_device(hh, path, reference_quirks != 0, g);
+    } catch (...) {
+      cudaFree(g.xadj);
+      cudaFree(g.adjncy);
+      cudaFree(g.adjwgt);
+      cudaFree(g.vwgt);
+      throw;
+    }
+    d_graph->n = g.n;
+    d_graph->nnz = g.nnz;
+    d_graph->xadj = g.xadj;
+    d_graph->adjncy = g.adjncy;
+    d_graph->adjwgt = g.adjwgt;
+    d_graph->vwgt = g.vwgt;
+  });
+}
+
+void gkw_free_device_graph(gkw_csr* d_graph) {
+  if (!d_graph) return;
+  cudaFree(const_cast<int32_t*>(d_graph->xadj));
+  cudaFree(const_cast<int32_t*>(d_graph->adjncy));
+  cudaFree(const_cast<int32_t*>(d_graph->adjwgt));
+  cudaFree(const_cast<int32_t*>(d_graph->vwgt));
+  d_graph->xadj = d_graph->adjncy = d_graph->adjwgt = d_graph->vwgt = nullptr;
+}
+
+gkw_status gkw_write_partition_device(gkw_handle* h, const char* path, int32_t n, const int32_t* d_part) {
+  if (!path) {
+    set_error("gkw_write_partition_device: NULL path");
+    return GKW_E_INVALID;
+  }
+  return guard([&] { write_partition_device(H(h), path, n, d_part); });
 }
 
 }  // extern "C"

@@ -133,24 +133,61 @@ __global__ void __launch_bounds__(kMatchLongThreads) k_match_long(const i32* __r
   }
 }
 
+i32 match_bucket(const DevGraph& g) {
+  const double avg = g.n ? (double)g.m / g.n : 0.0;
+  return avg <= 6.5 ? 0 : avg <= 14 ? 1 : avg <= 28 ? 2 : 3;
+}
+
+static void launch_match(Handle& h, const DevGraph& g, i32* cand, i32 G, i32* longlist, i32* longcnt) {
+  const int threads = 256;
+  auto go = [&](auto kern) {
+    const i64 tot = (i64)g.n * G;
+    launch(kern, (u32)((tot + threads - 1) / threads), threads, 0, h.stream, g.n, g.xadj, g.adjncy, g.adjwgt,
+           cand, longlist, longcnt);
+  };
+  if (G == 4) go(k_match<4>);
+  else if (G == 8) go(k_match<8>);
+  else if (G == 16) go(k_match<16>);
+  else go(k_match<32>);
+}
+
+void time_match_variants(Handle& h, const DevGraph& g, i32* cand) {
+  if (g.n == 0) return;
+  const i32 b = match_bucket(g);
+  cudaEvent_t e0, e1;
+  GKW_CUDA(cudaEventCreate(&e0));
+  GKW_CUDA(cudaEventCreate(&e1));
+  Pool::Mark mk = h.scratch.mark();
+  i32* longlist = h.scratch.alloc_n<i32>(g.n);
+  i32* longcnt = h.scratch.alloc_n<i32>(1);
+  const i32 lanes[4] = {4, 8, 16, 32};
+  for (i32 q = 0; q < 4; ++q) {
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      GKW_CUDA(cudaMemsetAsync(longcnt, 0, sizeof(i32), h.stream));
+      GKW_CUDA(cudaEventRecord(e0, h.stream));
+      launch_match(h, g, cand, lanes[q], longlist, longcnt);
+      GKW_CUDA(cudaEventRecord(e1, h.stream));
+      GKW_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      GKW_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      best = std::min(best, ms);
+    }
+    h.tune_match_ms[b][q] += best;
+  }
+  h.scratch.release(mk);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
 void run_match(Handle& h, const DevGraph& g, i32* cand, i64 maxdeg) {
   if (g.n == 0) return;
-  const double avg = g.n ? (double)g.m / g.n : 0.0;
-  const int threads = 256;
   const bool split = maxdeg < 0 || maxdeg > kMatchLong;
   Pool::Mark mk = h.scratch.mark();
   i32* longlist = split ? h.scratch.alloc_n<i32>(g.n) : nullptr;
   i32* longcnt = split ? h.scratch.alloc_n<i32>(1) : nullptr;
   if (split) GKW_CUDA(cudaMemsetAsync(longcnt, 0, sizeof(i32), h.stream));
-  auto go = [&](auto kern, int G) {
-    const i64 tot = (i64)g.n * G;
-    launch(kern, (u32)((tot + threads - 1) / threads), threads, 0, h.stream, g.n, g.xadj, g.adjncy,
-           g.adjwgt, cand, longlist, longcnt);
-  };
-  if (avg <= 6.5) go(k_match<4>, 4);
-  else if (avg <= 14) go(k_match<8>, 8);
-  else if (avg <= 28) go(k_match<16>, 16);
-  else go(k_match<32>, 32);
+  launch_match(h, g, cand, h.tuning.match_lanes[match_bucket(g)], longlist, longcnt);
   if (split)
     launch(k_match_long, (u32)h.sm_count * 2, kMatchLongThreads, 0, h.stream, g.xadj, g.adjncy, g.adjwgt, cand,
            (const i32*)longlist, (const i32*)longcnt);
@@ -829,7 +866,8 @@ __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__
     }
     const i32 total = __shfl_sync(kFull, inc, 31);
     const i32 exc = inc - len;
-    for (i32 idx = lane; idx < total; idx += 32) {
+    for (i32 base = 0; base < total; base += 32) {   // warp-uniform: every lane takes every shuffle
+      const i32 idx = base + lane;
       // the row r with exc_r <= idx < inc_r: the first lane whose inclusive sum exceeds idx
       i32 r = 0;
 #pragma unroll
@@ -837,9 +875,12 @@ __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__
         const i32 probe = __shfl_sync(kFull, inc, r + step - 1);
         if (probe <= idx) r += step;
       }
+      r = r < 31 ? r : 31;
       const i32 rs = __shfl_sync(kFull, src, r), rd = __shfl_sync(kFull, dst, r), re = __shfl_sync(kFull, exc, r);
-      cadj[rd + (idx - re)] = sadj[rs + (idx - re)];
-      cwgt[rd + (idx - re)] = swgt[rs + (idx - re)];
+      if (idx < total) {
+        cadj[rd + (idx - re)] = sadj[rs + (idx - re)];
+        cwgt[rd + (idx - re)] = swgt[rs + (idx - re)];
+      }
     }
   }
 #pragma unroll
@@ -964,6 +1005,7 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
   Pool::Mark mk = h.scratch.mark();
   i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
   u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
+  if (h.tune_collect) time_match_variants(h, g, cand);
   run_match(h, g, cand, g.maxdeg);
   run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
   out.cmap = h.hier.alloc_n<i32>(std::max(g.n, 1));

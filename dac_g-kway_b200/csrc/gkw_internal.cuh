@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/gkway.h"
+#include "metis_header.h"
 
 namespace gkw {
 
@@ -177,6 +178,11 @@ struct Handle {
   // thread-block cluster (a server's small jobs; see launch_coop)
   bool narrow = false;
   cudaEvent_t coop_ev = nullptr;   // this handle's last wide cooperative launch
+  gkw_tuning tuning{{4, 8, 16, 32}, 512, 32};   // launch shapes (gkw_autotune)
+  // while the autotuner collects: per average-degree bucket, the summed time
+  // of each match lane count (4, 8, 16, 32) over the levels met
+  bool tune_collect = false;
+  double tune_match_ms[4][4] = {};
   Handle() : hier(size_t(256) << 20), scratch(size_t(256) << 20) {}
 };
 void ensure_timer_events(Handle& h);
@@ -219,6 +225,10 @@ void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total);
 // maxdeg: the longest row if known (< 0: unknown); rows above the sub-warp
 // limit go to one CTA each.
 void run_match(Handle& h, const DevGraph& g, i32* cand, i64 maxdeg = -1);
+// Average-degree bucket of a level for gkw_tuning::match_lanes.
+i32 match_bucket(const DevGraph& g);
+// The autotuner's measurement of every match lane count on one level.
+void time_match_variants(Handle& h, const DevGraph& g, i32* cand);
 // returns the number of round launches the reference's loop would make
 // These run without host synchronisation; results that the host needs are
 // left in device memory (see CoopState) and read once per level.
@@ -345,6 +355,8 @@ void partition_multi_impl(Handle& h, const DevGraph& g0, i32 nk, const i32* ks, 
 void partition_multi_host(Handle& h, const DevGraph& host_graph, i32 nk, const i32* ks, const gkw_options& opt,
                           i32* parts_out, i64* cuts_out);
 Handle& handle_of(gkw_handle* h);   // the handle behind a C-ABI handle (capi.cu)
+// gkw_autotune: the fastest launch shapes for this graph into h.tuning.
+void autotune(Handle& h, const DevGraph& g, i32 k, const gkw_options& opt);
 // Many independent graphs partitioned as one disjoint union (batch.cu): host
 // arrays with global ids, graph g = vertices [graph_ptr[g], graph_ptr[g+1]).
 // part_out gets each graph's own part ids.  Returns false, having computed
@@ -353,6 +365,23 @@ Handle& handle_of(gkw_handle* h);   // the handle behind a C-ABI handle (capi.cu
 bool partition_batch_union(Handle& h, const DevGraph& host_union, i32 G, const i32* graph_ptr, const i32* ks,
                            const gkw_options& opt, i32* part_out, i64* cuts_out, i32* levels_out = nullptr);
 const char* last_error_cstr();
+
+// ---- METIS .graph files on the device (parse.cu; header: metis_header.h) ----
+// A graph in device memory allocated with cudaMalloc (gkw_free_device_graph).
+struct DeviceCsr {
+  i32 n = 0;
+  i64 nnz = 0;
+  i32* xadj = nullptr;
+  i32* adjncy = nullptr;
+  i32* adjwgt = nullptr;
+  i32* vwgt = nullptr;
+};
+// Parse a METIS .graph file on the device (the same result and errors as the
+// host reader); on error nothing stays allocated in `out` beyond what the
+// caller frees with its arrays.
+void read_metis_device(Handle& h, const char* path, bool reference_quirks, DeviceCsr& out);
+// One part id per line, formatted on the device.
+void write_partition_device(Handle& h, const char* path, i32 n, const i32* d_part);
 
 // ---- host helpers ----
 float max_part_weight(i64 total_vwgt, i32 k, double eps);

@@ -17,7 +17,10 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "gkway.hpp"
+#include "metis_header.h"
 
 extern "C" void gkw_io_set_error(const std::string& msg);
 
@@ -189,6 +192,59 @@ long long parse_parallel(const char* p, const char* end, int T, const LineFormat
 }
 
 }  // namespace
+
+}  // namespace gk
+
+// The header line of a METIS .graph text: "n m [fmt [ncon]]", after any
+// comment and blank lines; the same rules as gk::Graph's reading.
+bool gkw::parse_metis_header(const char* buf, size_t size, bool reference_quirks, gkw::MetisHeader* out,
+                             std::string* err) {
+  try {
+    gk::Cursor c{buf, buf + size};
+    const char *b, *e;
+    for (;;) {
+      if (!c.line(b, e)) throw std::runtime_error("graph file: missing header");
+      const char* t = b;
+      while (t < e && (*t == ' ' || *t == '\t')) ++t;
+      if (t < e && *t == '%') continue;
+      if (t == e) continue;
+      break;
+    }
+    long long n = 0, m = 0, fmt = 0, ncon = 1;
+    if (!gk::next_int(b, e, n) || !gk::next_int(b, e, m)) throw std::runtime_error("graph file: bad header");
+    std::string fmt_s;
+    {
+      const char* t = b;
+      while (t < e && (*t == ' ' || *t == '\t')) ++t;
+      const char* s0 = t;
+      while (t < e && *t >= '0' && *t <= '9') ++t;
+      fmt_s.assign(s0, t);
+      b = t;
+      if (!fmt_s.empty()) fmt = std::atoll(fmt_s.c_str());
+      long long nc;
+      if (gk::next_int(b, e, nc)) ncon = nc;
+    }
+    if (n < 0 || m < 0 || n >= (1LL << 31) || 2 * m >= (1LL << 31))
+      throw std::runtime_error("graph file: sizes out of range");
+    if (ncon != 1) throw std::runtime_error("graph file: only ncon = 1 is supported");
+    out->n = n;
+    out->m = m;
+    out->vsize = (fmt / 100) % 10 == 1;
+    out->vw = (fmt / 10) % 10 == 1;
+    out->ew = fmt % 10 == 1;
+    if (reference_quirks) {   // graph.hpp:93-97,125-137
+      out->vsize = out->vw = false;
+      out->ew = fmt_s == "11";
+    }
+    out->body = (size_t)(c.p - buf);
+    return true;
+  } catch (const std::exception& ex) {
+    *err = ex.what();
+    return false;
+  }
+}
+
+namespace gk {
 
 Graph::Graph(const std::string& input_path, bool reference_quirks) {
   const std::string buf = read_file(input_path);
@@ -451,7 +507,8 @@ void gkw_free(void* p) { std::free(p); }
 //                                        bisection instead of its k-way call
 //   GKW_SEED=<n>                         seed of the device initial partition
 void graph_partitioner(const std::string& GRAPH_FILE, const std::string& OUT_FILE, const int NUM_PARTITIONS) {
-  gk::Graph graph(GRAPH_FILE);
+  // the file is parsed on the device, partitioned there, and the part ids are
+  // formatted there; only the text crosses to and from the host
   gkw_options opt;
   gkw_default_options(&opt);
   if (const char* s = std::getenv("GKW_SEED")) opt.seed = std::strtoull(s, nullptr, 10);
@@ -460,17 +517,47 @@ void graph_partitioner(const std::string& GRAPH_FILE, const std::string& OUT_FIL
     if (!gk::use_metis_init(&opt, lib, rb && *rb == '1'))
       throw std::runtime_error(std::string("cannot load METIS from ") + lib);
   }
-  gk::GraphPartitioner gp(&opt);
-  gk::PartitionResult r = gp.partition_with_stats(graph, NUM_PARTITIONS);
-  const gkw_stats& s = r.stats;
+  if (FILE* f = fopen(GRAPH_FILE.c_str(), "rb")) fclose(f);   // a missing file is reported before any device work
+  else throw std::runtime_error("cannot open graph file: " + GRAPH_FILE);
+  gkw_handle* h = nullptr;
+  if (gkw_create(&h, 0) != GKW_OK) throw std::runtime_error(std::string("gkw_create: ") + gkw_last_error());
+  struct Cleanup {
+    gkw_handle* h;
+    gkw_csr g{};
+    int32_t* part = nullptr;
+    ~Cleanup() {
+      if (part) cudaFree(part);
+      gkw_free_device_graph(&g);
+      gkw_destroy(h);
+    }
+  } c{h};
+  const auto t0 = std::chrono::steady_clock::now();
+  if (gkw_read_metis_device(h, GRAPH_FILE.c_str(), 0, &c.g) != GKW_OK)
+    throw std::runtime_error(gkw_last_error());
+  const auto t1 = std::chrono::steady_clock::now();
+  if (cudaMalloc((void**)&c.part, sizeof(int32_t) * std::max<size_t>((size_t)c.g.n, 1)) != cudaSuccess)
+    throw std::runtime_error("cudaMalloc failed for the part ids");
+  int64_t cut = 0;
+  gkw_stats s{};
+  if (gkw_partition_device(h, &c.g, NUM_PARTITIONS, &opt, c.part, &cut, &s) != GKW_OK)
+    throw std::runtime_error(gkw_last_error());
   std::cout << "#################### Execution Time ################# \n";
   std::cout << "Total time: " << s.ms_total / 1000.0 << "s\n";
   std::cout << "Coarsen time: " << s.ms_coarsen / 1000.0 << "s\n";
   std::cout << "Init partition time: " << s.ms_init / 1000.0 << "s\n";
   std::cout << "Refinement time: " << s.ms_refine / 1000.0 << "s\n";
   std::cout << "#################### Partition Summary ################# \n";
-  std::cout << "***** h_cutsize " << r.cut << '\n';
+  std::cout << "***** h_cutsize " << cut << '\n';
   if ((double)s.max_part_weight > (double)s.maxw)
     std::cout << "!!!@@@ ERROR, max part weight " << s.max_part_weight << " is above " << s.maxw << '\n';
-  graph.dump_result(r.part, OUT_FILE);
+  char cwd[4096];
+  const std::string dir = getcwd(cwd, sizeof(cwd)) ? std::string(cwd) : std::string(".");
+  const std::string out_path = dir + "/" + OUT_FILE + ".out";
+  std::cout << "out_path:" << out_path << "\n";
+  if (gkw_write_partition_device(h, out_path.c_str(), c.g.n, c.part) != GKW_OK)
+    throw std::runtime_error(gkw_last_error());
+  const auto t2 = std::chrono::steady_clock::now();
+  if (std::getenv("GKW_TIMES"))
+    std::cout << "read " << std::chrono::duration<double>(t1 - t0).count() << "s, end to end "
+              << std::chrono::duration<double>(t2 - t0).count() << "s\n";
 }

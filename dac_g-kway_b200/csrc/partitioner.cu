@@ -457,6 +457,67 @@ void partition_multi_impl(Handle& h, const DevGraph& g0, i32 nk, const i32* ks, 
   }
 }
 
+// The autotuner (gkw_autotune).  Launch shapes never change a result, only
+// its time, so each candidate is timed on a full partition of the caller's
+// graph:
+//   * match lanes: one partition during which every level's match is also
+//     run with 4, 8, 16 and 32 lanes per vertex (best of three launches each,
+//     CUDA events); each average-degree bucket met keeps the lane count with
+//     the least summed time;
+//   * level-kernel density: vertices per CTA in {256, 512, 1024, 2048} x
+//     minimum CTAs in {16, 32, 64}, best of two partitions each by the
+//     refinement phase's event time.
+void autotune(Handle& h, const DevGraph& g, i32 k, const gkw_options& opt) {
+  i32* part = nullptr;
+  GKW_CUDA(cudaMalloc((void**)&part, sizeof(i32) * std::max(g.n, 1)));
+  struct Free {
+    i32* p;
+    ~Free() { cudaFree(p); }
+  } fr{part};
+  auto run = [&](gkw_stats* st) {
+    h.hier.reset();
+    h.scratch.reset();
+    i64 cut = 0;
+    partition_impl(h, g, k, opt, part, &cut, st);
+  };
+  gkw_stats st;
+  run(&st);   // warm
+  memset(h.tune_match_ms, 0, sizeof(h.tune_match_ms));
+  h.tune_collect = true;
+  try {
+    run(&st);
+  } catch (...) {
+    h.tune_collect = false;
+    throw;
+  }
+  h.tune_collect = false;
+  const i32 lanes[4] = {4, 8, 16, 32};
+  for (i32 b = 0; b < 4; ++b) {
+    i32 best = -1;
+    for (i32 q = 0; q < 4; ++q)
+      if (h.tune_match_ms[b][q] > 0 && (best < 0 || h.tune_match_ms[b][q] < h.tune_match_ms[b][best])) best = q;
+    if (best >= 0) h.tuning.match_lanes[b] = lanes[best];
+  }
+  gkw_tuning best = h.tuning;
+  double best_ms = 1e300;
+  for (i32 vpc : {256, 512, 1024, 2048}) {
+    for (i32 minc : {16, 32, 64}) {
+      h.tuning.level_verts_per_cta = vpc;
+      h.tuning.level_min_ctas = minc;
+      double t = 1e300;
+      for (int rep = 0; rep < 2; ++rep) {
+        run(&st);
+        t = std::min(t, st.ms_refine);
+      }
+      if (t < best_ms) {
+        best_ms = t;
+        best = h.tuning;
+      }
+    }
+  }
+  h.tuning = best;
+}
+
 // Copies a host CSR into the handle's hierarchy pool (unit weights where the
 // arrays are NULL).  The host arrays may be a slice of a larger concatenated
 // CSR: xadj values are then offset by xadj[0] and neighbour ids by vbase, and

@@ -29,12 +29,10 @@ constexpr i32 kSortMax = 4096;      // candidates sorted in one shared-memory pa
 constexpr i32 kSelBins = 2048;      // histogram bins of the threshold search above kSortMax
 constexpr i32 kMaxMoveCap = 2048;   // largest supported move cap
 constexpr int kLevelThreads = 512;
-// Level-kernel CTAs: one per kLevelVertsPerCta vertices of the level, at
-// least kLevelMinCtas.  Every phase of a round is a chain of dependent loads
-// per vertex, so even small levels run faster spread over many warps than
-// on the cheaper barrier of a few CTAs.
-constexpr i32 kLevelVertsPerCta = 512;
-constexpr i32 kLevelMinCtas = 32;
+// Level-kernel CTAs: one per gkw_tuning::level_verts_per_cta vertices of the
+// level (default 512), at least level_min_ctas (default 32).  Every phase of a
+// round is a chain of dependent loads per vertex, so even small levels run
+// faster spread over many warps than on the cheaper barrier of a few CTAs.
 constexpr i32 kGreedySmemParts = 4096;   // balance greedy pass: part weights in smem up to this k
 constexpr i32 kGreedyWords = 3 * kMaxMoveCap + kGreedySmemParts;
 static_assert((size_t)kGreedyWords * 4 >= (size_t)kSortMax * 8, "the sort's second buffer aliases the greedy region");
@@ -1899,8 +1897,8 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
     a.trace_cap = kTraceCap;
     a.trace_n = c->trace_n + slot;
   }
-  i32 grid = (i32)ceil_div(std::max(g.n, 1), kLevelVertsPerCta);
-  grid = std::max(grid, std::max(kLevelMinCtas, c->kacc / 4));   // large k: few gain-update warps per CTA
+  i32 grid = (i32)ceil_div(std::max(g.n, 1), std::max(h.tuning.level_verts_per_cta, 32));
+  grid = std::max(grid, std::max(h.tuning.level_min_ctas, c->kacc / 4));   // large k: few gain-update warps per CTA
   grid = std::min(grid, c->grid);
   grid = coop_grid(h, (const void*)k_level, grid, kLevelThreads, c->smem);
   void* args[] = {&a};

@@ -109,6 +109,29 @@ gkw_status gkw_create(gkw_handle** out, int32_t device);
 gkw_status gkw_destroy(gkw_handle* h);
 /* Use the caller's CUDA stream (a cudaStream_t) instead of the handle's own. */
 gkw_status gkw_set_stream(gkw_handle* h, void* stream);
+
+/* Launch shapes of a handle's kernels (results never depend on them).  No
+ * counterpart in the reference, whose shapes are fixed constants
+ * (declarations.h:12-18).
+ *   match_lanes[b]       lanes per vertex of the heavy-edge match on levels
+ *                        whose average degree is <= 6.5, <= 14, <= 28, above
+ *                        (b = 0..3; 4, 8, 16 or 32; rows above 512 entries
+ *                        always go to one CTA each)
+ *   level_verts_per_cta  level-kernel CTAs: one per this many vertices ...
+ *   level_min_ctas       ... and at least this many (capped at 2 per SM) */
+typedef struct gkw_tuning {
+  int32_t match_lanes[4];
+  int32_t level_verts_per_cta;
+  int32_t level_min_ctas;
+} gkw_tuning;
+gkw_status gkw_get_tuning(gkw_handle* h, gkw_tuning* out);
+gkw_status gkw_set_tuning(gkw_handle* h, const gkw_tuning* t);
+/* Autotuner: partitions the device-resident graph with candidate shapes --
+ * every match lane count on every level of its hierarchy, a grid of level-
+ * kernel densities -- timing each with CUDA events, and keeps the fastest in
+ * the handle (also returned in *out, may be NULL).  Takes a few dozen
+ * partitions of the graph; later partitions on the handle use the result. */
+gkw_status gkw_autotune(gkw_handle* h, const gkw_csr* d_graph, int32_t k, const gkw_options* opt, gkw_tuning* out);
 void* gkw_get_stream(gkw_handle* h);
 const char* gkw_last_error(void);
 void gkw_default_options(gkw_options* opt);
@@ -216,6 +239,21 @@ gkw_status gkw_read_metis(const char* path, int32_t reference_quirks, int32_t* n
  * <cwd>/<name>.out this way). */
 gkw_status gkw_write_partition(const char* path, int32_t n, const int32_t* part);
 void gkw_free(void* p);
+
+/* Read a METIS .graph file into device memory, parsing it on the device: the
+ * file's bytes are copied to the GPU once and split into lines, tokens and
+ * CSR rows there (the header line is read on the host).  Same format, result
+ * and error messages as gkw_read_metis.  On success the four arrays of
+ * *d_graph (0-based ids, n and nnz set) are device memory on the handle's
+ * device allocated with cudaMalloc; release them with gkw_free_device_graph.
+ * Replaces the reference's host parser (gkway/graph.hpp:70-152) for callers
+ * that partition on the device. */
+gkw_status gkw_read_metis_device(gkw_handle* h, const char* path, int32_t reference_quirks, gkw_csr* d_graph);
+void gkw_free_device_graph(gkw_csr* d_graph);
+/* Write one part id per line to `path`, the text formatted on the device from
+ * the device array d_part (n ids); the reference writes <cwd>/<name>.out this
+ * way on the host (gkway/graph.hpp:227-240). */
+gkw_status gkw_write_partition_device(gkw_handle* h, const char* path, int32_t n, const int32_t* d_part);
 
 /* Exact cut and part weights like gkw_cut, but with no device allocation and
  * no handle.  No counterpart in the reference.  For callers that may not

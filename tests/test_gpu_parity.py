@@ -289,3 +289,31 @@ def test_empty_and_tiny_graphs(handle, pkg, gen, orc):
     g = gen.delaunay(300, 2)
     part, cut, _ = handle.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, 1)
     assert cut == 0 and np.all(part == 0)
+
+
+def test_autotune_keeps_results(pkg, gen):
+    """The autotuner picks launch shapes by timing; results never depend on
+    them: the same part vector and cut before tuning, after it, and under
+    hand-set extreme shapes."""
+    import torch
+    from conftest import to_dev
+    h = pkg.Handle(0)
+    g = gen.circuit(60000, seed=3, levels=60, hub_max=2000)
+    dg = to_dev(g)
+    outs = []
+    for shapes in (None, "tune", dict(match_lanes=(32, 4, 4, 4), level_verts_per_cta=64, level_min_ctas=1),
+                   dict(match_lanes=(8, 32, 16, 4), level_verts_per_cta=4096, level_min_ctas=64)):
+        if shapes == "tune":
+            t = h.autotune(*dg, 32)
+            assert all(x in (4, 8, 16, 32) for x in t["match_lanes"])
+        elif shapes is not None:
+            h.set_tuning(**shapes)
+            assert h.tuning()["level_verts_per_cta"] == shapes["level_verts_per_cta"]
+        p = torch.empty(g.n, dtype=torch.int32, device="cuda:0")
+        cut, _ = h.partition_device(*dg, 32, p)
+        outs.append((p.cpu().numpy(), cut))
+    for part, cut in outs[1:]:
+        assert np.array_equal(part, outs[0][0]) and cut == outs[0][1]
+    with pytest.raises(pkg.GkwError):
+        h.set_tuning(match_lanes=(3, 8, 16, 32))
+    h.close()
