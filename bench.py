@@ -218,6 +218,8 @@ def bench_ours(args):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    # launch shapes for this graph (gkw_autotune: timed candidates; results never depend on them)
+    tuning = None if args.no_tune else h.autotune(xadj, adjncy, adjwgt, vwgt, K, opts)
     # warm-up
     for _ in range(args.warmup):
         h.partition_device(xadj, adjncy, adjwgt, vwgt, K, part, opts)
@@ -316,6 +318,7 @@ def bench_ours(args):
             "phase_ms": {"coarsen": st["ms_coarsen"], "init": st["ms_init"], "refine": st["ms_refine"],
                          "total": st["ms_total"]} if st else None,
             "clocks": clocks,
+            "tuning": tuning,
         }
         line.update(extras)
         print(json.dumps(line))
@@ -749,6 +752,8 @@ def main():
     ap.add_argument("--rates", default="20,1000", help="served: offered loads (requests/s)")
     ap.add_argument("--requests", type=int, default=400, help="served: most requests per load")
     ap.add_argument("--duration", type=float, default=10.0, help="served: seconds of arrivals per load")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="plain workload: skip gkw_autotune (default launch shapes; profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain workload: leave the batched and served objects out of the line")
     args = ap.parse_args()

@@ -459,7 +459,9 @@ void read_metis_device(Handle& h, const char* path, bool quirks, DeviceCsr& out)
   GKW_CUDA(cudaStreamSynchronize(h.stream));
   const i32 nnz = *reinterpret_cast<const i32*>(h.h_pinned);
   u64 ek = (u64)h.h_pinned[1];
-  if (ek == ~0ull) {
+  // the scatter also runs after an error: an out-of-range id earlier in the
+  // file than that error is the one to report (it stays inside each row)
+  {
     out.nnz = nnz;
     GKW_CUDA(cudaMalloc((void**)&out.adjncy, sizeof(i32) * std::max<size_t>(nnz, 1)));
     GKW_CUDA(cudaMalloc((void**)&out.adjwgt, sizeof(i32) * std::max<size_t>(nnz, 1)));

@@ -93,6 +93,7 @@ struct RefineCtx {
   i32* msrc = nullptr;   // source part of each candidate, taken before any move is applied
   u32* risk = nullptr;   // per part: 1 + its index among the round's at-risk parts, 0 if not at risk
   i32* riskpart = nullptr;   // the at-risk parts by index
+  i32* pnet = nullptr;       // net weight change of each part if every candidate moved
   RoundState* st = nullptr;
   u32* bmark = nullptr;
   i32* btarget = nullptr;
@@ -132,6 +133,7 @@ struct LevelArgs {
   i32* msrc;          // plain levels: source part of each candidate
   u32* risk;          // plain levels: 1 + index among the round's at-risk parts, or 0
   i32* riskpart;      // plain levels: the at-risk parts by index
+  i32* pnet;          // plain levels: net weight change of each part over all candidates
   RoundState* st;
   u32* bmark;
   i32 *btarget, *bgain, *blist;
@@ -261,6 +263,43 @@ __device__ __forceinline__ void block_append64(bool pred, u64 val, u64* list, i3
   __syncthreads();
 }
 
+__device__ __forceinline__ void block_append32(bool pred, i32 val, i32* list, i32* counter, i32* s_cnt,
+                                               i32* s_base) {
+  if (threadIdx.x == 0) *s_cnt = 0;
+  __syncthreads();
+  const u32 m = __ballot_sync(kFullMask, pred);   // one shared atomic per warp
+  const int lane = threadIdx.x & 31;
+  i32 wbase = 0;
+  if (lane == 0 && m) wbase = atomicAdd(s_cnt, __popc(m));
+  wbase = __shfl_sync(kFullMask, wbase, 0);
+  __syncthreads();
+  if (threadIdx.x == 0 && *s_cnt) *s_base = atomicAdd(counter, *s_cnt);
+  __syncthreads();
+  if (pred) list[*s_base + wbase + __popc(m & ((1u << lane) - 1))] = val;
+  __syncthreads();
+}
+
+// U (or P) appends of one phase, staged per CTA in shared memory (one global
+// atomic per CTA); entries beyond the stage go to the list directly.
+constexpr i32 kUStage = 1024;
+struct UStage {
+  i32 buf[kUStage];
+  i32 cnt;
+  i32 base;
+};
+__device__ __forceinline__ void ustage_push(UStage& S, i32 x, i32* U, i32* ucount) {
+  const i32 idx = atomicAdd(&S.cnt, 1);
+  if (idx < kUStage) S.buf[idx] = x;
+  else U[atomicAdd(ucount, 1)] = x;
+}
+__device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
+  __syncthreads();
+  const i32 c = S.cnt < kUStage ? S.cnt : kUStage;
+  if (threadIdx.x == 0 && c) S.base = atomicAdd(ucount, c);
+  __syncthreads();
+  for (i32 t = threadIdx.x; t < c; t += blockDim.x) U[S.base + t] = S.buf[t];
+}
+
 // ---------------------------------------------------------------------------
 // Phases.  `base` of every grid-stride loop is warp-uniform so that warp
 // collectives run converged.
@@ -269,11 +308,13 @@ __device__ __forceinline__ void block_append64(bool pred, u64 val, u64* list, i3
 // Projection (uncoarsen.hpp:325-356, expand_partition): part and boundary
 // inherited from the coarse vertex, gain 0, target = part, boundary vertices
 // flagged for the gain update.
-__device__ void ph_project(const LevelArgs& a) {
-  const int lane = threadIdx.x & 31;
+// U appends are aggregated per CTA (one global atomic per CTA and pass, not
+// one per warp: a million-vertex level would serialise 32k atomics on the
+// counter).
+__device__ void ph_project(const LevelArgs& a, i32* s_cnt, i32* s_base) {
   const i64 stride = (i64)gridDim.x * blockDim.x;
-  for (i64 base = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += stride) {
-    const i64 v = base + lane;
+  for (i64 b0 = (i64)blockIdx.x * blockDim.x; b0 < a.n; b0 += stride) {   // block-uniform trip count
+    const i64 v = b0 + threadIdx.x;
     bool b = false;
     if (v < a.n) {
       const i32 c = a.cmap[v];
@@ -295,7 +336,7 @@ __device__ void ph_project(const LevelArgs& a) {
       b = bc != 0 && !enter && (!a.batch || __ldg(a.gflags + __ldg(a.gid + v)) != 0);
       a.updflag[v] = b ? 1 : 0;
     }
-    warp_append(b, (i32)v, a.U, &a.st->ucount);
+    block_append32(b, (i32)v, a.U, &a.st->ucount, s_cnt, s_base);
   }
 }
 
@@ -326,7 +367,7 @@ __device__ void ph_lists(const LevelArgs& a) {
 // Vertices whose new gain is positive join P.
 // `count`: add the row lengths read to the level's entry counter (the update
 // passes of the rounds; the first pass of a level is counted as a full pass).
-__device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
+__device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, UStage& S) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid >= a.acc_warps) return;
   u32* acc = acc_all + (size_t)wid * a.kacc;
@@ -376,7 +417,7 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
         a.bnd[v] = b ? 1 : 0;
         a.gain[v] = (i32)g;
         a.target[v] = (i32)q_best;
-        if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) Pout[atomicAdd(pcount, 1)] = v;
+        if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) ustage_push(S, v, Pout, pcount);
       }
       __syncwarp();
       if (h0) accb[q0] = 0;
@@ -415,7 +456,7 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
       a.bnd[v] = b ? 1 : 0;
       a.gain[v] = (i32)g;
       a.target[v] = (i32)q_best;
-      if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) Pout[atomicAdd(pcount, 1)] = v;
+      if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) ustage_push(S, v, Pout, pcount);
     }
     __syncwarp();
     for (i32 e = beg + lane; e < end; e += 32) accb[ldc(a.part + a.adjncy[e])] = 0;
@@ -423,6 +464,17 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count) {
   }
   if (count && lane == 0 && rows) atomicAdd(reinterpret_cast<unsigned long long*>(&st->rows), rows);
 }
+
+// P appends are staged per CTA in shared memory (S) and flushed with one
+// global atomic; every thread of the CTA calls this.
+__device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count, UStage& S) {
+  if (threadIdx.x == 0) S.cnt = 0;
+  __syncthreads();
+  ph_update_rows(a, acc_all, count, S);
+  ustage_flush(S, a.P0, &a.st->pcount[0]);
+  __syncthreads();
+}
+
 
 // Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
 // boundary, gain > 0, a valid destination by weight, and no neighbour with a
@@ -493,6 +545,8 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
       if (cand) {
         a.msrc[v] = p;
         before = atomicAdd(a.pin + t, vw);
+        atomicAdd(a.pnet + t, (i32)vw);
+        atomicSub(a.pnet + p, (i32)vw);
       }
       block_append64(cand, move_key(g, v), a.cands, &st->ccount, s_cnt, s_base);
       // the final inflow of t is at least before + vw, and (float)(u32) is
@@ -998,26 +1052,6 @@ __device__ void ph_select_batch(const LevelArgs& a, u64* s, i32* greedy, u32* s_
   }
 }
 
-// U appends of one apply phase, staged per CTA in shared memory (one global
-// atomic per CTA); entries beyond the stage go to U directly.
-constexpr i32 kUStage = 1024;
-struct UStage {
-  i32 buf[kUStage];
-  i32 cnt;
-  i32 base;
-};
-__device__ __forceinline__ void ustage_push(UStage& S, i32 x, i32* U, i32* ucount) {
-  const i32 idx = atomicAdd(&S.cnt, 1);
-  if (idx < kUStage) S.buf[idx] = x;
-  else U[atomicAdd(ucount, 1)] = x;
-}
-__device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
-  __syncthreads();
-  const i32 c = S.cnt < kUStage ? S.cnt : kUStage;
-  if (threadIdx.x == 0 && c) S.base = atomicAdd(ucount, c);
-  __syncthreads();
-  for (i32 t = threadIdx.x; t < c; t += blockDim.x) U[S.base + t] = S.buf[t];
-}
 
 // One move, by one warp: v goes to its target; v and its neighbours are
 // flagged for the gain update and appended to U (uncoarsen.hpp:290-323).
@@ -1085,46 +1119,51 @@ __device__ __forceinline__ u64 block_reduce_u64(u64 x, u64* s_tmp) {
 constexpr i32 kRiskEvents = 1024;   // event limit of the at-risk balance check
 constexpr i32 kRiskParts = 1024;    // at-risk part limit of that check
 
-// The balance check of a round whose candidates are all kept (cnt <= cap),
-// without sorting them.  Only parts flagged in risk can be over MAXW at any
-// prefix (a part's running change D never exceeds its inflow bound), so only
-// the moves into or out of those parts matter.  Each such move is an event
-// (part, key, +-w), and the events are grouped by part (a counting sort over
-// the parts' dense indices).  A part's D after one of its events is the sum of
-// its events with keys up to that key, and it holds until the part's next
-// event.  An event with D > 0 and (float)(pw + D) > MAXW marks the key range
-// [key, next key of the part) -- the same index ranges the reference's table
-// marks (uncoarsen.hpp:239-288), in key order instead of index order.  The
-// applied moves are those with key <= K*, K* = the largest unmarked key, or
-// the smallest key if every key is marked (prefix 0 always counts as
-// balanced, :481-488).  Returns false (block-uniform) beyond kRiskEvents events
-// or kRiskParts parts; the caller then sorts.
+// The balance check of a round whose candidates are all kept (cnt <= cap)
+// and whose last index is not balanced, without sorting the candidates.
+// Only parts flagged in risk can be over MAXW at any index (a part's running
+// change D never exceeds its inflow bound), so only the moves into or out of
+// those parts matter.  Each such move is an event (part, key, +-w), and the
+// events are grouped by part (a counting sort over the parts' dense indices).
+// A part's D after one of its events is the sum of its events with keys up to
+// that key, and it holds until the part's next event; an event with D > 0 and
+// (float)(pw + D) > MAXW marks the key range [key, next key of the part) --
+// the index ranges the reference's table marks (uncoarsen.hpp:239-288), in
+// key order.  Every candidate key is then tested against the marked ranges,
+// and the moves with key <= K* apply, K* = the largest unmarked key, or the
+// smallest key if all are marked (prefix 0 always counts as balanced,
+// :481-488).  Returns false (block-uniform) beyond kRiskEvents events or
+// kRiskParts parts; the caller then runs the check over all parts.
 __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greedy, u64* keep, u64* s_tmp,
                                  u32* s_warp, u64* kstar, i32* napplied) {
-  __shared__ i32 s_ne;
+  __shared__ i32 s_ne, s_nbad;
   const i32 nrisk = ldc(&a.st->nrisk);
   if (nrisk > kRiskParts) return false;   // block-uniform
   u64* ev_key = s + kMaxMoveCap;      // [kRiskEvents] events as found
   u64* gk = ev_key + kRiskEvents;     // [kRiskEvents] grouped by part
-  u64* gnext = keep;                  // [kRiskEvents] next key of the same part
+  u64* bad_lo = keep;                 // [kRiskEvents] marked key ranges [lo, hi)
+  u64* bad_hi = keep + kRiskEvents;   // [kRiskEvents]
   i32* ev_b = greedy;                 // [kRiskEvents] part index of each event
   i32* ev_d = ev_b + kRiskEvents;     // [kRiskEvents] weight change
   i32* gb = ev_d + kRiskEvents;       // grouped: part index
   i32* gd = gb + kRiskEvents;         // grouped: weight change
-  i32* gbad = gd + kRiskEvents;       // grouped: marks its range
-  i32* bcnt = gbad + kRiskEvents;     // [kRiskParts] events per part
+  i32* bcnt = gd + kRiskEvents;       // [kRiskParts] events per part
   i32* boff = bcnt + kRiskParts;      // [kRiskParts] first grouped slot
   i32* bfill = boff + kRiskParts;     // [kRiskParts]
-  if (threadIdx.x == 0) s_ne = 0;
+  if (threadIdx.x == 0) {
+    s_ne = 0;
+    s_nbad = 0;
+  }
   for (i32 b = threadIdx.x; b < nrisk; b += blockDim.x) {
     bcnt[b] = 0;
     bfill[b] = 0;
   }
   __syncthreads();
-  u64 kmax = 0;
+  u64 kmin = ~0ull, kmax = 0;
   for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) {
     const u64 key = ldc(a.cands + i);
     s[i] = key;
+    kmin = key < kmin ? key : kmin;
     kmax = key > kmax ? key : kmax;
     const i32 v = (i32)(u32)key;
     const i32 src = ldc(a.msrc + v), dst = ldc(a.target + v);
@@ -1169,6 +1208,7 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
     gb[at] = b;
   }
   __syncthreads();
+  // marked key ranges
   for (i32 j = threadIdx.x; j < ne; j += blockDim.x) {
     const i32 b = gb[j];
     const u64 kj = gk[j];
@@ -1179,32 +1219,28 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
       if (kf <= kj) D += gd[f];
       else knext = kf < knext ? kf : knext;
     }
-    gnext[j] = knext;
-    gbad[j] = D > 0 && __uint2float_rn((u32)D + ldc(a.pw + ldc(a.riskpart + b))) > a.maxw;
-  }
-  u64 K = block_reduce_u64<true>(kmax, s_tmp);   // (its barriers publish the marks)
-  for (i32 guard = 0; guard <= ne; ++guard) {
-    // smallest start of a marked range that covers K
-    u64 lo = ~0ull;
-    for (i32 j = threadIdx.x; j < ne; j += blockDim.x)
-      if (gbad[j] && gk[j] <= K && K < gnext[j]) lo = gk[j] < lo ? gk[j] : lo;
-    lo = block_reduce_u64<false>(lo, s_tmp);
-    if (lo == ~0ull) break;   // K is unmarked
-    // the largest key below that start; none: every key is marked
-    u64 below = 0;
-    bool any = false;
-    for (i32 i = threadIdx.x; i < cnt; i += blockDim.x)
-      if (s[i] < lo) {
-        below = s[i] > below ? s[i] : below;
-        any = true;
-      }
-    const u64 pred = block_reduce_u64<true>(any ? below + 1 : 0, s_tmp);   // +1: 0 means none
-    if (pred == 0) {
-      K = lo;   // lo is the smallest key
-      break;
+    if (D > 0 && __uint2float_rn((u32)D + ldc(a.pw + ldc(a.riskpart + b))) > a.maxw) {
+      const i32 at = atomicAdd(&s_nbad, 1);
+      bad_lo[at] = kj;
+      bad_hi[at] = knext;
     }
-    K = pred - 1;
   }
+  kmin = block_reduce_u64<false>(kmin, s_tmp);   // (its barriers publish the ranges)
+  const i32 nbad = s_nbad;
+  // the largest candidate key in no marked range
+  u64 best = 0;
+  bool any = false;
+  for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const u64 key = s[i];
+    bool marked = false;
+    for (i32 r = 0; r < nbad && !marked; ++r) marked = bad_lo[r] <= key && key < bad_hi[r];
+    if (!marked) {
+      best = key > best ? key : best;
+      any = true;
+    }
+  }
+  const u64 top = block_reduce_u64<true>(any ? best + 1 : 0, s_tmp);   // +1: 0 means none
+  const u64 K = top ? top - 1 : kmin;
   __shared__ i32 s_c;
   if (threadIdx.x == 0) s_c = 0;
   __syncthreads();
@@ -1214,6 +1250,7 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
   __syncthreads();
   *kstar = K;
   *napplied = s_c;
+  (void)kmax;
   return true;
 }
 
@@ -1255,7 +1292,28 @@ __device__ void ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* ke
   i32 pos = B - 1;     // sorted: moves 0..pos of keep apply
   if (check) {
     bool done = false;
-    if (cnt <= a.move_cap) done = refine_threshold(a, cnt, s, greedy, keep, s_tmp, s_warp, &kstar, &napplied);
+    if (cnt <= a.move_cap) {
+      // The reference applies moves 0..pos for the LARGEST balanced index
+      // pos (Q11), so when the last index is balanced every candidate moves.
+      // Only the at-risk parts can break it; their change at the last index
+      // is their net change over all candidates.
+      __shared__ i32 s_lastbad;
+      if (threadIdx.x == 0) s_lastbad = 0;
+      __syncthreads();
+      const i32 nrisk = ldc(&st->nrisk);
+      for (i32 b = threadIdx.x; b < nrisk; b += blockDim.x) {
+        const i32 p = ldc(a.riskpart + b);
+        const i32 d = ldc(a.pnet + p);
+        if (d > 0 && __uint2float_rn((u32)d + ldc(a.pw + p)) > a.maxw) s_lastbad = 1;
+      }
+      __syncthreads();
+      if (!s_lastbad) {
+        done = true;   // kstar stays ~0: every candidate applies
+        trace_mark(a, 27);
+      }
+    }
+    if (!done && cnt <= a.move_cap)
+      done = refine_threshold(a, cnt, s, greedy, keep, s_tmp, s_warp, &kstar, &napplied);
     trace_mark(a, 25);
     if (!done) {
       select_sort(a, a.cands, cnt, s, greedy);   // s[0..B) sorted (ends with a block barrier)
@@ -1302,6 +1360,7 @@ __device__ void ph_fold(const LevelArgs& a) {
     }
     if (ldc(a.pin + p)) a.pin[p] = 0;
     if (ldc(a.risk + p)) a.risk[p] = 0;
+    if (ldc(a.pnet + p)) a.pnet[p] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.st->ccount = 0;
@@ -1560,7 +1619,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
   i64 fr = 0;
   trace_mark(a, 0);
   if (a.flags & LF_PROJECT) {
-    ph_project(a);
+    ph_project(a, &s_cnt, &s_base);
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
     trace_mark(a, 1);
   }
@@ -1569,7 +1628,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
     trace_mark(a, 2);
   }
-  if (a.flags & LF_UPDATE) ph_update(a, acc_all, false);
+  if (a.flags & LF_UPDATE) ph_update(a, acc_all, false, s_ustage);
   if (a.flags & LF_BALANCE) {
     if (a.batch) ph_bal_prep_batch(a, s_tmp, fr);
     else ph_bal_prep(a, s_tmp);
@@ -1605,7 +1664,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
       ph_apply_balance(a, s_ustage);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 14);
-      ph_update(a, acc_all, true);
+      ph_update(a, acc_all, true, s_ustage);
       if (a.batch) ph_bal_prep_batch(a, s_tmp, fr);
       else ph_bal_prep(a, s_tmp);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
@@ -1634,7 +1693,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
       }
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 23);
-      ph_update(a, acc_all, true);
+      ph_update(a, acc_all, true, s_ustage);
       if (!a.batch) ph_fold(a);
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 24);
@@ -1695,6 +1754,7 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->msrc = P.alloc_n<i32>(n);
   c->risk = P.alloc_n<u32>(c->k);
   c->riskpart = P.alloc_n<i32>(c->k);
+  c->pnet = P.alloc_n<i32>(c->k);
   c->st = P.alloc_n<RoundState>(1);
   c->bmark = P.alloc_n<u32>(n);
   c->btarget = P.alloc_n<i32>(n);
@@ -1714,6 +1774,7 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   GKW_CUDA(cudaMemsetAsync(c->pwd, 0, sizeof(u32) * c->k, h.stream));   // kept at zero between rounds
   GKW_CUDA(cudaMemsetAsync(c->pin, 0, sizeof(u32) * c->k, h.stream));
   GKW_CUDA(cudaMemsetAsync(c->risk, 0, sizeof(u32) * c->k, h.stream));
+  GKW_CUDA(cudaMemsetAsync(c->pnet, 0, sizeof(i32) * c->k, h.stream));
   GKW_CUDA(cudaMemsetAsync(c->epoch, 0, sizeof(u32), h.stream));
   GKW_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(GridBarrier), h.stream));
   GKW_CUDA(cudaMemsetAsync(c->err, 0, sizeof(i32), h.stream));
@@ -1863,6 +1924,7 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.msrc = c->msrc;
   a.risk = c->risk;
   a.riskpart = c->riskpart;
+  a.pnet = c->pnet;
   a.st = c->st;
   a.bmark = c->bmark;
   a.btarget = c->btarget;

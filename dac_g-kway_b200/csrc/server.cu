@@ -9,9 +9,10 @@
 //
 // Kernels whose CTAs wait on one another (grid barriers) must never hold part
 // of the SMs while waiting for CTAs that other such kernels keep from
-// starting.  Jobs of up to narrow_max_n vertices therefore run in narrow mode:
-// each of those kernels is one thread-block cluster, which the hardware starts
-// as a whole.  Larger jobs use wide grids, and wide launches take turns
+// starting.  Jobs of up to narrow_max_n vertices that start beside other jobs
+// therefore run in narrow mode: each of those kernels is one thread-block
+// cluster, which the hardware starts as a whole.  Larger jobs, and a job that
+// starts while no other runs, use wide grids, and wide launches take turns
 // (launch_coop chains them per device).
 //
 // Admission is by predicted device footprint.  Every slot is charged the
@@ -69,6 +70,7 @@ struct Job {
   i32 slot = -1;
   i32 n_levels = 0;
   i32 batch_graphs = 1;     // graphs of the union run this job was part of
+  bool alone = false;       // no other job was running when this one started
   bool done = false;
   Clock::time_point t_submit, t_start, t_end;
 };
@@ -194,7 +196,10 @@ void gkw_server::run(Slot& s, Job& j) {
   try {
     Handle& hh = handle_of(s.h);
     GKW_CUDA(cudaSetDevice(hh.device));
-    hh.narrow = j.host.n <= cfg.narrow_max_n;
+    // narrow only beside other jobs: a job that starts alone takes the whole
+    // device (jobs that start later beside it run narrow, and a wide grid
+    // only waits for their clusters to finish, never the reverse)
+    hh.narrow = j.host.n <= cfg.narrow_max_n && !j.alone;
     gkw_stats st;
     partition_host(hh, j.host, j.vbase, j.k, j.opt, j.part_out, &j.cut, &st);
     j.n_levels = st.n_levels;
@@ -366,6 +371,7 @@ void gkw_server::worker(size_t si) {
         c->slot = (i32)si;
         c->t_start = now;
         c->batch_graphs = (i32)jobs.size();
+        c->alone = running == 1;
       }
     }
     if (jobs.size() == 1) run(slots[si], *jobs[0]);
