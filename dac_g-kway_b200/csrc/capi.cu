@@ -128,6 +128,8 @@ gkw_status gkw_create(gkw_handle** out, int32_t device) {
       GKW_CUDA(e);
     }
     h->h.own_stream = true;
+    // GKW_GRAPHS=0: launch sequences always run as is (no CUDA-graph replay)
+    if (const char* gs = getenv("GKW_GRAPHS")) h->h.graphs_on = *gs != '0';
     e = cudaMallocHost(&h->h.h_pinned, 64 * sizeof(int64_t));
     if (e != cudaSuccess) {
       cudaStreamDestroy(h->h.stream);
@@ -167,6 +169,7 @@ gkw_status gkw_destroy(gkw_handle* h) {
     if (h->h.arena) cudaFree(h->h.arena);
     if (h->h.tev_ready)
       for (cudaEvent_t e : h->h.tev) cudaEventDestroy(e);
+    graph_cache_clear(h->h);
     forget_coop_event(h->h);
     delete h;
     cudaGetLastError();   // teardown is best effort: leave no error pending for later calls

@@ -279,8 +279,8 @@ void run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out, i32* d_rou
   Pool::Mark mk = h.scratch.mark();
   u64* kb = h.scratch.alloc_n<u64>(n);
   i32* chg = h.scratch.alloc_n<i32>(3);
-  int bps = 0;
-  GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_uf_persist, kUfThreads, 0));
+  static int bps = 0;   // the same on every device of the process (one B200 model)
+  if (!bps) GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_uf_persist, kUfThreads, 0));
   GKW_REQUIRE(bps >= 1, GKW_E_INTERNAL, "union-find kernel does not fit on an SM");
   i32 grid = std::min<i32>(h.sm_count * std::min(bps, 2), (i32)ceil_div(n, kUfThreads));
   grid = coop_grid(h, (const void*)k_uf_persist, grid, kUfThreads, 0);
@@ -893,6 +893,8 @@ __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__
 
 void ensure_arena(Handle& h, u64 words) {
   if (h.arena && h.arena_words >= words) return;
+  GKW_REQUIRE(!h.capturing, GKW_E_INTERNAL, "arena grown during a graph capture");
+  graph_cache_clear(h);   // graphs hold the old arena's address
   GKW_CUDA(cudaStreamSynchronize(h.stream));
   if (h.arena) GKW_CUDA(cudaFree(h.arena));
   h.arena = nullptr;
@@ -934,13 +936,15 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc
   if (avgL <= 48) {
     constexpr int W = 128, WARPS = 8;
     const size_t sm = sizeof(WarpTable<W>) * WARPS;
-    GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (!h.capturing)
+      GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, d_nc, g.xadj, g.adjncy, g.adjwgt, cmap,
            memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
   } else {
     constexpr int W = 512, WARPS = 8;
     const size_t sm = sizeof(WarpTable<W>) * WARPS;
-    GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (!h.capturing)
+      GKW_CUDA(cudaFuncSetAttribute(k_contract_warp<W, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     launch(k_contract_warp<W, WARPS>, gridw, WARPS * 32, sm, h.stream, d_nc, g.xadj, g.adjncy, g.adjwgt, cmap,
            memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, heavy, misc);
   }
@@ -949,7 +953,8 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc
   // (2*kCtaCap table slots, a power of two, + kCtaCap sorted outputs: 96 KB)
   constexpr i32 kCtaCap = 4096;
   const size_t csm = (size_t)kCtaCap * 2 * 4 * 2 + (size_t)kCtaCap * 8;
-  GKW_CUDA(cudaFuncSetAttribute(k_contract_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  if (!h.capturing)
+    GKW_CUDA(cudaFuncSetAttribute(k_contract_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   launch(k_contract_cta<false>, (u32)h.sm_count * 2, 512, csm, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
          g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, h.arena, words, h.arena_words);
   launch(k_contract_cta<true>, (u32)h.sm_count, 512, 0, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
@@ -1001,30 +1006,81 @@ __global__ void k_max_cvw(const i32* __restrict__ ncp, const i32* __restrict__ c
   if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
 }
 
+// The key of one level's launch sequence in the handle's graph cache:
+// everything the launches depend on.
+static std::string level_key(const Handle& h, const DevGraph& g, i32 cap, const CoarsenOut& out) {
+  struct K {
+    i64 n, m, maxdeg, cap;
+    const void* in[4];
+    const void* outp[5];
+    const void* sbase;
+    size_t stop;
+    gkw_tuning tuning;
+    i32 narrow, sms;
+    const void* arena;
+    u64 arena_words;
+    const void* scan;
+  } k;
+  memset(&k, 0, sizeof(k));
+  k.n = g.n;
+  k.m = g.m;
+  k.maxdeg = g.maxdeg;
+  k.cap = cap;
+  k.in[0] = g.xadj;
+  k.in[1] = g.adjncy;
+  k.in[2] = g.adjwgt;
+  k.in[3] = g.vwgt;
+  k.outp[0] = out.cmap;
+  k.outp[1] = out.cxadj;
+  k.outp[2] = out.cvwgt;
+  k.outp[3] = out.cadjncy;
+  k.outp[4] = out.cadjwgt;
+  const auto fp = h.scratch.fingerprint();
+  k.sbase = fp.first;
+  k.stop = fp.second;
+  k.tuning = h.tuning;
+  k.narrow = h.narrow;
+  k.sms = h.sm_count;
+  k.arena = h.arena;
+  k.arena_words = h.arena_words;
+  k.scan = h.scan;
+  return std::string("level", 5) + std::string(reinterpret_cast<const char*>(&k), sizeof(k));
+}
+
+// One coarsening step.  Its launch sequence (about twenty kernels and ten
+// memsets, all sized by the level's n and m) runs through the handle's graph
+// cache: repeated partitions of the same graph replay it as one CUDA graph.
+// One host sync per level reads the coarse sizes.
 void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
-  Pool::Mark mk = h.scratch.mark();
-  i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
-  u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
-  if (h.tune_collect) time_match_variants(h, g, cand);
-  run_match(h, g, cand, g.maxdeg);
-  run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
+  // coarse arrays at upper bounds (n_c <= n, m_c <= m)
   out.cmap = h.hier.alloc_n<i32>(std::max(g.n, 1));
-  run_group_map(h, g.n, keys, cap, out.cmap, &h.coop->nc);
-  h.scratch.release(mk);
-  // coarse arrays at upper bounds (n_c <= n, m_c <= m); one host sync per level
-  GKW_CUDA(cudaMemsetAsync(&h.coop->maxdeg, 0, sizeof(i32), h.stream));
   out.cxadj = h.hier.alloc_n<i32>((i64)g.n + 1);
   out.cvwgt = h.hier.alloc_n<i32>(std::max(g.n, 1));
   out.cadjncy = h.hier.alloc_n<i32>(std::max<i64>(g.m, 1));
   out.cadjwgt = h.hier.alloc_n<i32>(std::max<i64>(g.m, 1));
-  run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
-               &h.coop->mc);
-  GKW_CUDA(cudaMemsetAsync(&h.coop->max_cvw, 0, sizeof(i32), h.stream));
-  if (g.n > 0) {
-    const u32 gm = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)h.sm_count * 4));
-    launch(k_max_cvw, gm, 256, 0, h.stream, &h.coop->nc, out.cvwgt, &h.coop->max_cvw);
-    GKW_CHECK_LAUNCH();
-  }
+  ensure_arena(h, u64(4) << 20);   // never inside a capture
+  const bool tune = h.tune_collect;
+  auto body = [&] {
+    Pool::Mark mk = h.scratch.mark();
+    i32* cand = h.scratch.alloc_n<i32>(std::max(g.n, 1));
+    u64* keys = h.scratch.alloc_n<u64>(std::max(g.n, 1));
+    if (tune) time_match_variants(h, g, cand);
+    run_match(h, g, cand, g.maxdeg);
+    run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
+    run_group_map(h, g.n, keys, cap, out.cmap, &h.coop->nc);
+    h.scratch.release(mk);
+    GKW_CUDA(cudaMemsetAsync(&h.coop->maxdeg, 0, sizeof(i32), h.stream));
+    run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
+                 &h.coop->mc);
+    GKW_CUDA(cudaMemsetAsync(&h.coop->max_cvw, 0, sizeof(i32), h.stream));
+    if (g.n > 0) {
+      const u32 gm = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)h.sm_count * 4));
+      launch(k_max_cvw, gm, 256, 0, h.stream, &h.coop->nc, out.cvwgt, &h.coop->max_cvw);
+      GKW_CHECK_LAUNCH();
+    }
+  };
+  if (tune) body();   // the tuner's timings synchronise: never captured
+  else graph_run(h, level_key(h, g, cap, out), body);
   CoopState c = read_coop(h);
   if (c.arena_overflow) {   // very long coarse rows: grow the arena and redo the step
     ensure_arena(h, (u64)((double)(h.arena_words + (u64)c.arena_need) * 1.25) + 1024);

@@ -13,6 +13,8 @@ static thread_local std::string g_last_error;
 static std::atomic<uint64_t> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launches(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 uint64_t launch_total() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
@@ -151,12 +153,15 @@ __device__ __forceinline__ i32 block_exclusive_scan(i32 x, i32* s_warp, i32& tot
 // Single-pass scan with decoupled look-back.  Tile t publishes its aggregate
 // (status 1) and then its inclusive prefix (status 2) in a status word
 // (epoch << 34 | status << 32 | value); a word of an older epoch reads as
-// "not published".  Tiles take tickets from a persistent 64-bit counter in
-// launch order (tile = ticket - base, base = tickets handed out by earlier
-// calls), so a tile only waits on tiles that already hold an SM.  A wait
-// longer than kScanSpinCycles sets the error word and the tile continues
-// (the result is then reported as an error, never a hang).
+// "not published".  Tiles take tickets in launch order, so a tile only waits
+// on tiles that already hold an SM.  The ticket counter, the epoch and a
+// finished-tile counter live on the device: the last tile to finish resets
+// the counters and advances the epoch for the next scan, so a scan needs no
+// per-call argument from the host (it can be replayed from a CUDA graph).  A
+// wait longer than kScanSpinCycles sets the error word and the tile
+// continues (the result is then reported as an error, never a hang).
 constexpr long long kScanSpinCycles = 2000000000ll;
+constexpr u32 kScanEpochMask = (1u << 29) - 1;
 
 __device__ __forceinline__ u64 ld_relaxed_gpu_u64(const unsigned long long* p) {
   u64 v;
@@ -165,13 +170,18 @@ __device__ __forceinline__ u64 ld_relaxed_gpu_u64(const unsigned long long* p) {
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const i32* in, i32* out, i64 n, i32* total,
-                                                             ScanState* ss, u64 base, u64 epoch, i32 ntiles) {
+                                                             ScanState* ss, i32 ntiles) {
   __shared__ i32 s_warp[33];
   __shared__ i32 s_tile;
   __shared__ i32 s_excl;
-  if (threadIdx.x == 0) s_tile = (i32)(atomicAdd((unsigned long long*)&ss->ticket, 1ull) - base);
+  __shared__ u32 s_epoch;
+  if (threadIdx.x == 0) {
+    s_tile = (i32)atomicAdd(&ss->ticket, 1u);
+    s_epoch = *(volatile u32*)&ss->epoch;   // set by the previous scan, stream-ordered before this one
+  }
   __syncthreads();
   const i32 tile = s_tile;
+  const u64 epoch = s_epoch;
   const i64 b0 = (i64)tile * kScanTile + (i64)threadIdx.x * kScanItems;
   i32 v[kScanItems];
   i32 sum = 0;
@@ -235,6 +245,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const i32* in, i32*
     if (b0 + i < n) out[b0 + i] = run;
     run += v[i];
   }
+  if (threadIdx.x == 0) {
+    // the last tile to finish: every other tile has taken its ticket, read
+    // the epoch and published; reset for the next scan
+    __threadfence();
+    if (atomicAdd(&ss->done, 1u) == (u32)ntiles - 1) {
+      ss->ticket = 0;
+      ss->done = 0;
+      ss->epoch = (ss->epoch + 1) & kScanEpochMask;
+      __threadfence();
+    }
+  }
 }
 
 __global__ void k_set_i32(i32* p, i32 v) { *p = v; }
@@ -248,26 +269,31 @@ void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total) {
   const i64 nt64 = (n + kScanTile - 1) / kScanTile;
   GKW_REQUIRE(nt64 < (i64)1 << 30, GKW_E_UNSUPPORTED, "scan too large");
   const i32 nt = (i32)nt64;
-  if (h.scan_tiles_cap < nt) {
+  // the device epoch wraps after 2^29 scans: before it could meet a status
+  // word of the same epoch, start again from cleared state (never inside a
+  // graph capture: a captured scan's epoch is read on the device)
+  const bool fresh = h.scan_tiles_cap < nt || (h.scan_epoch >= kScanEpochMask - 4096 && !h.capturing);
+  if (fresh) {
+    GKW_REQUIRE(!h.capturing, GKW_E_INTERNAL, "scan state grown during a graph capture");
     // queued scans may still use the old state; the new state is cleared on
     // the handle's stream (which does not wait for the legacy stream), so the
     // scan below sees it cleared
     GKW_CUDA(cudaStreamSynchronize(h.stream));
-    if (h.scan) GKW_CUDA(cudaFree(h.scan));
-    h.scan = nullptr;
-    const i32 cap = std::max(nt, 1024);
-    GKW_CUDA(cudaMalloc(&h.scan, sizeof(ScanState) + sizeof(u64) * (size_t)cap));
-    GKW_CUDA(cudaMemsetAsync(h.scan, 0, sizeof(ScanState) + sizeof(u64) * (size_t)cap, h.stream));
-    h.scan_tiles_cap = cap;
-    h.scan_tickets = 0;
+    const i32 cap = std::max(nt, h.scan_tiles_cap < nt ? std::max(nt, 1024) : h.scan_tiles_cap);
+    if (h.scan_tiles_cap < nt) {
+      if (h.scan) GKW_CUDA(cudaFree(h.scan));
+      h.scan = nullptr;
+      GKW_CUDA(cudaMalloc(&h.scan, sizeof(ScanState) + sizeof(u64) * (size_t)cap));
+      h.scan_tiles_cap = cap;
+      graph_cache_clear(h);   // graphs hold the old state's address
+    }
+    GKW_CUDA(cudaMemsetAsync(h.scan, 0, sizeof(ScanState) + sizeof(u64) * (size_t)h.scan_tiles_cap, h.stream));
     h.scan_epoch = 0;
   }
-  h.scan_epoch += 1;
-  GKW_REQUIRE(h.scan_epoch < ((u64)1 << 29), GKW_E_INTERNAL, "scan epoch overflow");
-  launch(k_scan_1pass, nt, kScanThreads, 0, h.stream, in, out, n, total, h.scan, h.scan_tickets, h.scan_epoch,
-         nt);
+  h.scan_epoch += 1;   // host mirror of the device epoch (wrap guard only)
+  ++h.scans_enqueued;
+  launch(k_scan_1pass, nt, kScanThreads, 0, h.stream, in, out, n, total, h.scan, nt);
   GKW_CHECK_LAUNCH();
-  h.scan_tickets += (u64)nt;
 }
 
 namespace {
@@ -355,6 +381,22 @@ void launch_coop(Handle& h, const void* kern, i32 grid, i32 block, size_t smem, 
     return;
   }
   GKW_REQUIRE(h.device >= 0 && h.device < kMaxDevices, GKW_E_UNSUPPORTED, "device index too large");
+  if (h.capturing) {   // in a graph: graph_run chains the whole graph instead
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    GKW_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
+    count_launch();
+    h.capture_wide = true;
+    return;
+  }
   if (!h.coop_ev) GKW_CUDA(cudaEventCreateWithFlags(&h.coop_ev, cudaEventDisableTiming));
   std::lock_guard<std::mutex> lk(g_chain_mu[h.device]);
   if (g_chain_last[h.device] && g_chain_last[h.device] != h.coop_ev)
@@ -363,6 +405,85 @@ void launch_coop(Handle& h, const void* kern, i32 grid, i32 block, size_t smem, 
   count_launch();
   GKW_CUDA(cudaEventRecord(h.coop_ev, h.stream));
   g_chain_last[h.device] = h.coop_ev;
+}
+
+void graph_cache_clear(Handle& h) {
+  for (Handle::GraphEntry& e : h.graphs)
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+  h.graphs.clear();
+}
+
+bool graph_run(Handle& h, const std::string& key, const std::function<void()>& body) {
+  if (!h.graphs_on || h.capturing) {
+    body();
+    return false;
+  }
+  Handle::GraphEntry* e = nullptr;
+  for (Handle::GraphEntry& x : h.graphs)
+    if (x.key == key) e = &x;
+  if (!e) {   // first sight: run as is (pools grow, shapes settle)
+    if (h.graphs.size() >= 64) graph_cache_clear(h);
+    h.graphs.push_back(Handle::GraphEntry{key, 1});
+    body();
+    return false;
+  }
+  if (!e->exec) {   // second sight: capture, then run the graph
+    const u64 l0 = launch_total(), s0 = h.scans_enqueued, ep0 = h.scan_epoch;
+    cudaGraph_t g = nullptr;
+    h.capture_wide = false;
+    cudaError_t err = cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      h.capturing = true;
+      try {
+        body();
+      } catch (...) {
+        h.capturing = false;
+        cudaStreamEndCapture(h.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        uncount_launches(launch_total() - l0);
+        h.scans_enqueued = s0;
+        h.scan_epoch = ep0;
+        h.graphs_on = false;   // the body needs something a capture cannot hold: run it plainly from now on
+        body();
+        return false;
+      }
+      h.capturing = false;
+      err = cudaStreamEndCapture(h.stream, &g);
+    }
+    const u64 nl = launch_total() - l0, ns = h.scans_enqueued - s0;
+    uncount_launches(nl);   // nothing ran yet
+    h.scans_enqueued = s0;
+    h.scan_epoch = ep0;
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&e->exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      e->exec = nullptr;
+      h.graphs_on = false;
+      body();
+      return false;
+    }
+    e->launches = nl;
+    e->scans = ns;
+    e->wide = h.capture_wide;
+  }
+  if (e->wide) {   // wide launches of all handles take turns (launch_coop)
+    GKW_REQUIRE(h.device >= 0 && h.device < kMaxDevices, GKW_E_UNSUPPORTED, "device index too large");
+    if (!h.coop_ev) GKW_CUDA(cudaEventCreateWithFlags(&h.coop_ev, cudaEventDisableTiming));
+    std::lock_guard<std::mutex> lk(g_chain_mu[h.device]);
+    if (g_chain_last[h.device] && g_chain_last[h.device] != h.coop_ev)
+      GKW_CUDA(cudaStreamWaitEvent(h.stream, g_chain_last[h.device], 0));
+    GKW_CUDA(cudaGraphLaunch(e->exec, h.stream));
+    GKW_CUDA(cudaEventRecord(h.coop_ev, h.stream));
+    g_chain_last[h.device] = h.coop_ev;
+  } else {
+    GKW_CUDA(cudaGraphLaunch(e->exec, h.stream));
+  }
+  count_launches(e->launches);
+  h.scans_enqueued += e->scans;
+  h.scan_epoch += e->scans;
+  return true;
 }
 
 // Drop a handle's chain event (the handle is going away).

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <utility>
 #include <vector>
@@ -57,6 +58,12 @@ class Pool {
   T* alloc_n(size_t n) { return static_cast<T*>(alloc(n * sizeof(T))); }
   struct Mark { size_t chunk; size_t top; };
   Mark mark() const { return {cur_, chunks_.empty() ? 0 : chunks_[cur_].top}; }
+  // Where the next allocations will land (current chunk's base and top): two
+  // equal fingerprints hand out the same addresses for the same requests.
+  std::pair<const void*, size_t> fingerprint() const {
+    return chunks_.empty() ? std::pair<const void*, size_t>{nullptr, 0}
+                           : std::pair<const void*, size_t>{chunks_[cur_].base, chunks_[cur_].top};
+  }
   void release(Mark m);
   void reset() { release({0, 0}); }
   size_t capacity() const;
@@ -142,12 +149,15 @@ struct ArenaHdr {
   i32 pad;
 };
 
-// Single-pass scan state (one per handle): ticket counter, error word, tile
-// status words follow the header.
+// Single-pass scan state (one per handle): the current scan's ticket and
+// finished-tile counters and its epoch (all kept on the device, so a scan
+// replayed from a CUDA graph needs no host-side argument), the error word;
+// tile status words follow the header.
 struct ScanState {
-  u64 ticket;
+  u32 ticket;
+  u32 done;
+  u32 epoch;
   i32 err;
-  i32 pad;
   u64 tiles[1];
 };
 
@@ -167,8 +177,21 @@ struct Handle {
   ArenaHdr* arena = nullptr;    // long-row hash tables: header + words
   u64 arena_words = 0;
   i32 scan_tiles_cap = 0;
-  u64 scan_tickets = 0;         // tickets handed out so far
-  u64 scan_epoch = 0;
+  u64 scan_epoch = 0;           // host mirror of the device scan epoch (wrap guard)
+  u64 scans_enqueued = 0;
+  // CUDA-graph replay of launch sequences (graph_run): captured sequences by
+  // key, whether capture is on for this handle, and whether one is running
+  struct GraphEntry {
+    std::string key;
+    int seen = 0;
+    cudaGraphExec_t exec = nullptr;
+    u64 launches = 0, scans = 0;
+    bool wide = false;   // holds a cooperative (non-cluster) launch
+  };
+  std::vector<GraphEntry> graphs;
+  bool graphs_on = true;
+  bool capturing = false;
+  bool capture_wide = false;
   // timing events of the partition driver: 5 phase marks, then a start/end
   // pair per level-kernel launch; created on first use, destroyed with the handle
   static constexpr int kTimerEvents = 5 + 2 * kMaxLevels;
@@ -202,6 +225,18 @@ i32 coop_grid(Handle& h, const void* kern, i32 want, i32 block, size_t smem);
 // previous one to finish): two wide grids running at once could each hold
 // part of the SMs and wait for the rest.
 void launch_coop(Handle& h, const void* kern, i32 grid, i32 block, size_t smem, void** args);
+// Runs `body` (a sequence of launches, memsets and copies on h.stream, no
+// host synchronisation) through the handle's graph cache: the first time a
+// key is seen the body runs as is; the second time it is captured into a CUDA
+// graph, which then runs in its place, that time and every later time.  The
+// key must name everything the body's launches depend on (sizes, pointers,
+// the scratch pool's position, launch shapes).  Returns true if a graph ran.
+// Results never differ from running the body.
+bool graph_run(Handle& h, const std::string& key, const std::function<void()>& body);
+void graph_cache_clear(Handle& h);
+// Removes launches counted during a capture (they run only with the graph).
+void uncount_launches(uint64_t n);
+void count_launches(uint64_t n);
 void forget_coop_event(Handle& h);   // before the handle is destroyed
 
 // ---- kernel launches ----

@@ -933,11 +933,57 @@ __global__ void k_init_fill_batch(i32 n, const i32* __restrict__ gid, const i32*
   }
 }
 
+static void device_init_partition_body(Handle& h, const DevGraph& g, i32 k, double eps, u64 seed, i32 trials,
+                                       i32* d_part, const GggpBatch* batch);
+
+// The launch sequence (a handful of launches per recursion depth, sized by n
+// and k) runs through the handle's graph cache, except when traced or batched.
 void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 seed, i32 trials,
                            i32* d_part, const GggpBatch* batch) {
   GKW_REQUIRE(trials >= 1 && trials <= kInitTrials, GKW_E_INVALID, "init trials must be in [1, 8]");
+  if (g.n == 0) return;
+  GKW_CUDA(cudaFuncSetAttribute(k_gggp_big_trial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpBigSmem));
+  GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
+  const bool trace = getenv("GKW_TRACE") && *getenv("GKW_TRACE") == '1';
+  auto body = [&] { device_init_partition_body(h, g, k, eps, seed, trials, d_part, batch); };
+  if (trace || batch) {
+    body();
+    return;
+  }
+  struct K {
+    i64 n, m, k, trials;
+    double eps;
+    u64 seed;
+    const void* p[5];
+    const void* sbase;
+    size_t stop;
+    i32 narrow, sms;
+    const void* scan;
+  } key;
+  memset(&key, 0, sizeof(key));
+  key.n = g.n;
+  key.m = g.m;
+  key.k = k;
+  key.trials = trials;
+  key.eps = eps;
+  key.seed = seed;
+  key.p[0] = g.xadj;
+  key.p[1] = g.adjncy;
+  key.p[2] = g.adjwgt;
+  key.p[3] = g.vwgt;
+  key.p[4] = d_part;
+  const auto fp = h.scratch.fingerprint();
+  key.sbase = fp.first;
+  key.stop = fp.second;
+  key.narrow = h.narrow;
+  key.sms = h.sm_count;
+  key.scan = h.scan;
+  graph_run(h, std::string("gggp", 4) + std::string(reinterpret_cast<const char*>(&key), sizeof(key)), body);
+}
+
+static void device_init_partition_body(Handle& h, const DevGraph& g, i32 k, double eps, u64 seed, i32 trials,
+                                       i32* d_part, const GggpBatch* batch) {
   const i32 n = g.n;
-  if (n == 0) return;
   Pool::Mark mk = h.scratch.mark();
   i32* lo[2] = {h.scratch.alloc_n<i32>(n), h.scratch.alloc_n<i32>(n)};
   i32* hi[2] = {h.scratch.alloc_n<i32>(n), h.scratch.alloc_n<i32>(n)};
@@ -973,9 +1019,7 @@ void device_init_partition(Handle& h, const DevGraph& g, i32 k, double eps, u64 
     tcut = h.scratch.alloc_n<i64>((size_t)k * kInitTrials);
     tdev = h.scratch.alloc_n<i64>((size_t)k * kInitTrials);
     g_R = h.scratch.alloc_n<u8>((size_t)kInitTrials * n);
-    GKW_CUDA(cudaFuncSetAttribute(k_gggp_big_trial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpBigSmem));
   }
-  GKW_CUDA(cudaFuncSetAttribute(k_gggp_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGggpSmem));
   const u32 nb = ceil_div(n, 256);
   i32 depth = 0;
   if (batch) {

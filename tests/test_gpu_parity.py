@@ -317,3 +317,42 @@ def test_autotune_keeps_results(pkg, gen):
     with pytest.raises(pkg.GkwError):
         h.set_tuning(match_lanes=(3, 8, 16, 32))
     h.close()
+
+
+def test_graph_replay_matches_plain_launches(pkg, gen, orc):
+    """Repeated partitions replay each coarsening level's and the initial
+    partition's launch sequence from a captured CUDA graph (second sight:
+    capture; later: replay).  Every result equals a handle that never
+    captures (GKW_GRAPHS=0) and the oracle, also after the input's contents
+    change in place (same buffers and sizes, other weights)."""
+    import os
+    import torch
+    from conftest import to_dev
+    g = weighted(gen, gen.delaunay(60000, 17), seed=3)
+    os.environ["GKW_GRAPHS"] = "0"
+    try:
+        plain = pkg.Handle(0)
+    finally:
+        del os.environ["GKW_GRAPHS"]
+    h = pkg.Handle(0)
+    dg = to_dev(g)
+    k = 24
+    for step in range(6):
+        if step == 3:   # new edge weights in the same device buffers
+            src = np.repeat(np.arange(g.n), np.diff(g.xadj)).astype(np.int64)
+            lo, hi = np.minimum(src, g.adjncy), np.maximum(src, g.adjncy)
+            w = 1 + (lo * 1000003 + hi * 7919) % 8   # symmetric by construction
+            dg[2].copy_(torch.from_numpy(w.astype(np.int32)))
+        p1 = torch.empty(g.n, dtype=torch.int32, device="cuda:0")
+        p2 = torch.empty(g.n, dtype=torch.int32, device="cuda:0")
+        c1, s1 = h.partition_device(*dg, k, p1)
+        c2, s2 = plain.partition_device(*dg, k, p2)
+        assert np.array_equal(p1.cpu().numpy(), p2.cpu().numpy()) and c1 == c2, step
+        assert s1["level_n"] == s2["level_n"] and s1["refine_rounds"] == s2["refine_rounds"], step
+        if step in (2, 5):
+            cur = gen.Csr(g.xadj, g.adjncy, dg[2].cpu().numpy(), g.vwgt)
+            ref, info = orc.partition(cur, k, init=lambda x, a, ww, vw, kk: orc.init_partition(gen.Csr(x, a, ww, vw), kk),
+                                      enforce_balance=True)
+            assert np.array_equal(p1.cpu().numpy(), ref) and c1 == info["cut"], step
+    h.close()
+    plain.close()
