@@ -253,6 +253,21 @@ def bench_ours(args):
     ms = sum(step_ms) / len(step_ms)
     ms_max = max_over_ranks(ms, world, dev)
 
+    if args.device_only:
+        roof, phase_roof = roofline_report(steps_stats)
+        h.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": world * g.n_edges / (ms_max / 1e3), "unit": "edges/s",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                              "device_only": True, "gpu_launches": int(launches), "roofline": roof,
+                              "phase_roofline": phase_roof, "cut": int(cut),
+                              "phase_ms": {"coarsen": st["ms_coarsen"], "init": st["ms_init"],
+                                           "refine": st["ms_refine"], "total": st["ms_total"]},
+                              "clocks": clocks}))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
     # ---- e2e: host API, pinned host buffers, copies inside ----
     hx, ha, hw, hv = (torch.from_numpy(a).pin_memory() for a in (g.xadj, g.adjncy, g.adjwgt, g.vwgt))
     hpart = torch.empty(g.n, dtype=torch.int32).pin_memory()
@@ -713,6 +728,8 @@ def bench_configs(args):
             h.partition_device(*t, k, part)
         ms = []
         cut = st = None
+        sampler = ClockSampler(0)
+        sampler.start()
         for _ in range(max(1, args.steps)):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -723,13 +740,15 @@ def bench_configs(args):
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+        clocks = sampler.stop()
         p = part.cpu().numpy()
         W = int(g.vwgt.astype(np.int64).sum())
         pw = np.bincount(p, weights=g.vwgt, minlength=k)
         m = statistics.median(ms)
         out.append({"config": name, "n": g.n, "edges": g.n_edges, "k": k, "ms": m, "edges_per_s": g.n_edges / (m / 1e3),
                     "cut": int(cut), "balance": float(pw.max() * k / W), "levels": st["level_n"],
-                    "phase_ms": {"coarsen": st["ms_coarsen"], "init": st["ms_init"], "refine": st["ms_refine"]}})
+                    "phase_ms": {"coarsen": st["ms_coarsen"], "init": st["ms_init"], "refine": st["ms_refine"]},
+                    "clocks": clocks})
         print(json.dumps(out[-1]), flush=True)
         h.close()
         del t, part, flush
@@ -756,6 +775,9 @@ def main():
                     help="plain workload: skip gkw_autotune (default launch shapes; profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain workload: leave the batched and served objects out of the line")
+    ap.add_argument("--device-only", action="store_true",
+                    help="plain workload: only the device-resident steps (no e2e, CPU baseline, batched or "
+                         "served legs); for profiling runs")
     args = ap.parse_args()
     if args.workload == "configs":
         bench_configs(args)

@@ -119,11 +119,13 @@ class Stats(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("match_lanes", ctypes.c_int32 * 4), ("level_verts_per_cta", ctypes.c_int32),
-                ("level_min_ctas", ctypes.c_int32)]
+                ("level_min_ctas", ctypes.c_int32), ("coarsen_fused_max_n", ctypes.c_int32),
+                ("coarsen_verts_per_cta", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {"match_lanes": list(self.match_lanes), "level_verts_per_cta": int(self.level_verts_per_cta),
-                "level_min_ctas": int(self.level_min_ctas)}
+                "level_min_ctas": int(self.level_min_ctas), "coarsen_fused_max_n": int(self.coarsen_fused_max_n),
+                "coarsen_verts_per_cta": int(self.coarsen_verts_per_cta)}
 
 
 class ServerConfig(ctypes.Structure):
@@ -496,8 +498,10 @@ class Handle:
         check(lib().gkw_get_tuning(self._h, ctypes.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, match_lanes=(4, 8, 16, 32), level_verts_per_cta=512, level_min_ctas=32) -> None:
-        t = Tuning((ctypes.c_int32 * 4)(*match_lanes), int(level_verts_per_cta), int(level_min_ctas))
+    def set_tuning(self, match_lanes=(4, 8, 16, 32), level_verts_per_cta=512, level_min_ctas=32,
+                   coarsen_fused_max_n=0, coarsen_verts_per_cta=256) -> None:
+        t = Tuning((ctypes.c_int32 * 4)(*match_lanes), int(level_verts_per_cta), int(level_min_ctas),
+                   int(coarsen_fused_max_n), int(coarsen_verts_per_cta))
         check(lib().gkw_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, xadj, adjncy, adjwgt, vwgt, k: int, opts: Options | None = None) -> dict:

@@ -194,6 +194,8 @@ static void check_tuning(const gkw_tuning& t) {
                 GKW_E_INVALID, "match_lanes must be 4, 8, 16 or 32");
   GKW_REQUIRE(t.level_verts_per_cta >= 32 && t.level_min_ctas >= 1, GKW_E_INVALID,
               "level_verts_per_cta must be >= 32 and level_min_ctas >= 1");
+  GKW_REQUIRE(t.coarsen_fused_max_n >= 0 && t.coarsen_verts_per_cta >= 64, GKW_E_INVALID,
+              "coarsen_fused_max_n must be >= 0 and coarsen_verts_per_cta >= 64");
 }
 
 gkw_status gkw_get_tuning(gkw_handle* h, gkw_tuning* out) {

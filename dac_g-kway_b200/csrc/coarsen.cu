@@ -790,8 +790,10 @@ __global__ void __launch_bounds__(512) k_contract_cta(
         }
       }
       __syncthreads();
-      if (s_off == ~0ull) continue;   // block-uniform; redone after the arena grows
-      keys = arena_words + s_off;
+      const u64 off = s_off;
+      __syncthreads();   // every thread has read s_off before thread 0 can set it for the next row
+      if (off == ~0ull) continue;   // block-uniform; redone after the arena grows
+      keys = arena_words + off;
       vals = keys + hsz;
       out = reinterpret_cast<u64*>(vals + hsz);
     } else {
@@ -1006,6 +1008,857 @@ __global__ void k_max_cvw(const i32* __restrict__ ncp, const i32* __restrict__ c
   if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
 }
 
+// ===========================================================================
+// Fused coarsening step: one persistent launch per level runs every phase of
+// the step above -- heavy-edge candidates, union-find rounds, group sizes and
+// coarse ids, group orders, member lists, contraction, coarse xadj and row
+// compaction -- with grid barriers between the phases instead of about twenty
+// kernel launches and ten memsets.  The phase bodies apply the same rules to
+// the same keys as the per-phase kernels, so the level is identical; the
+// scans are grid-wide (each CTA scans a contiguous range after a barrier
+// publishes the CTA sums).  Data written by other CTAs in the launch is read
+// with ld.global.cg.  Dynamic shared memory (96 KB) is shared by the phases:
+// the warps' contraction tables, the CTA group sorts and the CTA table of
+// heavy coarse rows.
+// ===========================================================================
+constexpr int kFusedThreads = 512;
+constexpr int kFusedWarps = kFusedThreads / 32;
+constexpr i32 kFusedWcap = 128;      // warp table entries (as k_contract_warp<128, 8>)
+constexpr i32 kFusedCtaCap = 4096;   // heavy rows up to this length use the shared table
+constexpr size_t kFusedSmem = (size_t)kFusedCtaCap * 2 * 4 * 2 + (size_t)kFusedCtaCap * 8;   // 96 KB
+static_assert(kFusedSmem >= sizeof(WarpTable<kFusedWcap>) * kFusedWarps, "warp tables fit");
+static_assert(kFusedSmem >= sizeof(u64) * kGroupSmem, "CTA group sort fits");
+
+// misc counters of the fused step (zeroed by the host before the launch)
+enum { kFzLong = 0, kFzWarpG = 1, kFzGiant = 2, kFzCtaG = 3, kFzHeavy = 4, kFzBig = 5, kFzUb = 6, kFzWords = 8 };
+
+struct FusedArgs {
+  i32 n;
+  i64 m;
+  const i32* xadj;
+  const i32* adjncy;
+  const i32* adjwgt;
+  const i32* vwgt;
+  i32 lanes;     // match lanes per vertex (4, 8, 16, 32)
+  i32 split;     // rows above kMatchLong may exist
+  i32 cap;       // group cap
+  i32 max_rounds;
+  // outputs (coarse level at upper bounds)
+  i32* cmap;
+  i32* cxadj;
+  i32* cadjncy;
+  i32* cadjwgt;
+  i32* cvwgt;
+  // scratch
+  i32* cand;
+  u64* k0;
+  u64* k1;
+  i32* chg;        // [3]
+  i32* longlist;   // [n]
+  i32* gsize;      // [n]
+  i32* cbase;      // [n] first coarse id of each root
+  i32* goff;       // [n] member offset of each big group
+  i32* gcur;       // [n]
+  i32* members;    // [n]
+  i32* wlist;      // [n] groups sorted by a warp
+  i32* clist;      // [n] groups sorted by a CTA
+  i32* glist;      // [n] giant groups
+  u64* gscratch;   // [2n] giant sort network
+  i32* rowlen;     // [n + 1]
+  i32* ub;         // [n + 1]
+  i32* mcnt;       // [n + 1]
+  i32* memtab;     // [n * cap + 1]
+  i32* cnt;        // [n + 1]
+  i32* heavy;      // [n + 1]
+  i32* sadj;       // [m]
+  i32* swgt;       // [m]
+  i32* partial;    // [2 * grid] CTA sums of the grid scans
+  i32* misc;       // [kFzWords]
+  // per-level scalars and barrier (CoopState)
+  GridBarrier* bar;
+  i32* err;
+  i32* nc_out;
+  i32* mc_out;
+  i32* uf_rounds_out;
+  i32* maxdeg_out;
+  i32* max_cvw_out;
+  ArenaHdr* arena;
+  u32* arena_words;
+  u64 arena_cap;
+};
+
+template <int G>
+__device__ void fz_match(const FusedArgs& a) {
+  const i64 tot = (i64)a.n * G;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 base = (i64)blockIdx.x * blockDim.x; base < tot; base += stride) {   // block-uniform trip count
+    const i64 t = base + threadIdx.x;
+    const i32 v = (i32)(t / G);
+    const int sub = threadIdx.x & (G - 1);
+    u32 bw = 0, bd = kFull;
+    i32 bpos = INT_MAX, bu = -1;
+    bool skip = false;
+    if (v < a.n) {
+      const i32 beg = __ldg(a.xadj + v), end = __ldg(a.xadj + v + 1);
+      skip = a.split && end - beg > kMatchLong;   // uniform within the group
+      if (skip) {
+        if (sub == 0) a.longlist[atomicAdd(a.misc + kFzLong, 1)] = v;
+      } else {
+        for (i32 e = beg + sub; e < end; e += G) {
+          const u32 w = (u32)__ldg(a.adjwgt + e);
+          if (w == 0 || w < bw) continue;
+          const i32 u = __ldg(a.adjncy + e);
+          const u32 d = (u32)(__ldg(a.xadj + u + 1) - __ldg(a.xadj + u));
+          if (w > bw || d < bd) { bw = w; bd = d; bpos = e; bu = u; }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      const u32 ow = __shfl_xor_sync(kFull, bw, o, G);
+      const u32 od = __shfl_xor_sync(kFull, bd, o, G);
+      const i32 op = __shfl_xor_sync(kFull, bpos, o, G);
+      const i32 ou = __shfl_xor_sync(kFull, bu, o, G);
+      if (match_better(ow, od, op, bw, bd, bpos)) { bw = ow; bd = od; bpos = op; bu = ou; }
+    }
+    if (v < a.n && sub == 0 && !skip) a.cand[v] = bw > 0 ? bu : v;
+  }
+}
+
+// Long rows listed by fz_match: one CTA per row, as k_match_long (the rule's
+// order is total, so the thread count does not change the pick).
+__device__ void fz_match_long(const FusedArgs& a) {
+  __shared__ u32 s_w[kFusedWarps], s_d[kFusedWarps];
+  __shared__ i32 s_p[kFusedWarps], s_u[kFusedWarps];
+  const i32 nlong = ldcg(a.misc + kFzLong);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool vec = ((reinterpret_cast<uintptr_t>(a.adjncy) | reinterpret_cast<uintptr_t>(a.adjwgt)) & 15) == 0;
+  for (i32 r = blockIdx.x; r < nlong; r += gridDim.x) {
+    const i32 v = ldcg(a.longlist + r);
+    const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+    u32 bw = 0, bd = kFull;
+    i32 bpos = INT_MAX, bu = -1;
+    auto visit = [&](u32 w, i32 u, i32 e) {
+      if (w == 0 || w < bw) return;
+      const u32 d = (u32)(__ldg(a.xadj + u + 1) - __ldg(a.xadj + u));
+      if (match_better(w, d, e, bw, bd, bpos)) { bw = w; bd = d; bpos = e; bu = u; }
+    };
+    if (vec) {
+      i32 body = (beg + 3) & ~3;
+      i32 tail = body + ((end - body) & ~3);
+      if (tail < body) tail = body;
+      for (i32 e = beg + threadIdx.x; e < body && e < end; e += blockDim.x) visit((u32)a.adjwgt[e], a.adjncy[e], e);
+      for (i32 c = body / 4 + threadIdx.x; c < tail / 4; c += blockDim.x) {
+        const int4 w4 = __ldg(reinterpret_cast<const int4*>(a.adjwgt) + c);
+        const int4 u4 = __ldg(reinterpret_cast<const int4*>(a.adjncy) + c);
+        visit((u32)w4.x, u4.x, 4 * c);
+        visit((u32)w4.y, u4.y, 4 * c + 1);
+        visit((u32)w4.z, u4.z, 4 * c + 2);
+        visit((u32)w4.w, u4.w, 4 * c + 3);
+      }
+      for (i32 e = (tail > body ? tail : body) + threadIdx.x; e < end; e += blockDim.x)
+        visit((u32)a.adjwgt[e], a.adjncy[e], e);
+    } else {
+      for (i32 e = beg + threadIdx.x; e < end; e += blockDim.x) visit((u32)a.adjwgt[e], a.adjncy[e], e);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const u32 ow = __shfl_xor_sync(kFull, bw, o);
+      const u32 od = __shfl_xor_sync(kFull, bd, o);
+      const i32 op = __shfl_xor_sync(kFull, bpos, o);
+      const i32 ou = __shfl_xor_sync(kFull, bu, o);
+      if (match_better(ow, od, op, bw, bd, bpos)) { bw = ow; bd = od; bpos = op; bu = ou; }
+    }
+    if (lane == 0) {
+      s_w[wid] = bw;
+      s_d[wid] = bd;
+      s_p[wid] = bpos;
+      s_u[wid] = bu;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < kFusedWarps; ++w)
+        if (match_better(s_w[w], s_d[w], s_p[w], bw, bd, bpos)) { bw = s_w[w]; bd = s_d[w]; bpos = s_p[w]; bu = s_u[w]; }
+      a.cand[v] = bw > 0 ? bu : v;
+    }
+    __syncthreads();
+  }
+}
+
+// Block-wide exclusive scan of two i32 per thread; the block totals in tx, ty.
+__device__ __forceinline__ void fz_block_exscan2(i32& x, i32& y, i32* s_warp, i32& tx, i32& ty) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  i32 ix = x, iy = y;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const i32 px = __shfl_up_sync(kFull, ix, o), py = __shfl_up_sync(kFull, iy, o);
+    if (lane >= o) { ix += px; iy += py; }
+  }
+  if (lane == 31) { s_warp[wid] = ix; s_warp[32 + wid] = iy; }
+  __syncthreads();
+  if (wid == 0) {
+    const i32 wx = lane < kFusedWarps ? s_warp[lane] : 0, wy = lane < kFusedWarps ? s_warp[32 + lane] : 0;
+    i32 sx = wx, sy = wy;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const i32 px = __shfl_up_sync(kFull, sx, o), py = __shfl_up_sync(kFull, sy, o);
+      if (lane >= o) { sx += px; sy += py; }
+    }
+    if (lane < kFusedWarps) { s_warp[lane] = sx - wx; s_warp[32 + lane] = sy - wy; }
+    if (lane == kFusedWarps - 1) { s_warp[64] = sx; s_warp[65] = sy; }
+  }
+  __syncthreads();
+  x = ix - x + s_warp[wid];
+  y = iy - y + s_warp[32 + wid];
+  tx = s_warp[64];
+  ty = s_warp[65];
+  __syncthreads();
+}
+
+// Grid-wide exclusive scan of two sequences of N items inside the launch.
+// CTA b owns the contiguous range [b*span, (b+1)*span): pass 1 sums it, a
+// grid barrier publishes the CTA sums, pass 2 scans the range starting from
+// the sum of the lower CTAs.  item(i) -> (x, y); out(i, ex, ey) stores.  The
+// last CTA stores the totals through tot(tx, ty).  Integer sums: the result
+// equals a sequential exclusive scan.  Returns false if the barrier failed.
+template <class Item, class Out, class Tot>
+__device__ bool fz_grid_scan2(const FusedArgs& a, i64 N, Item item, Out out, Tot tot, i32* s_flag) {
+  __shared__ i32 s_warp[66];
+  __shared__ i32 s_pre[2];
+  const i64 span = (N + gridDim.x - 1) / gridDim.x;
+  const i64 lo = (i64)blockIdx.x * span, hi = lo + span < N ? lo + span : N;
+  i32 sx = 0, sy = 0;
+  for (i64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    i32 x, y;
+    item(i, x, y);
+    sx += x;
+    sy += y;
+  }
+  i32 tx, ty;
+  fz_block_exscan2(sx, sy, s_warp, tx, ty);
+  if (threadIdx.x == 0) {
+    a.partial[2 * blockIdx.x] = tx;
+    a.partial[2 * blockIdx.x + 1] = ty;
+  }
+  if (!grid_barrier(a.bar, a.err, s_flag)) return false;
+  if (threadIdx.x < 32) {
+    i32 px = 0, py = 0;
+    for (i32 b = threadIdx.x; b < (i32)blockIdx.x; b += 32) {
+      px += ldcg(a.partial + 2 * b);
+      py += ldcg(a.partial + 2 * b + 1);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      px += __shfl_xor_sync(kFull, px, o);
+      py += __shfl_xor_sync(kFull, py, o);
+    }
+    if (threadIdx.x == 0) { s_pre[0] = px; s_pre[1] = py; }
+  }
+  __syncthreads();
+  i32 cx = s_pre[0], cy = s_pre[1];
+  for (i64 b0 = lo; b0 < hi; b0 += blockDim.x) {   // block-uniform trip count
+    const i64 i = b0 + threadIdx.x;
+    i32 x = 0, y = 0;
+    if (i < hi) item(i, x, y);
+    i32 ex = x, ey = y, bx, by;
+    fz_block_exscan2(ex, ey, s_warp, bx, by);
+    if (i < hi) out(i, cx + ex, cy + ey);
+    cx += bx;
+    cy += by;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) tot(cx, cy);
+  return true;
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 2) k_coarsen_fused(FusedArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ i32 s_flag, s_any, s_count;
+  __shared__ u64 s_off;
+  const i32 n = a.n;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+
+  // ---- clear and initialise (the per-phase path's memsets) ----
+  for (i64 v = t0; v <= n; v += stride) {
+    if (v < n) {
+      const u64 key = (u64)(u32)v << 32;
+      a.k0[v] = key;
+      a.k1[v] = key;
+      a.gsize[v] = 0;
+      a.gcur[v] = 0;
+      a.cvwgt[v] = 0;
+    }
+    a.rowlen[v] = 0;
+    a.mcnt[v] = 0;
+    a.cnt[v] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.chg[0] = 0;
+    a.chg[1] = 0;
+    a.chg[2] = 0;
+    a.arena->used = 0;
+    a.arena->need = 0;
+    a.arena->overflow = 0;
+    *a.maxdeg_out = 0;
+    *a.max_cvw_out = 0;
+  }
+  // ---- heavy-edge candidates (coarsen.hpp:39-78) ----
+  switch (a.lanes) {
+    case 4: fz_match<4>(a); break;
+    case 8: fz_match<8>(a); break;
+    case 16: fz_match<16>(a); break;
+    default: fz_match<32>(a); break;
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  if (a.split) {
+    fz_match_long(a);
+    if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  }
+
+  // ---- union-find rounds (coarsen.hpp:80-118, 461-469), as k_uf_persist ----
+  {
+    i32 rounds = -1;
+    for (i32 it = 1;; ++it) {
+      if (it > a.max_rounds) {   // uniform across CTAs
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 2);
+        return;
+      }
+      const u64* src = (it & 1) ? a.k0 : a.k1;   // round it reads buffer (it-1)&1, raises it&1
+      u64* dst = (it & 1) ? a.k1 : a.k0;
+      if (threadIdx.x == 0) s_any = 0;
+      __syncthreads();
+      bool diff = false;
+      for (i64 v = t0; v < n; v += stride) {
+        const i32 c = ldcg(a.cand + v);
+        const u64 kv = ldcg(src + v);
+        const u64 kc = ldcg(src + c);
+        const u32 x = (u32)(kv >> 32), y = (u32)(kc >> 32);
+        atomicMax((unsigned long long*)&dst[v], (unsigned long long)kv);
+        if (x > y) {
+          atomicMax((unsigned long long*)&dst[c], (unsigned long long)(((u64)x << 32) | (u32)it));
+          diff = true;
+        } else if (x < y) {
+          atomicMax((unsigned long long*)&dst[v], (unsigned long long)(((u64)y << 32) | (u32)it));
+          diff = true;
+        }
+      }
+      if (diff) s_any = 1;
+      __syncthreads();
+      if (threadIdx.x == 0 && s_any) atomicOr(&a.chg[it % 3], 1);
+      if (blockIdx.x == 0 && threadIdx.x == 0) a.chg[(it + 1) % 3] = 0;
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      if (ldcg(&a.chg[it % 3]) == 0) {
+        rounds = it;
+        break;
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.uf_rounds_out = rounds;
+  }
+  const u64* keys = a.k0;   // both buffers hold the fixed point
+
+  // ---- group sizes (coarsen.hpp:351-359) ----
+  for (i64 v = t0; v < n; v += stride) atomicAdd(&a.gsize[(u32)(ldcg(keys + v) >> 32)], 1);
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  // ---- coarse ids: ceil(size/cap) per root, scanned; member offsets of big groups ----
+  {
+    const i32 cap = a.cap;
+    auto item = [&](i64 i, i32& x, i32& y) {
+      const i32 s = ldcg(a.gsize + i);
+      x = (s + cap - 1) / cap;
+      y = s > cap ? s : 0;
+    };
+    auto out = [&](i64 i, i32 ex, i32 ey) {
+      a.cbase[i] = ex;
+      a.goff[i] = ey;
+    };
+    auto tot = [&](i32 tx, i32 ty) {
+      *a.nc_out = tx;
+      a.misc[kFzBig] = ty;
+    };
+    if (!fz_grid_scan2(a, n, item, out, tot, &s_flag)) return;
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  // ---- scatter: cmap of small groups, member lists of big ones (coarsen.hpp:361-421) ----
+  for (i64 v = t0; v < n; v += stride) {
+    const i32 r = (i32)(u32)(ldcg(keys + v) >> 32);
+    const i32 s = ldcg(a.gsize + r);
+    if (s <= a.cap) {
+      a.cmap[v] = ldcg(a.cbase + r);
+    } else {
+      const i32 slot = atomicAdd(&a.gcur[r], 1);
+      a.members[ldcg(a.goff + r) + slot] = (i32)v;
+      if (r == (i32)v) {
+        if (s <= 32) a.wlist[atomicAdd(a.misc + kFzWarpG, 1)] = r;
+        else if (s <= kGroupSmem) a.clist[atomicAdd(a.misc + kFzCtaG, 1)] = r;
+        else a.glist[atomicAdd(a.misc + kFzGiant, 1)] = r;
+      }
+    }
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  // ---- big groups ordered by (dist, id): warps, CTAs, and rare giant groups ----
+  {
+    const i32 nwg = ldcg(a.misc + kFzWarpG);
+    const i64 warp0 = t0 >> 5, nwarps = stride >> 5;
+    for (i64 w = warp0; w < nwg; w += nwarps) {
+      const i32 r = ldcg(a.wlist + w);
+      const i32 s = ldcg(a.gsize + r);
+      u64 key = ~0ull;
+      if (lane < s) {
+        const i32 mb = ldcg(a.members + ldcg(a.goff + r) + lane);
+        key = ((ldcg(keys + mb) & 0xffffffffull) << 32) | (u32)mb;   // (dist, id)
+      }
+#pragma unroll
+      for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+          const u64 o = __shfl_xor_sync(kFull, key, j);
+          const bool up = (lane & kk) == 0;
+          const bool lower = (lane & j) == 0;
+          key = (lower == up) ? umin64(key, o) : umax64(key, o);
+        }
+      }
+      if (lane < s) a.cmap[(u32)key] = ldcg(a.cbase + r) + lane / a.cap;
+    }
+    const i32 ncg = ldcg(a.misc + kFzCtaG);
+    u64* sk = reinterpret_cast<u64*>(smem_raw);
+    for (i32 b = blockIdx.x; b < ncg; b += gridDim.x) {
+      const i32 r = ldcg(a.clist + b);
+      const i32 s = ldcg(a.gsize + r);
+      i32 P = 64;
+      while (P < s) P <<= 1;
+      for (i32 i = threadIdx.x; i < P; i += blockDim.x) {
+        u64 key = ~0ull;
+        if (i < s) {
+          const i32 mb = ldcg(a.members + ldcg(a.goff + r) + i);
+          key = ((ldcg(keys + mb) & 0xffffffffull) << 32) | (u32)mb;
+        }
+        sk[i] = key;
+      }
+      __syncthreads();
+      cta_bitonic_u64(sk, P);
+      const i32 cb = ldcg(a.cbase + r);
+      for (i32 i = threadIdx.x; i < s; i += blockDim.x) a.cmap[(u32)sk[i]] = cb + i / a.cap;
+      __syncthreads();
+    }
+    const i32 ng = ldcg(a.misc + kFzGiant);   // the same on every CTA
+    for (i32 gi = 0; gi < ng; ++gi) {
+      const i32 r = ldcg(a.glist + gi);
+      const i32 s = ldcg(a.gsize + r);
+      i64 P = 1;
+      while (P < s) P <<= 1;
+      const i32 mo = ldcg(a.goff + r);
+      u64* g = a.gscratch;
+      for (i64 i = t0; i < P; i += stride) {
+        u64 key = ~0ull;
+        if (i < s) {
+          const i32 mb = ldcg(a.members + mo + i);
+          key = ((ldcg(keys + mb) & 0xffffffffull) << 32) | (u32)mb;
+        }
+        g[i] = key;
+      }
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      for (i64 kk = 2; kk <= P; kk <<= 1) {
+        for (i64 j = kk >> 1; j > 0; j >>= 1) {
+          for (i64 i = t0; i < P; i += stride) {
+            const i64 l = i ^ j;
+            if (l > i) {
+              const u64 x = ldcg(g + i), y = ldcg(g + l);
+              const bool up = (i & kk) == 0;
+              if (up ? (x > y) : (x < y)) { g[i] = y; g[l] = x; }
+            }
+          }
+          if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        }
+      }
+      const i32 cb = ldcg(a.cbase + r);
+      for (i64 i = t0; i < s; i += stride) a.cmap[(u32)ldcg(g + i)] = cb + (i32)(i / a.cap);
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    }
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+
+  // ---- contraction (coarsen.hpp:157-349) ----
+  const i32 cap = a.cap;
+  for (i64 v = t0; v < n; v += stride) {   // coarse weights, row lengths, member lists
+    const i32 c = ldcg(a.cmap + v);
+    atomicAdd((u32*)&a.cvwgt[c], (u32)a.vwgt[v]);
+    atomicAdd(&a.rowlen[c], a.xadj[v + 1] - a.xadj[v]);
+    const i32 slot = atomicAdd(&a.mcnt[c], 1);
+    a.memtab[(i64)c * cap + slot] = (i32)v;
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  {   // upper-bound row offsets: exclusive scan of the row lengths (n + 1 entries)
+    auto item = [&](i64 i, i32& x, i32& y) {
+      x = ldcg(a.rowlen + i);
+      y = 0;
+    };
+    auto out = [&](i64 i, i32 ex, i32) { a.ub[i] = ex; };
+    auto tot = [&](i32 tx, i32) { a.misc[kFzUb] = tx; };
+    if (!fz_grid_scan2(a, (i64)n + 1, item, out, tot, &s_flag)) return;
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  const i32 nc = ldcg(a.nc_out);
+  {   // one warp per coarse vertex, as k_contract_warp<128, 8>
+    WarpTable<kFusedWcap>& T = reinterpret_cast<WarpTable<kFusedWcap>*>(smem_raw)[wid];
+    const i64 nw = (i64)gridDim.x * kFusedWarps;
+    for (i64 c = (i64)blockIdx.x * kFusedWarps + wid; c < nc; c += nw) {
+      const i32 L = ldcg(a.rowlen + c);
+      const i32 nm = ldcg(a.mcnt + c);
+      if (L > kFusedWcap || nm > 32) {
+        if (lane == 0) a.heavy[atomicAdd(a.misc + kFzHeavy, 1)] = (i32)c;
+        continue;
+      }
+      i32 mbeg = 0, mlen = 0;
+      if (lane < nm) {
+        const i32 v = ldcg(a.memtab + c * (i64)cap + lane);
+        mbeg = a.xadj[v];
+        mlen = a.xadj[v + 1] - mbeg;
+      }
+      i32 moff = mlen;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const i32 y = __shfl_up_sync(kFull, moff, o);
+        if (lane >= o) moff += y;
+      }
+      moff -= mlen;
+      auto entry_pos = [&](i32 i) {
+        i32 pos = -1;
+        for (i32 jm = 0; jm < nm; ++jm) {
+          const i32 oj = __shfl_sync(kFull, moff, jm);
+          const i32 lj = __shfl_sync(kFull, mlen, jm);
+          const i32 bj = __shfl_sync(kFull, mbeg, jm);
+          if (i >= oj && i < oj + lj) pos = bj + (i - oj);
+        }
+        return pos;
+      };
+      const i32 o = ldcg(a.ub + c);
+      if (L <= 32) {
+        u64 kv = ~0ull;
+        const i32 pos = entry_pos(lane);
+        if (lane < L) {
+          const u32 key = (u32)ldcg(a.cmap + a.adjncy[pos]);
+          if (key != (u32)c) kv = ((u64)key << 32) | (u32)a.adjwgt[pos];
+        }
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+          for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+            const u64 ot = __shfl_xor_sync(kFull, kv, jj);
+            const bool up = (lane & kk) == 0;
+            const bool lower = (lane & jj) == 0;
+            kv = (lower == up) ? umin64(kv, ot) : umax64(kv, ot);
+          }
+        }
+        const u32 key = (u32)(kv >> 32);
+        const u32 w = (u32)kv;
+        const u32 kprev = __shfl_up_sync(kFull, key, 1);
+        const u32 knext = __shfl_down_sync(kFull, key, 1);
+        const bool head = lane == 0 || kprev != key;
+        const bool last = lane == 31 || knext != key;
+        u32 S = w;
+        i32 start = head ? lane : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const u32 y = __shfl_up_sync(kFull, S, d);
+          const i32 z = __shfl_up_sync(kFull, start, d);
+          if (lane >= d) {
+            S += y;
+            start = start > z ? start : z;
+          }
+        }
+        const u32 before = __shfl_sync(kFull, S, start > 0 ? start - 1 : 0);
+        const u32 total = S - (start > 0 ? before : 0u);
+        const bool valid = last && key != 0xffffffffu;
+        const u32 bal = __ballot_sync(kFull, valid);
+        if (valid) {
+          const i32 at = o + __popc(bal & ((1u << lane) - 1));
+          a.sadj[at] = (i32)key;
+          a.swgt[at] = (i32)total;
+        }
+        if (lane == 0) a.cnt[c] = __popc(bal);
+        continue;
+      }
+      u32 hsz = 64;
+      while (hsz < 2u * (u32)L) hsz <<= 1;
+      for (u32 i = lane; i < hsz; i += 32) { T.keys[i] = kEmpty; T.vals[i] = 0; }
+      __syncwarp();
+      for (i32 b = 0; b < L; b += 32) {
+        const i32 i = b + lane;
+        const i32 pos = entry_pos(i);
+        if (i < L) {
+          const u32 key = (u32)ldcg(a.cmap + a.adjncy[pos]);
+          if (key != (u32)c) table_add(T.keys, T.vals, hsz, key, (u32)a.adjwgt[pos]);
+        }
+      }
+      __syncwarp();
+      i32 U = 0;
+      for (u32 base = 0; base < hsz; base += 32) {
+        const u32 sl = base + lane;
+        const bool occ = T.keys[sl] != kEmpty;
+        const u32 bal = __ballot_sync(kFull, occ);
+        if (occ) {
+          const i32 at = U + __popc(bal & ((1u << lane) - 1));
+          T.out[at] = ((u64)T.keys[sl] << 32) | T.vals[sl];
+        }
+        U += __popc(bal);
+      }
+      __syncwarp();
+      if (U <= 32) {
+        u64 key = lane < U ? T.out[lane] : ~0ull;
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+          for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+            const u64 ot = __shfl_xor_sync(kFull, key, jj);
+            const bool up = (lane & kk) == 0;
+            const bool lower = (lane & jj) == 0;
+            key = (lower == up) ? umin64(key, ot) : umax64(key, ot);
+          }
+        }
+        if (lane < U) {
+          a.sadj[o + lane] = (i32)(u32)(key >> 32);
+          a.swgt[o + lane] = (i32)(u32)key;
+        }
+      } else {
+        i32 P = 64;
+        while (P < U) P <<= 1;
+        for (i32 i = U + lane; i < P; i += 32) T.out[i] = ~0ull;
+        __syncwarp();
+        warp_bitonic_u64(T.out, P, lane);
+        for (i32 i = lane; i < U; i += 32) {
+          const u64 kv = T.out[i];
+          a.sadj[o + i] = (i32)(u32)(kv >> 32);
+          a.swgt[o + i] = (i32)(u32)kv;
+        }
+      }
+      if (lane == 0) a.cnt[c] = U;
+      __syncwarp();
+    }
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  {   // heavy coarse rows, one CTA each: the shared table, or the arena beyond kFusedCtaCap
+    const i32 nh = ldcg(a.misc + kFzHeavy);
+    for (i32 b = blockIdx.x; b < nh; b += gridDim.x) {
+      const i32 c = ldcg(a.heavy + b);
+      const i32 L = ldcg(a.rowlen + c);
+      const bool global_table = L > kFusedCtaCap;
+      u32 hsz = 64;
+      while (hsz < 2u * (u32)L) hsz <<= 1;
+      u32 *tk, *tv;
+      u64* out;
+      if (global_table) {
+        const u64 words = 3ull * hsz;   // keys + vals + hsz/2 u64 outputs
+        if (threadIdx.x == 0) {
+          const u64 off = atomicAdd((unsigned long long*)&a.arena->used, (unsigned long long)words);
+          if (off + words > a.arena_cap) {
+            atomicAdd((unsigned long long*)&a.arena->need, (unsigned long long)words);
+            atomicExch(&a.arena->overflow, 1);
+            s_off = ~0ull;
+          } else {
+            s_off = off;
+          }
+        }
+        __syncthreads();
+        const u64 off = s_off;
+        __syncthreads();   // every thread has read s_off before thread 0 can set it for the next row
+        if (off == ~0ull) continue;   // block-uniform; the level is redone after the arena grows
+        tk = a.arena_words + off;
+        tv = tk + hsz;
+        out = reinterpret_cast<u64*>(tv + hsz);
+      } else {
+        tk = reinterpret_cast<u32*>(smem_raw);
+        tv = tk + 2 * kFusedCtaCap;
+        out = reinterpret_cast<u64*>(tv + 2 * kFusedCtaCap);
+      }
+      for (u32 i = threadIdx.x; i < hsz; i += blockDim.x) { tk[i] = kEmpty; tv[i] = 0; }
+      if (threadIdx.x == 0) s_count = 0;
+      __syncthreads();
+      const i32 nm = ldcg(a.mcnt + c);
+      for (i32 j = 0; j < nm; ++j) {
+        const i32 v = ldcg(a.memtab + c * (i64)cap + j);
+        const i32 beg = a.xadj[v], end = a.xadj[v + 1];
+        for (i32 e = beg + threadIdx.x; e < end; e += blockDim.x) {
+          const u32 key = (u32)ldcg(a.cmap + a.adjncy[e]);
+          if (key != (u32)c) table_add(tk, tv, hsz, key, (u32)a.adjwgt[e]);
+        }
+      }
+      __syncthreads();
+      for (u32 sl = threadIdx.x; sl < hsz; sl += blockDim.x) {
+        if (tk[sl] != kEmpty) {
+          const i32 pos = atomicAdd(&s_count, 1);
+          out[pos] = ((u64)tk[sl] << 32) | tv[sl];
+        }
+      }
+      __syncthreads();
+      const i32 U = s_count;
+      i32 P = 64;
+      while (P < U) P <<= 1;
+      for (i32 i = U + threadIdx.x; i < P; i += blockDim.x) out[i] = ~0ull;
+      __syncthreads();
+      cta_bitonic_u64(out, P);
+      const i32 o = ldcg(a.ub + c);
+      for (i32 i = threadIdx.x; i < U; i += blockDim.x) {
+        const u64 kv = out[i];
+        a.sadj[o + i] = (i32)(u32)(kv >> 32);
+        a.swgt[o + i] = (i32)(u32)kv;
+      }
+      if (threadIdx.x == 0) a.cnt[c] = U;
+      __syncthreads();
+    }
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  {   // coarse xadj: exclusive scan of the row counts (rows beyond n_c are empty)
+    auto item = [&](i64 i, i32& x, i32& y) {
+      x = ldcg(a.cnt + i);
+      y = 0;
+    };
+    auto out = [&](i64 i, i32 ex, i32) { a.cxadj[i] = ex; };
+    auto tot = [&](i32 tx, i32) { *a.mc_out = tx; };
+    if (!fz_grid_scan2(a, (i64)n + 1, item, out, tot, &s_flag)) return;
+  }
+  if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+  {   // compact the rows (one warp per 32 rows, as k_copy_rows); longest row, heaviest vertex
+    const i64 warp = t0 >> 5, nwarps = stride >> 5;
+    i32 mx = 0, mw = 0;
+    for (i64 c0 = warp * 32; c0 < nc; c0 += nwarps * 32) {
+      const i64 c = c0 + lane;
+      i32 src = 0, dst = 0, len = 0;
+      if (c < nc) {
+        src = ldcg(a.ub + c);
+        dst = ldcg(a.cxadj + c);
+        len = ldcg(a.cnt + c);
+        const i32 w = ldcg(a.cvwgt + c);
+        mw = w > mw ? w : mw;
+      }
+      mx = len > mx ? len : mx;
+      i32 inc = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const i32 y = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += y;
+      }
+      const i32 total = __shfl_sync(kFull, inc, 31);
+      const i32 exc = inc - len;
+      for (i32 base = 0; base < total; base += 32) {
+        const i32 idx = base + lane;
+        i32 r = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const i32 probe = __shfl_sync(kFull, inc, r + step - 1);
+          if (probe <= idx) r += step;
+        }
+        r = r < 31 ? r : 31;
+        const i32 rs = __shfl_sync(kFull, src, r), rd = __shfl_sync(kFull, dst, r), re = __shfl_sync(kFull, exc, r);
+        if (idx < total) {
+          a.cadjncy[rd + (idx - re)] = ldcg(a.sadj + rs + (idx - re));
+          a.cadjwgt[rd + (idx - re)] = ldcg(a.swgt + rs + (idx - re));
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const i32 y = __shfl_xor_sync(kFull, mx, o);
+      mx = mx > y ? mx : y;
+      const i32 z = __shfl_xor_sync(kFull, mw, o);
+      mw = mw > z ? mw : z;
+    }
+    if (lane == 0 && mx > 0) atomicMax(a.maxdeg_out, mx);
+    if (lane == 0 && mw > 0) atomicMax(a.max_cvw_out, mw);
+  }
+}
+
+static int fused_blocks_per_sm() {
+  static int bps = -1;   // the same on every device of the process (one B200 model)
+  if (bps < 0) {
+    int b = 0;
+    if (cudaFuncSetAttribute(k_coarsen_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_coarsen_fused, kFusedThreads, kFusedSmem) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      b = 0;
+    }
+    bps = b;
+  }
+  return bps;
+}
+
+// Whether a level runs as one fused launch: levels of at most the handle's
+// fused_max_n vertices whose rows are short on average (long coarse rows are
+// the per-phase path's wide warp tables), never while the tuner times the
+// match variants.
+static bool use_fused(Handle& h, const DevGraph& g) {
+  return !h.tune_collect && g.n > 0 && (i64)g.n <= (i64)h.tuning.coarsen_fused_max_n &&
+         (double)g.m <= 48.0 * (double)g.n && fused_blocks_per_sm() >= 1;
+}
+
+static void run_coarsen_fused(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
+  if (!h.capturing)   // per device (the occupancy probe set it on the first device only)
+    GKW_CUDA(cudaFuncSetAttribute(k_coarsen_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmem));
+  Pool::Mark mk = h.scratch.mark();
+  const i32 n = g.n;
+  const i64 nu = (i64)n + 1;
+  const i32 bps = fused_blocks_per_sm();
+  const i32 vpc = std::max(64, h.tuning.coarsen_verts_per_cta);
+  i32 grid = (i32)std::min<i64>((i64)h.sm_count * bps, std::max<i64>(1, ((i64)n + vpc - 1) / vpc));
+  grid = coop_grid(h, (const void*)k_coarsen_fused, grid, kFusedThreads, kFusedSmem);
+  FusedArgs a;
+  a.n = n;
+  a.m = g.m;
+  a.xadj = g.xadj;
+  a.adjncy = g.adjncy;
+  a.adjwgt = g.adjwgt;
+  a.vwgt = g.vwgt;
+  a.lanes = h.tuning.match_lanes[match_bucket(g)];
+  a.split = g.maxdeg < 0 || g.maxdeg > kMatchLong;
+  a.cap = cap;
+  a.max_rounds = n + 2;
+  a.cmap = out.cmap;
+  a.cxadj = out.cxadj;
+  a.cadjncy = out.cadjncy;
+  a.cadjwgt = out.cadjwgt;
+  a.cvwgt = out.cvwgt;
+  a.cand = h.scratch.alloc_n<i32>(n);
+  a.k0 = h.scratch.alloc_n<u64>(n);
+  a.k1 = h.scratch.alloc_n<u64>(n);
+  a.chg = h.scratch.alloc_n<i32>(4);
+  a.longlist = h.scratch.alloc_n<i32>(n);
+  a.gsize = h.scratch.alloc_n<i32>(n);
+  a.cbase = h.scratch.alloc_n<i32>(n);
+  a.goff = h.scratch.alloc_n<i32>(n);
+  a.gcur = h.scratch.alloc_n<i32>(n);
+  a.members = h.scratch.alloc_n<i32>(n);
+  a.wlist = h.scratch.alloc_n<i32>(n);
+  a.clist = h.scratch.alloc_n<i32>(n);
+  a.glist = h.scratch.alloc_n<i32>(n);
+  a.gscratch = h.scratch.alloc_n<u64>(2 * (size_t)n);
+  a.rowlen = h.scratch.alloc_n<i32>(nu);
+  a.ub = h.scratch.alloc_n<i32>(nu);
+  a.mcnt = h.scratch.alloc_n<i32>(nu);
+  a.memtab = h.scratch.alloc_n<i32>((i64)n * cap + 1);
+  a.cnt = h.scratch.alloc_n<i32>(nu);
+  a.heavy = h.scratch.alloc_n<i32>(nu);
+  a.sadj = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
+  a.swgt = h.scratch.alloc_n<i32>(std::max<i64>(g.m, 1));
+  a.partial = h.scratch.alloc_n<i32>(2 * (size_t)grid);
+  a.misc = h.scratch.alloc_n<i32>(kFzWords);
+  a.bar = &h.coop->bar;
+  a.err = &h.coop->err;
+  a.nc_out = &h.coop->nc;
+  a.mc_out = &h.coop->mc;
+  a.uf_rounds_out = &h.coop->uf_rounds;
+  a.maxdeg_out = &h.coop->maxdeg;
+  a.max_cvw_out = &h.coop->max_cvw;
+  a.arena = h.arena;
+  a.arena_words = reinterpret_cast<u32*>(h.arena + 1);
+  a.arena_cap = h.arena_words;
+  GKW_CUDA(cudaMemsetAsync(a.misc, 0, sizeof(i32) * kFzWords, h.stream));
+  void* args[] = {&a};
+  launch_coop(h, (const void*)k_coarsen_fused, grid, kFusedThreads, kFusedSmem, args);
+  h.scratch.release(mk);
+}
+
 // The key of one level's launch sequence in the handle's graph cache:
 // everything the launches depend on.
 static std::string level_key(const Handle& h, const DevGraph& g, i32 cap, const CoarsenOut& out) {
@@ -1079,8 +1932,14 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
       GKW_CHECK_LAUNCH();
     }
   };
-  if (tune) body();   // the tuner's timings synchronise: never captured
-  else graph_run(h, level_key(h, g, cap, out), body);
+  if (use_fused(h, g)) {
+    // one launch: no graph needed (a launch is as cheap as a graph of one)
+    run_coarsen_fused(h, g, cap, out);
+  } else if (tune) {
+    body();   // the tuner's timings synchronise: never captured
+  } else {
+    graph_run(h, level_key(h, g, cap, out), body);
+  }
   CoopState c = read_coop(h);
   if (c.arena_overflow) {   // very long coarse rows: grow the arena and redo the step
     ensure_arena(h, (u64)((double)(h.arena_words + (u64)c.arena_need) * 1.25) + 1024);

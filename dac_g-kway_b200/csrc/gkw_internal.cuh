@@ -201,7 +201,7 @@ struct Handle {
   // thread-block cluster (a server's small jobs; see launch_coop)
   bool narrow = false;
   cudaEvent_t coop_ev = nullptr;   // this handle's last wide cooperative launch
-  gkw_tuning tuning{{4, 8, 16, 32}, 512, 32};   // launch shapes (gkw_autotune)
+  gkw_tuning tuning{{4, 8, 16, 32}, 512, 32, 0, 256};   // launch shapes (gkw_autotune)
   // while the autotuner collects: per average-degree bucket, the summed time
   // of each match lane count (4, 8, 16, 32) over the levels met
   bool tune_collect = false;

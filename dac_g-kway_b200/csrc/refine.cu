@@ -1189,6 +1189,7 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
     }
   }
   __syncthreads();
+  trace_mark(a, 29);
   const i32 ne = s_ne;
   if (ne > kRiskEvents) return false;   // block-uniform
   {   // first grouped slot of each part: exclusive scan, two parts per thread
@@ -1226,6 +1227,7 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
     }
   }
   kmin = block_reduce_u64<false>(kmin, s_tmp);   // (its barriers publish the ranges)
+  trace_mark(a, 30);
   const i32 nbad = s_nbad;
   // the largest candidate key in no marked range
   u64 best = 0;
@@ -1312,8 +1314,10 @@ __device__ void ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* ke
         trace_mark(a, 27);
       }
     }
-    if (!done && cnt <= a.move_cap)
+    if (!done && cnt <= a.move_cap) {
+      trace_mark(a, 28);
       done = refine_threshold(a, cnt, s, greedy, keep, s_tmp, s_warp, &kstar, &napplied);
+    }
     trace_mark(a, 25);
     if (!done) {
       select_sort(a, a.cands, cnt, s, greedy);   // s[0..B) sorted (ends with a block barrier)

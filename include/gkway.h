@@ -118,11 +118,18 @@ gkw_status gkw_set_stream(gkw_handle* h, void* stream);
  *                        (b = 0..3; 4, 8, 16 or 32; rows above 512 entries
  *                        always go to one CTA each)
  *   level_verts_per_cta  level-kernel CTAs: one per this many vertices ...
- *   level_min_ctas       ... and at least this many (capped at 2 per SM) */
+ *   level_min_ctas       ... and at least this many (capped at 2 per SM)
+ *   coarsen_fused_max_n  coarsening levels of at most this many vertices run
+ *                        as one fused launch with grid barriers between the
+ *                        phases (default 0: every level as per-phase kernels)
+ *   coarsen_verts_per_cta  fused coarsening CTAs: one per this many vertices
+ *                        (capped at the co-resident CTAs; default 256) */
 typedef struct gkw_tuning {
   int32_t match_lanes[4];
   int32_t level_verts_per_cta;
   int32_t level_min_ctas;
+  int32_t coarsen_fused_max_n;
+  int32_t coarsen_verts_per_cta;
 } gkw_tuning;
 gkw_status gkw_get_tuning(gkw_handle* h, gkw_tuning* out);
 gkw_status gkw_set_tuning(gkw_handle* h, const gkw_tuning* t);

@@ -356,3 +356,27 @@ def test_graph_replay_matches_plain_launches(pkg, gen, orc):
             assert np.array_equal(p1.cpu().numpy(), ref) and c1 == info["cut"], step
     h.close()
     plain.close()
+
+
+def test_fused_coarsening_matches_per_phase(pkg, gen, cases):
+    """A coarsening level runs either as one fused launch (grid barriers
+    between the phases) or as the per-phase kernels; every level, the part
+    vector and the cut are the same for every launch shape of the fused one:
+    one CTA, a thread-block cluster, a wide cooperative grid."""
+    from graphs import weighted
+    graphs = list(cases) + [("circuit_60k_hubs", gen.circuit(60000, seed=3, levels=60, hub_max=2000)),
+                            ("delaunay_60k_w", weighted(gen, gen.delaunay(60000, 17), seed=3))]
+    per_phase = pkg.Handle(0)
+    per_phase.set_tuning(coarsen_fused_max_n=0)
+    fused = pkg.Handle(0)
+    for name, g in graphs:
+        for k in (8, 64):
+            p0, c0, s0 = per_phase.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k)
+            for vpc in (1 << 30, 4096, 64):   # one CTA; few CTAs (a cluster); wide
+                fused.set_tuning(coarsen_fused_max_n=1 << 30, coarsen_verts_per_cta=vpc)
+                p1, c1, s1 = fused.partition(g.xadj, g.adjncy, g.adjwgt, g.vwgt, k)
+                assert np.array_equal(p1, p0) and c1 == c0, (name, k, vpc)
+                assert s1["level_n"] == s0["level_n"] and s1["level_m"] == s0["level_m"], (name, k, vpc)
+                assert s1["refine_rounds"] == s0["refine_rounds"], (name, k, vpc)
+    per_phase.close()
+    fused.close()
