@@ -206,8 +206,9 @@ void run_match(Handle& h, const DevGraph& g, i32* cand, i64 maxdeg) {
 // round -- no host round trip per round.
 // ===========================================================================
 constexpr int kUfThreads = 512;
+constexpr int kUfIlp = 2;   // vertices per thread whose loads are issued together
 
-__global__ void __launch_bounds__(kUfThreads) k_uf_persist(i32 n, const i32* __restrict__ cand, u64* k0, u64* k1,
+__global__ void __launch_bounds__(kUfThreads, 3) k_uf_persist(i32 n, const i32* __restrict__ cand, u64* k0, u64* k1,
                                                           i32* chg, GridBarrier* bar, i32* err, i32* rounds_out,
                                                           i32 max_rounds) {
   __shared__ i32 s_flag, s_any;
@@ -224,30 +225,48 @@ __global__ void __launch_bounds__(kUfThreads) k_uf_persist(i32 n, const i32* __r
     chg[2] = 0;
   }
   if (!grid_barrier(bar, err, &s_flag)) return;
-  u64* buf[2] = {k0, k1};
   i32 rounds = -1;
   for (i32 it = 1;; ++it) {
     if (it > max_rounds) {   // uniform across CTAs
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(err, 2);
       return;
     }
-    const u64* src = buf[(it - 1) & 1];
-    u64* dst = buf[it & 1];
+    const u64* src = (it & 1) ? k0 : k1;   // round it reads buffer (it-1)&1, raises it&1
+    u64* dst = (it & 1) ? k1 : k0;
     if (threadIdx.x == 0) s_any = 0;
     __syncthreads();
     bool diff = false;
-    for (i64 v = t0; v < n; v += stride) {
-      const i32 c = cand[v];
-      const u64 kv = ldcg(src + v);
-      const u64 kc = ldcg(src + c);
-      const u32 a = (u32)(kv >> 32), b = (u32)(kc >> 32);
-      atomicMax((unsigned long long*)&dst[v], (unsigned long long)kv);
-      if (a > b) {
-        atomicMax((unsigned long long*)&dst[c], (unsigned long long)(((u64)a << 32) | (u32)it));
-        diff = true;
-      } else if (a < b) {
-        atomicMax((unsigned long long*)&dst[v], (unsigned long long)(((u64)b << 32) | (u32)it));
-        diff = true;
+    for (i64 v0 = t0; v0 < n; v0 += stride * kUfIlp) {
+      // kUfIlp vertices at a time: their candidate loads, then their key
+      // gathers, then the raises (one vertex's steps in the same order)
+      i32 c[kUfIlp];
+      u64 kv[kUfIlp], kc[kUfIlp];
+#pragma unroll
+      for (int q = 0; q < kUfIlp; ++q) {
+        const i64 v = v0 + q * stride;
+        c[q] = v < n ? cand[v] : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < kUfIlp; ++q) {
+        const i64 v = v0 + q * stride;
+        if (v < n) {
+          kv[q] = ldcg(src + v);
+          kc[q] = ldcg(src + c[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kUfIlp; ++q) {
+        const i64 v = v0 + q * stride;
+        if (v >= n) continue;
+        const u32 a = (u32)(kv[q] >> 32), b = (u32)(kc[q] >> 32);
+        atomicMax((unsigned long long*)&dst[v], (unsigned long long)kv[q]);
+        if (a > b) {
+          atomicMax((unsigned long long*)&dst[c[q]], (unsigned long long)(((u64)a << 32) | (u32)it));
+          diff = true;
+        } else if (a < b) {
+          atomicMax((unsigned long long*)&dst[v], (unsigned long long)(((u64)b << 32) | (u32)it));
+          diff = true;
+        }
       }
     }
     if (diff) s_any = 1;
@@ -282,7 +301,7 @@ void run_union_find(Handle& h, i32 n, const i32* cand, u64* keys_out, i32* d_rou
   static int bps = 0;   // the same on every device of the process (one B200 model)
   if (!bps) GKW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_uf_persist, kUfThreads, 0));
   GKW_REQUIRE(bps >= 1, GKW_E_INTERNAL, "union-find kernel does not fit on an SM");
-  i32 grid = std::min<i32>(h.sm_count * std::min(bps, 2), (i32)ceil_div(n, kUfThreads));
+  i32 grid = std::min<i32>(h.sm_count * std::min(bps, 4), (i32)ceil_div(n, kUfThreads));
   grid = coop_grid(h, (const void*)k_uf_persist, grid, kUfThreads, 0);
   i32 max_rounds = n + 2;
   GridBarrier* barp = &h.coop->bar;

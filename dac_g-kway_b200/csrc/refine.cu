@@ -60,7 +60,6 @@ struct RoundState {
   u64 rows;   // adjacency entries read by the gain updates of the rounds
   i64 cand_sum;   // refinement candidates over the rounds (diagnostic)
   i32 needcheck;  // some part could exceed MAXW if every candidate moved (plain levels)
-  i32 nrisk;      // parts flagged in risk this round
 };
 
 
@@ -91,9 +90,10 @@ struct RefineCtx {
   u32* pwd = nullptr;    // part-weight changes of a round's moves, folded into pw by the gain update
   u32* pin = nullptr;    // weight the round's candidates would bring into each part
   i32* msrc = nullptr;   // source part of each candidate, taken before any move is applied
-  u32* risk = nullptr;   // per part: 1 + its index among the round's at-risk parts, 0 if not at risk
-  i32* riskpart = nullptr;   // the at-risk parts by index
-  i32* pnet = nullptr;       // net weight change of each part if every candidate moved
+  u64* cinfo = nullptr;  // per candidate list entry: source part << 32 | destination part
+  i32* cw = nullptr;     // per candidate list entry: vertex weight
+  u32* risk = nullptr;   // per part: 1 if the round's candidates could push it over MAXW
+  i32* pnet = nullptr;   // net weight change of each part if every candidate moved
   RoundState* st = nullptr;
   u32* bmark = nullptr;
   i32* btarget = nullptr;
@@ -131,8 +131,9 @@ struct LevelArgs {
   u32* pwd;           // plain levels: refinement moves add their weight changes here
   u32* pin;           // plain levels: per-part inflow of the round's candidates
   i32* msrc;          // plain levels: source part of each candidate
-  u32* risk;          // plain levels: 1 + index among the round's at-risk parts, or 0
-  i32* riskpart;      // plain levels: the at-risk parts by index
+  u64* cinfo;         // plain levels: (source << 32 | destination) of candidate list entry i
+  i32* cw;            // plain levels: vertex weight of candidate list entry i
+  u32* risk;          // plain levels: 1 if the round's candidates could push the part over MAXW
   i32* pnet;          // plain levels: net weight change of each part over all candidates
   RoundState* st;
   u32* bmark;
@@ -143,6 +144,7 @@ struct LevelArgs {
   i32* err;
   LevelStatsDev* stat_slot;
   i32 acc_warps;
+  i32 upd_lanes;     // lanes per vertex of the first gain pass (8, 16, or 32: a warp)
   u64* trace;        // optional phase timeline: (phase id << 56) | globaltimer ns
   i32 trace_cap;
   i32* trace_n;
@@ -282,6 +284,7 @@ __device__ __forceinline__ void block_append32(bool pred, i32 val, i32* list, i3
 // U (or P) appends of one phase, staged per CTA in shared memory (one global
 // atomic per CTA); entries beyond the stage go to the list directly.
 constexpr i32 kUStage = 1024;
+static_assert(kLevelThreads <= kUStage, "the projection's U stage holds at least one chunk");
 struct UStage {
   i32 buf[kUStage];
   i32 cnt;
@@ -308,14 +311,16 @@ __device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
 // Projection (uncoarsen.hpp:325-356, expand_partition): part and boundary
 // inherited from the coarse vertex, gain 0, target = part, boundary vertices
 // flagged for the gain update.
-// U appends are aggregated per CTA (one global atomic per CTA and pass, not
-// one per warp: a million-vertex level would serialise 32k atomics on the
-// counter).
-__device__ void ph_project(const LevelArgs& a, i32* s_cnt, i32* s_base) {
+// U appends are staged per CTA in shared memory and flushed with one global
+// atomic per half-full stage (a million-vertex level would otherwise
+// serialise tens of thousands of atomics on the counter), with one block
+// barrier per chunk of vertices.
+__device__ void ph_project(const LevelArgs& a, UStage& S) {
+  if (threadIdx.x == 0) S.cnt = 0;
+  __syncthreads();
   const i64 stride = (i64)gridDim.x * blockDim.x;
   for (i64 b0 = (i64)blockIdx.x * blockDim.x; b0 < a.n; b0 += stride) {   // block-uniform trip count
     const i64 v = b0 + threadIdx.x;
-    bool b = false;
     if (v < a.n) {
       const i32 c = a.cmap[v];
       i32 p, bc;
@@ -333,11 +338,21 @@ __device__ void ph_project(const LevelArgs& a, i32* s_cnt, i32* s_base) {
       a.gain[v] = 0;
       a.target[v] = p;
       a.inP[v] = 0;
-      b = bc != 0 && !enter && (!a.batch || __ldg(a.gflags + __ldg(a.gid + v)) != 0);
+      const bool b = bc != 0 && !enter && (!a.batch || __ldg(a.gflags + __ldg(a.gid + v)) != 0);
       a.updflag[v] = b ? 1 : 0;
+      if (b) S.buf[atomicAdd(&S.cnt, 1)] = (i32)v;   // room: flushed below once half full
     }
-    block_append32(b, (i32)v, a.U, &a.st->ucount, s_cnt, s_base);
+    __syncthreads();
+    if (S.cnt > kUStage - (i32)blockDim.x) {   // block-uniform
+      if (threadIdx.x == 0) S.base = atomicAdd(&a.st->ucount, S.cnt);
+      __syncthreads();
+      for (i32 t = threadIdx.x; t < S.cnt; t += blockDim.x) a.U[S.base + t] = S.buf[t];
+      __syncthreads();
+      if (threadIdx.x == 0) S.cnt = 0;
+      __syncthreads();
+    }
   }
+  ustage_flush(S, a.U, &a.st->ucount);
 }
 
 // U from the caller's flags, P from the current gains (per-phase entry points).
@@ -380,6 +395,7 @@ __device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, USt
   for (i64 i = (i64)blockIdx.x * a.acc_warps + wid; i < nU; i += nw) {
     const i32 v = ldc(a.U + i);
     const i32 p = ldc(a.part + v);
+    const i32 wasP = ldc(a.inP + v);   // U holds v once: no other warp writes inP[v] in this phase
     const i32 pb = part_base_of(a, v);   // rows are indexed by the graph's own part ids
     u32* accb = acc - pb;
     const i32 beg = a.xadj[v], end = a.xadj[v + 1];
@@ -417,7 +433,10 @@ __device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, USt
         a.bnd[v] = b ? 1 : 0;
         a.gain[v] = (i32)g;
         a.target[v] = (i32)q_best;
-        if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) ustage_push(S, v, Pout, pcount);
+        if ((i32)g > 0 && !wasP) {
+          a.inP[v] = 1;
+          ustage_push(S, v, Pout, pcount);
+        }
       }
       __syncwarp();
       if (h0) accb[q0] = 0;
@@ -456,7 +475,10 @@ __device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, USt
       a.bnd[v] = b ? 1 : 0;
       a.gain[v] = (i32)g;
       a.target[v] = (i32)q_best;
-      if ((i32)g > 0 && atomicExch(&a.inP[v], 1) == 0) ustage_push(S, v, Pout, pcount);
+      if ((i32)g > 0 && !wasP) {
+        a.inP[v] = 1;
+        ustage_push(S, v, Pout, pcount);
+      }
     }
     __syncwarp();
     for (i32 e = beg + lane; e < end; e += 32) accb[ldc(a.part + a.adjncy[e])] = 0;
@@ -475,6 +497,106 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count, UStage& 
   __syncthreads();
 }
 
+// The first gain pass of a level (every boundary vertex of U) on a graph of
+// short rows: G lanes per vertex instead of a warp, so 32/G vertices' load
+// chains run at once in each warp -- the same rule as ph_update_rows per
+// vertex.  Each group's connection row (kacc words) lies in `rows`, the
+// level kernel's sort and greedy buffers (free during an update phase); the
+// rows are zeroed here and every vertex clears the entries it touched.
+template <int G>
+__device__ void ph_update_first_groups(const LevelArgs& a, u32* rows, UStage& S) {
+  constexpr int kGpw = 32 / G;   // groups per warp
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int sub = lane & (G - 1), grp = lane / G;
+  const u32 gmask = (G == 32 ? kFullMask : ((1u << G) - 1u)) << (grp * G);
+  const i32 ngrp = (i32)(blockDim.x / G);
+  for (i32 q = threadIdx.x; q < ngrp * a.kacc; q += blockDim.x) rows[q] = 0;
+  if (threadIdx.x == 0) S.cnt = 0;
+  __syncthreads();
+  u32* acc = rows + (size_t)(wid * kGpw + grp) * a.kacc;
+  RoundState* st = a.st;
+  const i32 nU = ldc(&st->ucount);
+  i32* Pout = a.P0;
+  i32* pcount = &st->pcount[0];
+  const i64 step = (i64)gridDim.x * ngrp;
+  // warp-uniform trip count: a warp's groups take vertices base .. base + kGpw - 1
+  for (i64 base = ((i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / G; base < nU; base += step) {
+    const i64 i = base + grp;
+    const bool act = i < nU;
+    i32 v = 0, p = 0, wasP = 1, beg = 0, end = 0;
+    if (act) {
+      v = ldc(a.U + i);
+      p = ldc(a.part + v);
+      wasP = ldc(a.inP + v);
+      beg = a.xadj[v];
+      end = a.xadj[v + 1];
+    }
+    u32* accb = acc - (act ? part_base_of(a, v) : 0);   // rows are indexed by the graph's own part ids
+    // entries sub and sub + G keep their part ids in registers; longer rows reload
+    const i32 e0 = beg + sub, e1 = e0 + G;
+    const bool h0 = e0 < end, h1 = e1 < end;
+    const i32 q0 = h0 ? ldc(a.part + a.adjncy[e0]) : p, q1 = h1 ? ldc(a.part + a.adjncy[e1]) : p;
+    bool bl = q0 != p || q1 != p;
+    if (h0) atomicAdd(&accb[q0], (u32)a.adjwgt[e0]);
+    if (h1) atomicAdd(&accb[q1], (u32)a.adjwgt[e1]);
+    for (i32 e = e1 + G; e < end; e += G) {
+      const i32 q = ldc(a.part + a.adjncy[e]);
+      atomicAdd(&accb[q], (u32)a.adjwgt[e]);
+      bl |= q != p;
+    }
+    const bool b = (__ballot_sync(kFullMask, bl) & gmask) != 0;
+    __syncwarp();
+    u64 best = 0;
+    if (b) {
+      const u32 id = accb[p];
+      if (q0 != p) best = ((u64)(accb[q0] - id) << 32) | (u32)(~(u32)q0);
+      if (q1 != p) {
+        const u64 key = ((u64)(accb[q1] - id) << 32) | (u32)(~(u32)q1);
+        best = best > key ? best : key;
+      }
+      for (i32 e = e1 + G; e < end; e += G) {
+        const i32 q = ldc(a.part + a.adjncy[e]);
+        if (q != p) {
+          const u64 key = ((u64)(accb[q] - id) << 32) | (u32)(~(u32)q);
+          best = best > key ? best : key;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      const u64 ot = __shfl_xor_sync(kFullMask, best, o, G);
+      best = best > ot ? best : ot;
+    }
+    if (act && sub == 0) {
+      u32 g = 0, q_best = (u32)p;
+      const u32 gb = (u32)(best >> 32);
+      if (b && gb > 0) { g = gb; q_best = ~(u32)best; }
+      a.updflag[v] = 0;
+      a.bnd[v] = b ? 1 : 0;
+      a.gain[v] = (i32)g;
+      a.target[v] = (i32)q_best;
+      if ((i32)g > 0 && !wasP) {
+        a.inP[v] = 1;
+        ustage_push(S, v, Pout, pcount);
+      }
+    }
+    __syncwarp();
+    if (h0) accb[q0] = 0;
+    if (h1) accb[q1] = 0;
+    for (i32 e = e1 + G; e < end; e += G) accb[ldc(a.part + a.adjncy[e])] = 0;
+    __syncwarp();
+  }
+  ustage_flush(S, a.P0, &a.st->pcount[0]);
+  __syncthreads();
+}
+
+// The first gain pass: groups of upd_lanes lanes per vertex, or a warp.
+__device__ void ph_update_first(const LevelArgs& a, u32* acc_all, u32* rows, UStage& S) {
+  if (a.upd_lanes == 8) ph_update_first_groups<8>(a, rows, S);
+  else if (a.upd_lanes == 16) ph_update_first_groups<16>(a, rows, S);
+  else ph_update(a, acc_all, false, S);
+}
+
 
 // Move candidates (uncoarsen.hpp:111-173, create_independent_move_buffer):
 // boundary, gain > 0, a valid destination by weight, and no neighbour with a
@@ -484,13 +606,22 @@ __device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count, UStage& 
 // MAXW even with every candidate moved in, every prefix of the sorted moves
 // is balanced and the select phase needs neither the sort nor the check;
 // otherwise the parts that could pass it are flagged in risk.
-__device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
+__device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base, u32* s_pwc) {
   RoundState* st = a.st;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (a.batch) *a.mcount = 0;   // the round's moves
     else st->ucount = 0;          // U was consumed by the last gain update
   }
   const int lane = threadIdx.x & 31;
+  // plain levels: the part weights (no move changes them during this phase)
+  // in shared memory, which takes two dependent global loads off each
+  // candidate's chain
+  const bool pwc = !a.batch && a.k <= kGreedyWords;   // block-uniform
+  if (pwc) {
+    for (i32 q = threadIdx.x; q < a.k; q += blockDim.x) s_pwc[q] = ldc(a.pw + q);
+    __syncthreads();
+  }
+  auto pw_of = [&](i32 q) -> u32 { return pwc ? s_pwc[q] : ldc(a.pw + q); };
   const i32 nP = ldc(&st->pcount[0]);
   // entry r*32*W + lane*W + w goes to warp w, lane `lane`: the entries of a
   // round spread over all warps, so each warp checks at most a few of them
@@ -511,7 +642,7 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
       xe = a.xadj[v + 1];
       if (!a.batch) p = ldc(a.part + v);
       if (g > 0 && bv && graph_flag(a, v, 0)) {   // batched: graphs that refine here
-        pwt = ldc(a.pw + t);
+        pwt = pw_of(t);
         check = valid_move(pwt, vw, maxw_of(a, t));
       }
     }
@@ -529,7 +660,7 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
         if (u < cv) {
           const i32 gu = ldc(a.gain + u), tu = ldc(a.target + u);   // issued together
           const u32 vu = (u32)a.vwgt[u];
-          if (gu > 0) blocked = valid_move(ldc(a.pw + tu), vu, maxw_of(a, tu));
+          if (gu > 0) blocked = valid_move(pw_of(tu), vu, maxw_of(a, tu));
         }
       }
       const bool any_blocked = __any_sync(kFullMask, blocked);
@@ -548,19 +679,28 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base) {
         atomicAdd(a.pnet + t, (i32)vw);
         atomicSub(a.pnet + p, (i32)vw);
       }
-      block_append64(cand, move_key(g, v), a.cands, &st->ccount, s_cnt, s_base);
+      // CTA-aggregated append of the key with its source, destination and
+      // weight (the balance check reads those by list position)
+      if (threadIdx.x == 0) *s_cnt = 0;
+      __syncthreads();
+      const i32 local = cand ? atomicAdd(s_cnt, 1) : -1;
+      __syncthreads();
+      if (threadIdx.x == 0 && *s_cnt) *s_base = atomicAdd(&st->ccount, *s_cnt);
+      __syncthreads();
+      if (cand) {
+        const i32 at = *s_base + local;
+        a.cands[at] = move_key(g, v);
+        a.cinfo[at] = ((u64)(u32)p << 32) | (u32)t;
+        a.cw[at] = (i32)vw;
+      }
+      __syncthreads();
       // the final inflow of t is at least before + vw, and (float)(u32) is
-      // monotone, so one add that passes MAXW shows the final sum passes it
+      // monotone, so one add that passes MAXW shows the final sum passes it:
+      // part t could pass MAXW, and the select phase checks it
       if (cand) {
         const u64 in = (u64)pwt + before + vw;
         if (in >> 32 || __uint2float_rn((u32)in) > a.maxw) {
-          // part t could pass MAXW: the select phase checks it.  The first
-          // thread to flag it gives it a dense index (read after the barrier).
-          if (atomicCAS(a.risk + t, 0u, 0xffffffffu) == 0u) {
-            const i32 id = atomicAdd(&st->nrisk, 1);
-            a.riskpart[id] = t;
-            atomicExch(a.risk + t, (u32)id + 1u);
-          }
+          a.risk[t] = 1;
           st->needcheck = 1;
         }
       }
@@ -1117,74 +1257,133 @@ __device__ __forceinline__ u64 block_reduce_u64(u64 x, u64* s_tmp) {
 }
 
 constexpr i32 kRiskEvents = 1024;   // event limit of the at-risk balance check
-constexpr i32 kRiskParts = 1024;    // at-risk part limit of that check
+constexpr i32 kRiskParts = 1024;    // part limit of that check (k)
+constexpr i32 kRiskCands = 1024;    // candidate limit of that check
 
-// The balance check of a round whose candidates are all kept (cnt <= cap)
-// and whose last index is not balanced, without sorting the candidates.
-// Only parts flagged in risk can be over MAXW at any index (a part's running
-// change D never exceeds its inflow bound), so only the moves into or out of
-// those parts matter.  Each such move is an event (part, key, +-w), and the
-// events are grouped by part (a counting sort over the parts' dense indices).
-// A part's D after one of its events is the sum of its events with keys up to
-// that key, and it holds until the part's next event; an event with D > 0 and
-// (float)(pw + D) > MAXW marks the key range [key, next key of the part) --
-// the index ranges the reference's table marks (uncoarsen.hpp:239-288), in
-// key order.  Every candidate key is then tested against the marked ranges,
-// and the moves with key <= K* apply, K* = the largest unmarked key, or the
-// smallest key if all are marked (prefix 0 always counts as balanced,
-// :481-488).  Returns false (block-uniform) beyond kRiskEvents events or
-// kRiskParts parts; the caller then runs the check over all parts.
-__device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greedy, u64* keep, u64* s_tmp,
-                                 u32* s_warp, u64* kstar, i32* napplied) {
-  __shared__ i32 s_ne, s_nbad;
-  const i32 nrisk = ldc(&a.st->nrisk);
-  if (nrisk > kRiskParts) return false;   // block-uniform
+// The balance check of a round whose candidates are all kept (cnt <= cap),
+// without sorting the candidates.  Only parts flagged in risk can be over
+// MAXW at any index (a part's running change D never exceeds its inflow
+// bound), so only the moves into or out of those parts matter.
+//  * Last index: the reference applies moves 0..pos for the LARGEST balanced
+//    index pos (Q11), so when the last index is balanced every candidate
+//    moves.  A flagged part's change at the last index is its net change
+//    over all candidates (pnet).
+//  * Otherwise each move into or out of a flagged part is an event (part,
+//    key, +-w), the events are grouped by part (a counting sort), and a
+//    part's D after one of its events is the sum of its events with keys up
+//    to that key, which holds until the part's next event; an event with
+//    D > 0 and (float)(pw + D) > MAXW marks the key range [key, next key of
+//    the part) -- the index ranges the reference's table marks
+//    (uncoarsen.hpp:239-288), in key order.  Every candidate key is tested
+//    against the marked ranges, and the moves with key <= K* apply, K* = the
+//    largest unmarked key, or the smallest key if all are marked (prefix 0
+//    always counts as balanced, :481-488).
+// All global loads come first and at once, from two halves of the CTA: warps
+// 0-7 fetch the candidate list entries (key, source, destination, weight,
+// written beside each other by the candidates phase), warps 8-15 every
+// part's flag, net change and weight.  Everything after one block barrier is
+// shared memory.  Returns false (block-uniform) when the last index is not
+// balanced and k > kRiskParts, cnt > kRiskCands or the events exceed
+// kRiskEvents; the caller then runs the check over all parts.
+__device__ bool refine_check_risk(const LevelArgs& a, i32 cnt, u64* s, i32* greedy, u64* keep, u64* s_tmp,
+                                  u32* s_warp, u64* kstar, i32* napplied) {
+  __shared__ i32 s_ne, s_nbad, s_lastbad;
+  constexpr i32 kHalf = kLevelThreads / 2;
+  constexpr i32 kPerThread = kRiskCands / kHalf;   // candidates per loading thread
+  static_assert(kRiskCands % kHalf == 0, "candidates split evenly over the loading threads");
   u64* ev_key = s + kMaxMoveCap;      // [kRiskEvents] events as found
   u64* gk = ev_key + kRiskEvents;     // [kRiskEvents] grouped by part
   u64* bad_lo = keep;                 // [kRiskEvents] marked key ranges [lo, hi)
   u64* bad_hi = keep + kRiskEvents;   // [kRiskEvents]
-  i32* ev_b = greedy;                 // [kRiskEvents] part index of each event
+  i32* ev_b = greedy;                 // [kRiskEvents] part of each event
   i32* ev_d = ev_b + kRiskEvents;     // [kRiskEvents] weight change
-  i32* gb = ev_d + kRiskEvents;       // grouped: part index
+  i32* gb = ev_d + kRiskEvents;       // grouped: part
   i32* gd = gb + kRiskEvents;         // grouped: weight change
   i32* bcnt = gd + kRiskEvents;       // [kRiskParts] events per part
   i32* boff = bcnt + kRiskParts;      // [kRiskParts] first grouped slot
   i32* bfill = boff + kRiskParts;     // [kRiskParts]
+  i32* rpw = bfill + kRiskParts;      // [kRiskParts] part weight before the round
+  i32* rflag = rpw + kRiskParts;      // [kRiskParts] part flagged in risk
+  static_assert(4 * kRiskEvents + 5 * kRiskParts <= kGreedyWords, "check arrays fit the greedy region");
+  static_assert(kMaxMoveCap + 2 * kRiskEvents <= kSortMax, "event keys fit the sort buffer");
+  static_assert(kRiskCands <= kMaxMoveCap, "candidate keys fit the sort buffer");
+  const i32 k = a.k;
+  const bool small = k <= kRiskParts && cnt <= kRiskCands;   // block-uniform
   if (threadIdx.x == 0) {
     s_ne = 0;
     s_nbad = 0;
+    s_lastbad = 0;
   }
-  for (i32 b = threadIdx.x; b < nrisk; b += blockDim.x) {
-    bcnt[b] = 0;
-    bfill[b] = 0;
-  }
+  if (small)
+    for (i32 b = threadIdx.x; b < k; b += blockDim.x) {
+      bcnt[b] = 0;
+      bfill[b] = 0;
+    }
   __syncthreads();
-  u64 kmin = ~0ull, kmax = 0;
-  for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const u64 key = ldc(a.cands + i);
-    s[i] = key;
-    kmin = key < kmin ? key : kmin;
-    kmax = key > kmax ? key : kmax;
-    const i32 v = (i32)(u32)key;
-    const i32 src = ldc(a.msrc + v), dst = ldc(a.target + v);
-    const i32 w = a.vwgt[v];
-    const u32 rs = ldc(a.risk + src), rd = ldc(a.risk + dst);
-    if (rs) {
-      const i32 e = atomicAdd(&s_ne, 1);
-      if (e < kRiskEvents) {
-        ev_key[e] = key;
-        ev_b[e] = (i32)rs - 1;
-        ev_d[e] = -w;
-        atomicAdd(&bcnt[rs - 1], 1);
+  u64 key[kPerThread];
+  i32 src[kPerThread], dst[kPerThread], w[kPerThread];
+  if (threadIdx.x < kHalf) {
+    if (small) {
+#pragma unroll
+      for (i32 q = 0; q < kPerThread; ++q) {
+        const i32 i = threadIdx.x + q * kHalf;
+        key[q] = ~0ull;
+        src[q] = dst[q] = w[q] = 0;
+        if (i < cnt) {
+          key[q] = ldc(a.cands + i);
+          const u64 inf = ldc(a.cinfo + i);
+          w[q] = ldc(a.cw + i);
+          src[q] = (i32)(u32)(inf >> 32);
+          dst[q] = (i32)(u32)inf;
+        }
       }
     }
-    if (rd) {
-      const i32 e = atomicAdd(&s_ne, 1);
-      if (e < kRiskEvents) {
-        ev_key[e] = key;
-        ev_b[e] = (i32)rd - 1;
-        ev_d[e] = w;
-        atomicAdd(&bcnt[rd - 1], 1);
+  } else {
+    bool bad = false;
+    for (i32 p = threadIdx.x - kHalf; p < k; p += kHalf) {
+      const u32 f = ldc(a.risk + p);
+      const i32 d = ldc(a.pnet + p);
+      const u32 pw = ldc(a.pw + p);
+      if (small) {
+        rflag[p] = (i32)f;
+        rpw[p] = (i32)pw;
+      }
+      if (f && d > 0 && __uint2float_rn((u32)d + pw) > a.maxw) bad = true;
+    }
+    if (bad) s_lastbad = 1;
+  }
+  __syncthreads();
+  if (!s_lastbad) {   // block-uniform: the last index is balanced, every candidate moves
+    *kstar = ~0ull;
+    *napplied = cnt;
+    return true;
+  }
+  if (!small) return false;
+  u64 kmin = ~0ull;
+  if (threadIdx.x < kHalf) {
+#pragma unroll
+    for (i32 q = 0; q < kPerThread; ++q) {
+      const i32 i = threadIdx.x + q * kHalf;
+      if (i >= cnt) continue;
+      s[i] = key[q];
+      kmin = key[q] < kmin ? key[q] : kmin;
+      if (rflag[src[q]]) {
+        const i32 e = atomicAdd(&s_ne, 1);
+        if (e < kRiskEvents) {
+          ev_key[e] = key[q];
+          ev_b[e] = src[q];
+          ev_d[e] = -w[q];
+          atomicAdd(&bcnt[src[q]], 1);
+        }
+      }
+      if (rflag[dst[q]]) {
+        const i32 e = atomicAdd(&s_ne, 1);
+        if (e < kRiskEvents) {
+          ev_key[e] = key[q];
+          ev_b[e] = dst[q];
+          ev_d[e] = w[q];
+          atomicAdd(&bcnt[dst[q]], 1);
+        }
       }
     }
   }
@@ -1194,11 +1393,11 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
   if (ne > kRiskEvents) return false;   // block-uniform
   {   // first grouped slot of each part: exclusive scan, two parts per thread
     const i32 b0 = 2 * threadIdx.x;
-    const u32 c0 = b0 < nrisk ? (u32)bcnt[b0] : 0u, c1 = b0 + 1 < nrisk ? (u32)bcnt[b0 + 1] : 0u;
+    const u32 c0 = b0 < k ? (u32)bcnt[b0] : 0u, c1 = b0 + 1 < k ? (u32)bcnt[b0 + 1] : 0u;
     u32 tot;
     const u32 ex = block_exscan_u32(c0 + c1, s_warp, tot);
-    if (b0 < nrisk) boff[b0] = (i32)ex;
-    if (b0 + 1 < nrisk) boff[b0 + 1] = (i32)(ex + c0);
+    if (b0 < k) boff[b0] = (i32)ex;
+    if (b0 + 1 < k) boff[b0 + 1] = (i32)(ex + c0);
   }
   __syncthreads();
   for (i32 e = threadIdx.x; e < ne; e += blockDim.x) {
@@ -1220,7 +1419,7 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
       if (kf <= kj) D += gd[f];
       else knext = kf < knext ? kf : knext;
     }
-    if (D > 0 && __uint2float_rn((u32)D + ldc(a.pw + ldc(a.riskpart + b))) > a.maxw) {
+    if (D > 0 && __uint2float_rn((u32)D + (u32)rpw[b]) > a.maxw) {
       const i32 at = atomicAdd(&s_nbad, 1);
       bad_lo[at] = kj;
       bad_hi[at] = knext;
@@ -1233,26 +1432,22 @@ __device__ bool refine_threshold(const LevelArgs& a, i32 cnt, u64* s, i32* greed
   u64 best = 0;
   bool any = false;
   for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const u64 key = s[i];
+    const u64 kk = s[i];
     bool marked = false;
-    for (i32 r = 0; r < nbad && !marked; ++r) marked = bad_lo[r] <= key && key < bad_hi[r];
+    for (i32 r = 0; r < nbad && !marked; ++r) marked = bad_lo[r] <= kk && kk < bad_hi[r];
     if (!marked) {
-      best = key > best ? key : best;
+      best = kk > best ? kk : best;
       any = true;
     }
   }
   const u64 top = block_reduce_u64<true>(any ? best + 1 : 0, s_tmp);   // +1: 0 means none
   const u64 K = top ? top - 1 : kmin;
-  __shared__ i32 s_c;
-  if (threadIdx.x == 0) s_c = 0;
-  __syncthreads();
-  i32 c = 0;
+  u32 c = 0;
   for (i32 i = threadIdx.x; i < cnt; i += blockDim.x) c += s[i] <= K;
-  if (c) atomicAdd(&s_c, c);
-  __syncthreads();
+  u32 tot;
+  (void)block_exscan_u32(c, s_warp, tot);
   *kstar = K;
-  *napplied = s_c;
-  (void)kmax;
+  *napplied = (i32)tot;
   return true;
 }
 
@@ -1294,30 +1489,7 @@ __device__ void ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* ke
   i32 pos = B - 1;     // sorted: moves 0..pos of keep apply
   if (check) {
     bool done = false;
-    if (cnt <= a.move_cap) {
-      // The reference applies moves 0..pos for the LARGEST balanced index
-      // pos (Q11), so when the last index is balanced every candidate moves.
-      // Only the at-risk parts can break it; their change at the last index
-      // is their net change over all candidates.
-      __shared__ i32 s_lastbad;
-      if (threadIdx.x == 0) s_lastbad = 0;
-      __syncthreads();
-      const i32 nrisk = ldc(&st->nrisk);
-      for (i32 b = threadIdx.x; b < nrisk; b += blockDim.x) {
-        const i32 p = ldc(a.riskpart + b);
-        const i32 d = ldc(a.pnet + p);
-        if (d > 0 && __uint2float_rn((u32)d + ldc(a.pw + p)) > a.maxw) s_lastbad = 1;
-      }
-      __syncthreads();
-      if (!s_lastbad) {
-        done = true;   // kstar stays ~0: every candidate applies
-        trace_mark(a, 27);
-      }
-    }
-    if (!done && cnt <= a.move_cap) {
-      trace_mark(a, 28);
-      done = refine_threshold(a, cnt, s, greedy, keep, s_tmp, s_warp, &kstar, &napplied);
-    }
+    if (cnt <= a.move_cap) done = refine_check_risk(a, cnt, s, greedy, keep, s_tmp, s_warp, &kstar, &napplied);
     trace_mark(a, 25);
     if (!done) {
       select_sort(a, a.cands, cnt, s, greedy);   // s[0..B) sorted (ends with a block barrier)
@@ -1369,7 +1541,6 @@ __device__ void ph_fold(const LevelArgs& a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.st->ccount = 0;
     a.st->needcheck = 0;
-    a.st->nrisk = 0;
   }
 }
 
@@ -1623,7 +1794,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
   i64 fr = 0;
   trace_mark(a, 0);
   if (a.flags & LF_PROJECT) {
-    ph_project(a, &s_cnt, &s_base);
+    ph_project(a, s_ustage);
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
     trace_mark(a, 1);
   }
@@ -1632,7 +1803,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
     if (!grid_barrier(a.bar, a.err, &s_flag)) return;
     trace_mark(a, 2);
   }
-  if (a.flags & LF_UPDATE) ph_update(a, acc_all, false, s_ustage);
+  if (a.flags & LF_UPDATE) ph_update_first(a, acc_all, reinterpret_cast<u32*>(smem_raw), s_ustage);
   if (a.flags & LF_BALANCE) {
     if (a.batch) ph_bal_prep_batch(a, s_tmp, fr);
     else ph_bal_prep(a, s_tmp);
@@ -1681,7 +1852,7 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 3);
         return;
       }
-      ph_candidates(a, &s_cnt, &s_base);
+      ph_candidates(a, &s_cnt, &s_base, reinterpret_cast<u32*>(greedy));
       if (!grid_barrier(a.bar, a.err, &s_flag)) return;
       trace_mark(a, 20);
       if (a.batch) {
@@ -1756,8 +1927,9 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->pwd = P.alloc_n<u32>(c->k);
   c->pin = P.alloc_n<u32>(c->k);
   c->msrc = P.alloc_n<i32>(n);
+  c->cinfo = P.alloc_n<u64>(n);
+  c->cw = P.alloc_n<i32>(n);
   c->risk = P.alloc_n<u32>(c->k);
-  c->riskpart = P.alloc_n<i32>(c->k);
   c->pnet = P.alloc_n<i32>(c->k);
   c->st = P.alloc_n<RoundState>(1);
   c->bmark = P.alloc_n<u32>(n);
@@ -1886,6 +2058,15 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   memset(&a, 0, sizeof(a));
   a.n = g.n;
   a.k = c->k;
+  {   // first gain pass: lane groups on short rows, when their connection rows
+      // fit in the sort and greedy buffers
+    const size_t room = ((size_t)kSortMax * 8 + (size_t)kGreedyWords * 4) / 4;
+    const double avg = g.n ? (double)g.m / g.n : 0.0;
+    const size_t kr = (size_t)std::max(c->kacc, 1);
+    a.upd_lanes = (avg <= 8.0 && (kLevelThreads / 8) * kr <= room)    ? 8
+                  : (avg <= 16.0 && (kLevelThreads / 16) * kr <= room) ? 16
+                                                                       : 32;
+  }
   a.xadj = g.xadj;
   a.adjncy = g.adjncy;
   a.adjwgt = g.adjwgt;
@@ -1926,8 +2107,9 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.pwd = c->pwd;
   a.pin = c->pin;
   a.msrc = c->msrc;
+  a.cinfo = c->cinfo;
+  a.cw = c->cw;
   a.risk = c->risk;
-  a.riskpart = c->riskpart;
   a.pnet = c->pnet;
   a.st = c->st;
   a.bmark = c->bmark;
