@@ -190,8 +190,9 @@ void* gkw_get_stream(gkw_handle* h) { return h ? (void*)h->h.stream : nullptr; }
 
 static void check_tuning(const gkw_tuning& t) {
   for (int b = 0; b < 4; ++b)
-    GKW_REQUIRE(t.match_lanes[b] == 4 || t.match_lanes[b] == 8 || t.match_lanes[b] == 16 || t.match_lanes[b] == 32,
-                GKW_E_INVALID, "match_lanes must be 4, 8, 16 or 32");
+    GKW_REQUIRE(t.match_lanes[b] == 2 || t.match_lanes[b] == 4 || t.match_lanes[b] == 8 || t.match_lanes[b] == 16 ||
+                    t.match_lanes[b] == 32,
+                GKW_E_INVALID, "match_lanes must be 2, 4, 8, 16 or 32");
   GKW_REQUIRE(t.level_verts_per_cta >= 32 && t.level_min_ctas >= 1, GKW_E_INVALID,
               "level_verts_per_cta must be >= 32 and level_min_ctas >= 1");
   GKW_REQUIRE(t.coarsen_fused_max_n >= 0 && t.coarsen_verts_per_cta >= 64, GKW_E_INVALID,

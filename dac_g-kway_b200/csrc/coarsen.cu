@@ -145,7 +145,8 @@ static void launch_match(Handle& h, const DevGraph& g, i32* cand, i32 G, i32* lo
     launch(kern, (u32)((tot + threads - 1) / threads), threads, 0, h.stream, g.n, g.xadj, g.adjncy, g.adjwgt,
            cand, longlist, longcnt);
   };
-  if (G == 4) go(k_match<4>);
+  if (G == 2) go(k_match<2>);
+  else if (G == 4) go(k_match<4>);
   else if (G == 8) go(k_match<8>);
   else if (G == 16) go(k_match<16>);
   else go(k_match<32>);
@@ -160,8 +161,8 @@ void time_match_variants(Handle& h, const DevGraph& g, i32* cand) {
   Pool::Mark mk = h.scratch.mark();
   i32* longlist = h.scratch.alloc_n<i32>(g.n);
   i32* longcnt = h.scratch.alloc_n<i32>(1);
-  const i32 lanes[4] = {4, 8, 16, 32};
-  for (i32 q = 0; q < 4; ++q) {
+  const i32 lanes[kMatchLaneChoices] = {2, 4, 8, 16, 32};
+  for (i32 q = 0; q < kMatchLaneChoices; ++q) {
     float best = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
       GKW_CUDA(cudaMemsetAsync(longcnt, 0, sizeof(i32), h.stream));
@@ -630,9 +631,22 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
   WarpTable<WCAP>& T = tabs[wid];
   const i32 nc = *ncp;
   const i64 nw = (i64)gridDim.x * WARPS;
-  for (i64 c = (i64)blockIdx.x * WARPS + wid; c < nc; c += nw) {
-    const i32 L = rowlen[c];
-    const i32 nm = mcnt[c];
+  // The next coarse vertex's header (row length, member count, this lane's
+  // member) is loaded while the current one is contracted: two of the five
+  // dependent loads of a coarse row leave the chain.
+  i64 c = (i64)blockIdx.x * WARPS + wid;
+  i32 nL = 0, nnm = 0, nmv = 0;
+  auto header = [&](i64 cc) {
+    if (cc < nc) {
+      nL = rowlen[cc];
+      nnm = mcnt[cc];
+      nmv = lane < cap ? memtab[cc * (i64)cap + lane] : 0;
+    }
+  };
+  header(c);
+  for (; c < nc; c += nw) {
+    const i32 L = nL, nm = nnm, mv = nmv;
+    header(c + nw);
     if (L > WCAP || nm > 32) {
       if (lane == 0) heavy[atomicAdd(nheavy, 1)] = (i32)c;
       continue;
@@ -640,10 +654,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
     // lane j < nm: member j's row; exclusive prefix of the row lengths
     i32 mbeg = 0, mlen = 0;
     if (lane < nm) {
-      const i32 v = memtab[c * (i64)cap + lane];
-      mbeg = xadj[v];
-      mlen = xadj[v + 1] - mbeg;
+      mbeg = xadj[mv];
+      mlen = xadj[mv + 1] - mbeg;
     }
+    const i32 o = ub[c];   // needed only at the writes
     i32 moff = mlen;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -662,7 +676,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
       }
       return pos;
     };
-    const i32 o = ub[c];
     if (L <= 32) {
       // all entries in registers: sort (key, w), merge equal keys, drop self
       u64 kv = ~0ull;
@@ -1324,6 +1337,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_coarsen_fused(FusedArgs a)
   }
   // ---- heavy-edge candidates (coarsen.hpp:39-78) ----
   switch (a.lanes) {
+    case 2: fz_match<2>(a); break;
     case 4: fz_match<4>(a); break;
     case 8: fz_match<8>(a); break;
     case 16: fz_match<16>(a); break;

@@ -20,6 +20,7 @@ typedef int64_t i64;
 typedef uint64_t u64;
 
 constexpr int kMaxLevels = GKW_MAX_LEVELS;
+constexpr int kMatchLaneChoices = 5;   // heavy-edge match lanes per vertex: 2, 4, 8, 16, 32
 
 // ---------------------------------------------------------------------------
 // Errors: C-ABI calls return a status; the message is kept per host thread.
@@ -205,7 +206,7 @@ struct Handle {
   // while the autotuner collects: per average-degree bucket, the summed time
   // of each match lane count (4, 8, 16, 32) over the levels met
   bool tune_collect = false;
-  double tune_match_ms[4][4] = {};
+  double tune_match_ms[4][kMatchLaneChoices] = {};
   Handle() : hier(size_t(256) << 20), scratch(size_t(256) << 20) {}
 };
 void ensure_timer_events(Handle& h);

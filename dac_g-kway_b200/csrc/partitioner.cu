@@ -516,10 +516,10 @@ void autotune(Handle& h, const DevGraph& g, i32 k, const gkw_options& opt) {
     throw;
   }
   h.tune_collect = false;
-  const i32 lanes[4] = {4, 8, 16, 32};
+  const i32 lanes[kMatchLaneChoices] = {2, 4, 8, 16, 32};
   for (i32 b = 0; b < 4; ++b) {
     i32 best = -1;
-    for (i32 q = 0; q < 4; ++q)
+    for (i32 q = 0; q < kMatchLaneChoices; ++q)
       if (h.tune_match_ms[b][q] > 0 && (best < 0 || h.tune_match_ms[b][q] < h.tune_match_ms[b][best])) best = q;
     if (best >= 0) h.tuning.match_lanes[b] = lanes[best];
   }

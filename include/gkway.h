@@ -115,7 +115,7 @@ gkw_status gkw_set_stream(gkw_handle* h, void* stream);
  * (declarations.h:12-18).
  *   match_lanes[b]       lanes per vertex of the heavy-edge match on levels
  *                        whose average degree is <= 6.5, <= 14, <= 28, above
- *                        (b = 0..3; 4, 8, 16 or 32; rows above 512 entries
+ *                        (b = 0..3; 2, 4, 8, 16 or 32; rows above 512 entries
  *                        always go to one CTA each)
  *   level_verts_per_cta  level-kernel CTAs: one per this many vertices ...
  *   level_min_ctas       ... and at least this many (capped at 2 per SM)

@@ -301,11 +301,11 @@ def test_autotune_keeps_results(pkg, gen):
     g = gen.circuit(60000, seed=3, levels=60, hub_max=2000)
     dg = to_dev(g)
     outs = []
-    for shapes in (None, "tune", dict(match_lanes=(32, 4, 4, 4), level_verts_per_cta=64, level_min_ctas=1),
+    for shapes in (None, "tune", dict(match_lanes=(32, 2, 4, 2), level_verts_per_cta=64, level_min_ctas=1),
                    dict(match_lanes=(8, 32, 16, 4), level_verts_per_cta=4096, level_min_ctas=64)):
         if shapes == "tune":
             t = h.autotune(*dg, 32)
-            assert all(x in (4, 8, 16, 32) for x in t["match_lanes"])
+            assert all(x in (2, 4, 8, 16, 32) for x in t["match_lanes"])
         elif shapes is not None:
             h.set_tuning(**shapes)
             assert h.tuning()["level_verts_per_cta"] == shapes["level_verts_per_cta"]
