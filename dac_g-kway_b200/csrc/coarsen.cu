@@ -329,14 +329,31 @@ __global__ void k_group_count(i32 n, const u64* __restrict__ keys, i32* __restri
   if (v < n) atomicAdd(&gsize[(u32)(keys[v] >> 32)], 1);
 }
 
+// Coarse ids per root: ceil(size / cap) (scanned afterwards).  A group above
+// the cap also takes its block of the member list here, from a counter with
+// one atomic per warp: the blocks' order does not matter, since every group
+// is ordered by (dist, id) within its own block.
 __global__ void k_group_chunks(i32 n, const i32* __restrict__ gsize, i32 cap, i32* __restrict__ chunks,
-                               i32* __restrict__ bigsz) {
+                               i32* __restrict__ goff, i32* __restrict__ mcounter) {
   const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  i32 s = 0;
   if (v < n) {
-    const i32 s = gsize[v];
+    s = gsize[v];
     chunks[v] = (s + cap - 1) / cap;
-    bigsz[v] = s > cap ? s : 0;
   }
+  const i32 big = s > cap ? s : 0;
+  i32 inc = big;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const i32 y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += y;
+  }
+  const i32 tot = __shfl_sync(kFull, inc, 31);
+  i32 base = 0;
+  if (lane == 31 && tot) base = atomicAdd(mcounter, tot);
+  base = __shfl_sync(kFull, base, 31);
+  if (big) goff[v] = base + inc - big;
 }
 
 // counts[]: [0] groups of 7..32 members (warp sort), [1] groups above kGroupSmem
@@ -513,10 +530,9 @@ void run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap, i32* d
   GKW_CUDA(cudaMemsetAsync(gcur, 0, sizeof(i32) * n, h.stream));
   GKW_CUDA(cudaMemsetAsync(counts, 0, sizeof(i32) * 8, h.stream));
   launch(k_group_count, nb, 256, 0, h.stream, n, keys, gsize);
-  launch(k_group_chunks, nb, 256, 0, h.stream, n, gsize, cap, chunks, bigsz);
+  launch(k_group_chunks, nb, 256, 0, h.stream, n, gsize, cap, chunks, bigsz, counts + 3);
   GKW_CHECK_LAUNCH();
   exclusive_scan_i32(h, chunks, chunks, n, d_nc);   // chunks -> chunk base, total = n_c
-  exclusive_scan_i32(h, bigsz, bigsz, n, counts + 3);   // member offsets of big groups
   launch(k_group_scatter, nb, 256, 0, h.stream, n, keys, gsize, chunks, bigsz, gcur, cap, cmap, members,
          biglist, ctalist, giantlist, counts);
   const u32 ng = std::max<u32>(1, std::min<u32>(ceil_div(n, 8 * 32), (u32)h.sm_count * 16));
@@ -676,14 +692,44 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
       }
       return pos;
     };
+    // Rows whose entries other than self loops fit one per lane merge in
+    // registers: every row of up to 32 entries, and rows of up to 64 entries
+    // with at most 32 left after the self loops (the members' edges to one
+    // another) are dropped -- most coarse rows of a mesh.
+    u64 kv = ~0ull;
+    bool in_regs = false;
     if (L <= 32) {
-      // all entries in registers: sort (key, w), merge equal keys, drop self
-      u64 kv = ~0ull;
       const i32 pos = entry_pos(lane);
       if (lane < L) {
         const u32 key = (u32)cmap[adjncy[pos]];
         if (key != (u32)c) kv = ((u64)key << 32) | (u32)adjwgt[pos];
       }
+      in_regs = true;
+    } else if (L <= 64) {
+      const i32 p0 = entry_pos(lane), p1 = entry_pos(lane + 32);
+      u64 e0 = ~0ull, e1 = ~0ull;
+      {
+        const u32 k0 = (u32)cmap[adjncy[p0]];
+        if (k0 != (u32)c) e0 = ((u64)k0 << 32) | (u32)adjwgt[p0];
+      }
+      if (lane + 32 < L) {
+        const u32 k1 = (u32)cmap[adjncy[p1]];
+        if (k1 != (u32)c) e1 = ((u64)k1 << 32) | (u32)adjwgt[p1];
+      }
+      const u32 m0 = __ballot_sync(kFull, e0 != ~0ull), m1 = __ballot_sync(kFull, e1 != ~0ull);
+      const i32 n0 = __popc(m0), tot = n0 + __popc(m1);
+      if (tot <= 32) {   // warp-uniform: compact the kept entries to one per lane
+        const u32 lt = (1u << lane) - 1u;
+        if (e0 != ~0ull) T.out[__popc(m0 & lt)] = e0;
+        if (e1 != ~0ull) T.out[n0 + __popc(m1 & lt)] = e1;
+        __syncwarp();
+        kv = lane < tot ? T.out[lane] : ~0ull;
+        __syncwarp();
+        in_regs = true;
+      }
+    }
+    if (in_regs) {
+      // sort (key, w), merge equal keys (self loops are already out)
 #pragma unroll
       for (int kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
