@@ -64,6 +64,65 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, i32* err, i32* s_fl
   return *s_flag == 0;
 }
 
+// Grid barrier that also sums one count per CTA (thread 0's `mine`: the CTA's
+// list appends in the phase before the barrier), so that the phase after it
+// knows the list's length without another round trip to L2.  Three 64-bit
+// words rotate: barrier k adds (mine << 32 | arrival) to word k % 3, whose
+// arrival parts flip bit 31 exactly when the last CTA arrives, as in
+// grid_barrier (the word starts at zero, so the low half never carries into
+// the count).  The last CTA to arrive clears word (k + 2) % 3: every CTA has
+// passed that word's last use (barrier k - 1), and none can reach its next use
+// (barrier k + 2) before this CTA's release at barrier k + 1.  After the flip
+// a word does not change until it is cleared, so every CTA reads the same
+// total.  The host zeroes words 0 and 1 before the launch.  A one-CTA or
+// one-cluster grid sums nothing: *total = -1 and the caller loads its counter.
+__device__ __forceinline__ u64 atom_add_release_gpu_u64(u64* p, u64 v) {
+  u64 old;
+  asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ u64 ld_acquire_gpu_u64(const u64* p) {
+  u64 v;
+  asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier_count(CountBarrier* cb, u32 k, i32* err, i32* s_flag, i32* s_total,
+                                                   u32 mine, i32* total) {
+  if (gridDim.x == 1 || cluster_ncta() == gridDim.x) {
+    *total = -1;
+    return grid_barrier(nullptr, err, s_flag);   // these forms use no barrier word
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u64* w = reinterpret_cast<u64*>(&cb->w[k % 3]);
+    const u64 add = ((u64)mine << 32) | (u64)(blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u);
+    const u64 old = atom_add_release_gpu_u64(w, add);
+    u64 cur = old + add;
+    i32 bad = 0;
+    if (cur & 0x80000000ull) {   // the last arrival: cur is the word's final value
+      cb->w[(k + 2) % 3] = 0;
+    } else {
+      const long long t0 = clock64();
+      for (;;) {
+        cur = ld_acquire_gpu_u64(w);
+        if (cur & 0x80000000ull) break;
+        if (clock64() - t0 > kGridBarrierCycles) {
+          atomicExch(err, 1);
+          bad = 1;
+          break;
+        }
+      }
+    }
+    *s_flag = bad;
+    *s_total = (i32)(u32)(cur >> 32);
+  }
+  __syncthreads();
+  *total = *s_total;
+  return *s_flag == 0;
+}
+
 __device__ __forceinline__ i32 ldcg(const i32* p) { return __ldcg(p); }
 __device__ __forceinline__ u32 ldcg(const u32* p) { return __ldcg(p); }
 __device__ __forceinline__ u64 ldcg(const u64* p) {

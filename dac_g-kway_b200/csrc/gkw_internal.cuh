@@ -126,6 +126,12 @@ struct GridBarrier {
   u32 pad;
 };
 
+// Three rotating 64-bit barrier words that also sum a count per CTA
+// (grid_barrier_count, device_util.cuh); zero before a launch.
+struct CountBarrier {
+  unsigned long long w[3];
+};
+
 // Device-side state of one handle shared by the cooperative kernels and the
 // per-level scalars read back once per level.
 struct CoopState {

@@ -102,6 +102,7 @@ struct RefineCtx {
   u32* brem = nullptr;
   u32* epoch = nullptr;   // never reset: marks of earlier rounds stay stale
   GridBarrier* bar = nullptr;
+  CountBarrier* cbar = nullptr;   // the refinement rounds' barriers (zeroed before each launch)
   i32* err = nullptr;
   LevelStatsDev* stats = nullptr;
   u64* trace = nullptr;     // GKW_TRACE=1: per-level phase timelines
@@ -141,6 +142,7 @@ struct LevelArgs {
   u32* brem;          // part weights of the balance greedy pass when k > kGreedySmemParts
   u32* epoch;
   GridBarrier* bar;
+  CountBarrier* cbar;   // plain levels' refinement rounds: barriers that sum the list appends
   i32* err;
   LevelStatsDev* stat_slot;
   i32 acc_warps;
@@ -382,12 +384,12 @@ __device__ void ph_lists(const LevelArgs& a) {
 // Vertices whose new gain is positive join P.
 // `count`: add the row lengths read to the level's entry counter (the update
 // passes of the rounds; the first pass of a level is counted as a full pass).
-__device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, UStage& S) {
+__device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, UStage& S, i32 nU_known) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid >= a.acc_warps) return;
   u32* acc = acc_all + (size_t)wid * a.kacc;
   RoundState* st = a.st;
-  const i32 nU = ldc(&st->ucount);
+  const i32 nU = nU_known >= 0 ? nU_known : ldc(&st->ucount);
   i32* Pout = a.P0;          // P is never compacted within a level: entries whose
   i32* pcount = &st->pcount[0];   // gain dropped stay and are skipped by gain
   const i64 nw = (i64)gridDim.x * a.acc_warps;
@@ -489,12 +491,15 @@ __device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, USt
 
 // P appends are staged per CTA in shared memory (S) and flushed with one
 // global atomic; every thread of the CTA calls this.
-__device__ void ph_update(const LevelArgs& a, u32* acc_all, bool count, UStage& S) {
+// Returns (thread 0) the CTA's appends to P.  nU_known: the length of U when
+// the caller has it (from grid_barrier_count), else -1.
+__device__ u32 ph_update(const LevelArgs& a, u32* acc_all, bool count, UStage& S, i32 nU_known = -1) {
   if (threadIdx.x == 0) S.cnt = 0;
   __syncthreads();
-  ph_update_rows(a, acc_all, count, S);
+  ph_update_rows(a, acc_all, count, S, nU_known);
   ustage_flush(S, a.P0, &a.st->pcount[0]);
   __syncthreads();
+  return (u32)S.cnt;
 }
 
 // The first gain pass of a level (every boundary vertex of U) on a graph of
@@ -606,7 +611,9 @@ __device__ void ph_update_first(const LevelArgs& a, u32* acc_all, u32* rows, USt
 // MAXW even with every candidate moved in, every prefix of the sorted moves
 // is balanced and the select phase needs neither the sort nor the check;
 // otherwise the parts that could pass it are flagged in risk.
-__device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base, u32* s_pwc) {
+// Returns (thread 0) the CTA's appended candidates (plain levels).  nP_known:
+// the length of P when the caller has it, else -1.
+__device__ u32 ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base, u32* s_pwc, i32 nP_known = -1) {
   RoundState* st = a.st;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (a.batch) *a.mcount = 0;   // the round's moves
@@ -622,7 +629,8 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base, u32* 
     __syncthreads();
   }
   auto pw_of = [&](i32 q) -> u32 { return pwc ? s_pwc[q] : ldc(a.pw + q); };
-  const i32 nP = ldc(&st->pcount[0]);
+  const i32 nP = nP_known >= 0 ? nP_known : ldc(&st->pcount[0]);
+  u32 mine = 0;
   // entry r*32*W + lane*W + w goes to warp w, lane `lane`: the entries of a
   // round spread over all warps, so each warp checks at most a few of them
   const i64 W = (i64)gridDim.x * (blockDim.x >> 5);
@@ -685,7 +693,10 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base, u32* 
       __syncthreads();
       const i32 local = cand ? atomicAdd(s_cnt, 1) : -1;
       __syncthreads();
-      if (threadIdx.x == 0 && *s_cnt) *s_base = atomicAdd(&st->ccount, *s_cnt);
+      if (threadIdx.x == 0 && *s_cnt) {
+        *s_base = atomicAdd(&st->ccount, *s_cnt);
+        mine += (u32)*s_cnt;
+      }
       __syncthreads();
       if (cand) {
         const i32 at = *s_base + local;
@@ -705,7 +716,7 @@ __device__ void ph_candidates(const LevelArgs& a, i32* s_cnt, i32* s_base, u32* 
         }
       }
     }
-  }
+  }  return mine;
 }
 
 // Sort the candidates by (gain desc, id asc) and keep the first min(cnt, cap)
@@ -1468,16 +1479,19 @@ __device__ bool refine_check_risk(const LevelArgs& a, i32 cnt, u64* s, i32* gree
 // round: the moves of this phase add their weights to pwd, which the gain
 // update folds into pw.  Move j is applied by global warp j (mod the warp
 // count), so a CTA owns an index below B iff blockIdx.x * warps_per_cta < B.
-__device__ void ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* keep, u32* s_warp, u64* s_tmp,
-                                UStage& S) {
+// Returns (thread 0) the CTA's appends to U.  cnt: the round's candidates.
+__device__ u32 ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* keep, u32* s_warp, u64* s_tmp,
+                               UStage& S, i32 cnt) {
   RoundState* st = a.st;
-  const i32 cnt = ldc(&st->ccount);
   const i32 B = cnt < a.move_cap ? cnt : a.move_cap;
-  const bool check = ldc(&st->needcheck) != 0;
   const i32 nw = blockDim.x >> 5;
   const i64 warp = (i64)blockIdx.x * nw + (threadIdx.x >> 5);
   const i64 nwarps = (i64)gridDim.x * nw;
-  if ((i64)blockIdx.x * nw >= B) return;   // block-uniform: no move index of this CTA is kept
+  if ((i64)blockIdx.x * nw >= B) return 0;   // block-uniform: no move index of this CTA is kept
+  // the warp's first candidate, loaded beside the check flag (used when every
+  // candidate applies)
+  const u64 key0 = warp < cnt ? ldc(a.cands + warp) : 0ull;
+  const bool check = ldc(&st->needcheck) != 0;
   __shared__ unsigned long long s_gsum;
   if (threadIdx.x == 0) {
     s_gsum = 0;
@@ -1515,12 +1529,13 @@ __device__ void ph_refine_apply(const LevelArgs& a, u64* s, i32* greedy, u64* ke
     for (i64 j = warp; j <= pos; j += nwarps) apply_move(a, S, keep[j], a.pwd, &s_gsum);
   } else {
     for (i64 j = warp; j < cnt; j += nwarps) {
-      const u64 key = ldc(a.cands + j);
+      const u64 key = j == warp ? key0 : ldc(a.cands + j);
       if (key <= kstar) apply_move(a, S, key, a.pwd, &s_gsum);   // warp-uniform
     }
   }
   ustage_flush(S, a.U, &st->ucount);
   if (threadIdx.x == 0 && s_gsum) atomicAdd((unsigned long long*)&st->gain_sum, s_gsum);
+  return (u32)S.cnt;
 }
 
 // Plain level, after the moves of a round: their part-weight changes join pw,
@@ -1792,6 +1807,13 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
   RoundState* st = a.st;
   // batched levels: the rotating flag use counter (uniform over the grid)
   i64 fr = 0;
+  // the counting barriers' words start at zero: block 0 clears them before
+  // its first grid barrier, which every CTA passes before the first of them
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.cbar->w[0] = 0;
+    a.cbar->w[1] = 0;
+    a.cbar->w[2] = 0;
+  }
   trace_mark(a, 0);
   if (a.flags & LF_PROJECT) {
     ph_project(a, s_ustage);
@@ -1847,30 +1869,49 @@ __global__ void __launch_bounds__(kLevelThreads, GKW_LEVEL_MIN_BLOCKS) k_level(L
     }
   }
   if (a.flags & LF_REFINE) {
+    // plain levels: the round's list lengths ride on the barriers
+    // (grid_barrier_count); P only grows within a level.  A launch without an
+    // earlier phase passes one grid barrier first, which orders block 0's
+    // clearing of the counting words before every CTA's first use.
+    if (!(a.flags & (LF_PROJECT | LF_LISTS | LF_UPDATE | LF_BALANCE)))
+      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+    __shared__ i32 s_total;
+    u32 cbk = 0;
+    i32 nP = a.batch ? -1 : ldc(&st->pcount[0]);
     for (i64 r = 0;; ++r) {
       if (r > a.max_rounds) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, 3);
         return;
       }
-      ph_candidates(a, &s_cnt, &s_base, reinterpret_cast<u32*>(greedy));
-      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
-      trace_mark(a, 20);
+      const u32 my_cands = ph_candidates(a, &s_cnt, &s_base, reinterpret_cast<u32*>(greedy), nP);
       if (a.batch) {
+        if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        trace_mark(a, 20);
         ++fr;
         ph_select_batch(a, s_sort, greedy, s_warp, false, fr);
         if (!grid_barrier(a.bar, a.err, &s_flag)) return;
         trace_mark(a, 21);
         if (ldc(a.anyf + fr % 3) == 0) break;
         ph_apply_refine(a, s_ustage);
-      } else {
-        if (ldc(&st->ccount) == 0) break;   // every CTA reads the same count
-        ph_refine_apply(a, s_sort, greedy, s_keep, s_warp, s_tmp, s_ustage);
+        if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        trace_mark(a, 23);
+        ph_update(a, acc_all, true, s_ustage);
+        if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        trace_mark(a, 24);
+        continue;
       }
-      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      i32 nC, nU, nPadd;
+      if (!grid_barrier_count(a.cbar, cbk++, a.err, &s_flag, &s_total, my_cands, &nC)) return;
+      if (nC < 0) nC = ldc(&st->ccount);
+      trace_mark(a, 20);
+      if (nC == 0) break;   // every CTA has the same count
+      const u32 my_u = ph_refine_apply(a, s_sort, greedy, s_keep, s_warp, s_tmp, s_ustage, nC);
+      if (!grid_barrier_count(a.cbar, cbk++, a.err, &s_flag, &s_total, my_u, &nU)) return;
       trace_mark(a, 23);
-      ph_update(a, acc_all, true, s_ustage);
-      if (!a.batch) ph_fold(a);
-      if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+      const u32 my_p = ph_update(a, acc_all, true, s_ustage, nU);
+      ph_fold(a);
+      if (!grid_barrier_count(a.cbar, cbk++, a.err, &s_flag, &s_total, my_p, &nPadd)) return;
+      nP = nPadd < 0 ? ldc(&st->pcount[0]) : nP + nPadd;
       trace_mark(a, 24);
     }
   }
@@ -1939,6 +1980,7 @@ static void ctx_common(Handle& h, Pool& P, RefineCtx* c, size_t n) {
   c->brem = P.alloc_n<u32>(c->k);
   c->epoch = P.alloc_n<u32>(1);
   c->bar = P.alloc_n<GridBarrier>(1);
+  c->cbar = P.alloc_n<CountBarrier>(1);
   c->err = P.alloc_n<i32>(1);
   c->stats = P.alloc_n<LevelStatsDev>(kStatSlots);
   if (const char* t = getenv("GKW_TRACE"); t && *t == '1') {
@@ -2119,6 +2161,7 @@ void level_run(Handle& h, RefineCtx* c, const DevGraph& g, const LevelJob& j, i3
   a.brem = c->brem;
   a.epoch = c->epoch;
   a.bar = c->bar;
+  a.cbar = c->cbar;
   a.err = c->err;
   a.stat_slot = c->stats + slot;
   a.acc_warps = c->acc_warps;
