@@ -45,13 +45,14 @@ __global__ void k_init_count(i32 n, const i32* __restrict__ lo, i32* __restrict_
   if (v < n) atomicAdd(&cnt[lo[v]], 1);
 }
 
+// Warp maximum of a 64-bit key in two 32-bit reductions (redux.sync): the
+// largest high half, then the largest low half among the lanes holding it --
+// two dependent steps instead of five shuffle rounds on a growth step's chain.
 __device__ __forceinline__ u64 warp_max_u64(u64 x) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const u64 y = __shfl_xor_sync(kFull32, x, o);
-    x = x > y ? x : y;
-  }
-  return x;
+  const u32 hi = (u32)(x >> 32), lo = (u32)x;
+  const u32 mh = __reduce_max_sync(kFull32, hi);
+  const u32 ml = __reduce_max_sync(kFull32, hi == mh ? lo : 0u);
+  return ((u64)mh << 32) | ml;
 }
 
 __device__ __forceinline__ i64 warp_sum_i64(i64 x) {

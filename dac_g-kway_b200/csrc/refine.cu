@@ -305,6 +305,16 @@ __device__ __forceinline__ void ustage_flush(UStage& S, i32* U, i32* ucount) {
   for (i32 t = threadIdx.x; t < c; t += blockDim.x) U[S.base + t] = S.buf[t];
 }
 
+// Maximum of a 64-bit key over a converged warp in two 32-bit reductions
+// (redux.sync): the largest high half, then the largest low half among the
+// lanes that hold it.
+__device__ __forceinline__ u64 warp_max_key(u64 x) {
+  const u32 hi = (u32)(x >> 32), lo = (u32)x;
+  const u32 mh = __reduce_max_sync(kFullMask, hi);
+  const u32 ml = __reduce_max_sync(kFullMask, hi == mh ? lo : 0u);
+  return ((u64)mh << 32) | ml;
+}
+
 // ---------------------------------------------------------------------------
 // Phases.  `base` of every grid-stride loop is warp-uniform so that warp
 // collectives run converged.
@@ -422,11 +432,7 @@ __device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, USt
           const u64 key = ((u64)(accb[q1] - id) << 32) | (u32)(~(u32)q1);
           best = best > key ? best : key;
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          const u64 ot = __shfl_xor_sync(kFullMask, best, o);
-          best = best > ot ? best : ot;
-        }
+        best = warp_max_key(best);
         const u32 gb = (u32)(best >> 32);
         if (gb > 0) { g = gb; q_best = ~(u32)best; }
       }
@@ -464,11 +470,7 @@ __device__ void ph_update_rows(const LevelArgs& a, u32* acc_all, bool count, USt
           best = best > key ? best : key;
         }
       }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const u64 ot = __shfl_xor_sync(kFullMask, best, o);
-        best = best > ot ? best : ot;
-      }
+      best = warp_max_key(best);
       const u32 gb = (u32)(best >> 32);
       if (gb > 0) { g = gb; q_best = ~(u32)best; }
     }
