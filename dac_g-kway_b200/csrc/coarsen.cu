@@ -4,6 +4,7 @@
 // shared-memory hashing, no host round trip per union-find iteration).
 #include <algorithm>
 #include <climits>
+#include <cstddef>
 
 #include "device_util.cuh"
 
@@ -384,15 +385,15 @@ __global__ void k_group_scatter(i32 n, const u64* __restrict__ keys, const i32* 
 __device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
 __device__ __forceinline__ u64 umax64(u64 a, u64 b) { return a < b ? b : a; }
 
-// one warp per big group with <= 32 members
-__global__ void k_group_sort_warp(const i32* __restrict__ biglist, const i32* __restrict__ counts,
-                                  const u64* __restrict__ keys, const i32* __restrict__ gsize,
-                                  const i32* __restrict__ goff, const i32* __restrict__ cbase,
-                                  const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap) {
+// one warp per big group with <= 32 members (CTAs [0, nblocks) of the launch)
+__device__ void group_sort_warps(const i32* __restrict__ biglist, const i32* __restrict__ counts,
+                                 const u64* __restrict__ keys, const i32* __restrict__ gsize,
+                                 const i32* __restrict__ goff, const i32* __restrict__ cbase,
+                                 const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap, u32 nblocks) {
   const i32 nbig = counts[0];
   const int lane = threadIdx.x & 31;
   const i64 warp0 = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
+  const i64 nwarps = ((i64)nblocks * blockDim.x) >> 5;
   for (i64 w = warp0; w < nbig; w += nwarps) {
     const i32 r = biglist[w];
     const i32 s = gsize[r];
@@ -433,14 +434,15 @@ __device__ void cta_bitonic_u64(u64* a, i32 P) {
   }
 }
 
-// one CTA per big group with 33..kGroupSmem members
-__global__ void k_group_sort_cta(const i32* __restrict__ biglist, const i32* __restrict__ counts,
-                                 const u64* __restrict__ keys, const i32* __restrict__ gsize,
-                                 const i32* __restrict__ goff, const i32* __restrict__ cbase,
-                                 const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap) {
+// one CTA per big group with 33..kGroupSmem members (CTA `cta` of `nctas`)
+__device__ void group_sort_ctas(const i32* __restrict__ biglist, const i32* __restrict__ counts,
+                                const u64* __restrict__ keys, const i32* __restrict__ gsize,
+                                const i32* __restrict__ goff, const i32* __restrict__ cbase,
+                                const i32* __restrict__ members, i32 cap, i32* __restrict__ cmap, u32 cta,
+                                u32 nctas) {
   __shared__ u64 sk[kGroupSmem];
   const i32 nbig = counts[4];
-  for (i32 b = blockIdx.x; b < nbig; b += gridDim.x) {
+  for (i32 b = (i32)cta; b < nbig; b += (i32)nctas) {
     const i32 r = biglist[b];
     const i32 s = gsize[r];
     i32 P = 64;
@@ -458,6 +460,21 @@ __global__ void k_group_sort_cta(const i32* __restrict__ biglist, const i32* __r
     for (i32 i = threadIdx.x; i < s; i += blockDim.x) cmap[(u32)sk[i]] = cbase[r] + i / cap;
     __syncthreads();
   }
+}
+
+// The group orders of one level in one launch: CTAs [0, nwarp_blocks) sort
+// the groups of up to 32 members by warps, the CTAs after them the groups of
+// up to kGroupSmem members, one CTA each.
+__global__ void k_group_sort(const i32* __restrict__ wlist, const i32* __restrict__ clist,
+                             const i32* __restrict__ counts, const u64* __restrict__ keys,
+                             const i32* __restrict__ gsize, const i32* __restrict__ goff,
+                             const i32* __restrict__ cbase, const i32* __restrict__ members, i32 cap,
+                             i32* __restrict__ cmap, u32 nwarp_blocks) {
+  if (blockIdx.x < nwarp_blocks)
+    group_sort_warps(wlist, counts, keys, gsize, goff, cbase, members, cap, cmap, nwarp_blocks);
+  else
+    group_sort_ctas(clist, counts, keys, gsize, goff, cbase, members, cap, cmap, blockIdx.x - nwarp_blocks,
+                    gridDim.x - nwarp_blocks);
 }
 
 // Giant groups (more than kGroupSmem members, rare): every CTA of one
@@ -536,9 +553,8 @@ void run_group_map(Handle& h, i32 n, const u64* keys, i32 cap, i32* cmap, i32* d
   launch(k_group_scatter, nb, 256, 0, h.stream, n, keys, gsize, chunks, bigsz, gcur, cap, cmap, members,
          biglist, ctalist, giantlist, counts);
   const u32 ng = std::max<u32>(1, std::min<u32>(ceil_div(n, 8 * 32), (u32)h.sm_count * 16));
-  launch(k_group_sort_warp, ng, 256, 0, h.stream, biglist, counts, keys, gsize, bigsz, chunks, members, cap, cmap);
-  launch(k_group_sort_cta, (u32)h.sm_count * 2, 256, 0, h.stream, ctalist, counts, keys, gsize, bigsz, chunks,
-         members, cap, cmap);
+  launch(k_group_sort, ng + (u32)h.sm_count * 2, 256, 0, h.stream, biglist, ctalist, counts, keys, gsize, bigsz,
+         chunks, members, cap, cmap, ng);
   GKW_CHECK_LAUNCH();
   {
     const i32* gl = giantlist;
@@ -834,8 +850,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_contract_warp(
 // (bump allocation: keys and values of hsz words each, then hsz/2 sorted
 // outputs as u64).  A row that does not fit in the arena records the words it
 // needs and sets the overflow flag; the host grows the arena and runs the
-// contraction again.
-template <bool GLOBAL_TABLE>
+// contraction again.  Both kinds of row run in one launch.
 __global__ void __launch_bounds__(512) k_contract_cta(
     const i32* __restrict__ heavy, const i32* __restrict__ nheavy, i32 cta_cap,
     const i32* __restrict__ xadj, const i32* __restrict__ adjncy, const i32* __restrict__ adjwgt,
@@ -849,13 +864,12 @@ __global__ void __launch_bounds__(512) k_contract_cta(
   for (i32 b = blockIdx.x; b < nh; b += gridDim.x) {
     const i32 c = heavy[b];
     const i32 L = rowlen[c];
-    const bool mine = GLOBAL_TABLE ? (L > cta_cap) : (L <= cta_cap);
-    if (!mine) continue;   // block-uniform
+    const bool global_table = L > cta_cap;   // block-uniform
     u32 hsz = 64;
     while (hsz < 2u * (u32)L) hsz <<= 1;
     u32 *keys, *vals;
     u64* out;
-    if (GLOBAL_TABLE) {
+    if (global_table) {
       const u64 words = 3ull * hsz;   // keys + vals + hsz/2 u64 outputs
       if (threadIdx.x == 0) {
         const u64 off = atomicAdd((unsigned long long*)&arena->used, (unsigned long long)words);
@@ -920,15 +934,17 @@ __global__ void __launch_bounds__(512) k_contract_cta(
 // and copy the 32 rows' entries as one flat range, each lane finding its
 // entry's row by a binary search over the lanes' prefix sums.  A hub row of
 // thousands of entries is then copied by all 32 lanes, not by one thread.
+// Also the level's longest coarse row and heaviest coarse vertex (both
+// *maxdeg and *max_cvw start at zero).
 __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__ ub, const i32* __restrict__ cnt,
                             const i32* __restrict__ cx, const i32* __restrict__ sadj,
                             const i32* __restrict__ swgt, i32* __restrict__ cadj, i32* __restrict__ cwgt,
-                            i32* __restrict__ maxdeg) {
+                            i32* __restrict__ maxdeg, const i32* __restrict__ cvw, i32* __restrict__ max_cvw) {
   const i32 nc = *ncp;
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * blockDim.x) >> 5;
-  i32 mx = 0;
+  i32 mx = 0, mw = 0;
   for (i64 c0 = warp * 32; c0 < nc; c0 += nwarps * 32) {
     const i64 c = c0 + lane;
     i32 src = 0, dst = 0, len = 0;
@@ -936,6 +952,7 @@ __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__
       src = ub[c];
       dst = cx[c];
       len = cnt[c];
+      mw = cvw[c] > mw ? cvw[c] : mw;
     }
     mx = len > mx ? len : mx;
     i32 inc = len;
@@ -967,8 +984,11 @@ __global__ void k_copy_rows(const i32* __restrict__ ncp, const i32* __restrict__
   for (int o = 16; o > 0; o >>= 1) {
     const i32 y = __shfl_xor_sync(kFull, mx, o);
     mx = mx > y ? mx : y;
+    const i32 z = __shfl_xor_sync(kFull, mw, o);
+    mw = mw > z ? mw : z;
   }
   if (lane == 0 && mx > 0) atomicMax(maxdeg, mx);
+  if (lane == 0 && mw > 0) atomicMax(max_cvw, mw);
 }
 
 void ensure_arena(Handle& h, u64 words) {
@@ -1034,16 +1054,14 @@ void run_contract(Handle& h, const DevGraph& g, const i32* cmap, const i32* d_nc
   constexpr i32 kCtaCap = 4096;
   const size_t csm = (size_t)kCtaCap * 2 * 4 * 2 + (size_t)kCtaCap * 8;
   if (!h.capturing)
-    GKW_CUDA(cudaFuncSetAttribute(k_contract_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-  launch(k_contract_cta<false>, (u32)h.sm_count * 2, 512, csm, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
-         g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, h.arena, words, h.arena_words);
-  launch(k_contract_cta<true>, (u32)h.sm_count, 512, 0, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
+    GKW_CUDA(cudaFuncSetAttribute(k_contract_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  launch(k_contract_cta, (u32)h.sm_count * 2, 512, csm, h.stream, heavy, misc, kCtaCap, g.xadj, g.adjncy,
          g.adjwgt, cmap, memtab, mcnt, cap, rowlen, ub, sadj, swgt, cnt, h.arena, words, h.arena_words);
   GKW_CHECK_LAUNCH();
   exclusive_scan_i32(h, cnt, cxadj, nu, d_mc);   // cxadj[n_c] = m_c (rows beyond n_c are empty)
   if (nc_ub > 0)
     launch(k_copy_rows, ceil_div(nc_ub, 256), 256, 0, h.stream, d_nc, ub, cnt, cxadj, sadj, swgt, cadjncy,
-           cadjwgt, &h.coop->maxdeg);
+           cadjwgt, &h.coop->maxdeg, (const i32*)cvwgt, &h.coop->max_cvw);
   GKW_CHECK_LAUNCH();
   h.scratch.release(mk);
 }
@@ -1070,20 +1088,6 @@ CoopState read_coop(Handle& h) {
   if (c.err == 2) throw Error{GKW_E_INTERNAL, "union-find did not converge"};
   if (c.scan_err) throw Error{GKW_E_INTERNAL, "scan: look-back wait timed out"};
   return c;
-}
-
-// Heaviest coarse vertex (*out starts at 0).
-__global__ void k_max_cvw(const i32* __restrict__ ncp, const i32* __restrict__ cvw, i32* __restrict__ out) {
-  const i32 nc = *ncp;
-  i32 m = 0;
-  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x)
-    m = m > cvw[c] ? m : cvw[c];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const i32 y = __shfl_xor_sync(kFull, m, o);
-    m = m > y ? m : y;
-  }
-  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
 }
 
 // ===========================================================================
@@ -2001,15 +2005,11 @@ void coarsen_level(Handle& h, const DevGraph& g, i32 cap, CoarsenOut& out) {
     run_union_find(h, g.n, cand, keys, &h.coop->uf_rounds);
     run_group_map(h, g.n, keys, cap, out.cmap, &h.coop->nc);
     h.scratch.release(mk);
-    GKW_CUDA(cudaMemsetAsync(&h.coop->maxdeg, 0, sizeof(i32), h.stream));
+    static_assert(offsetof(CoopState, maxdeg) == offsetof(CoopState, max_cvw) + sizeof(i32),
+                  "max_cvw and maxdeg are cleared together");
+    GKW_CUDA(cudaMemsetAsync(&h.coop->max_cvw, 0, 2 * sizeof(i32), h.stream));
     run_contract(h, g, out.cmap, &h.coop->nc, g.n, cap, out.cxadj, out.cadjncy, out.cadjwgt, out.cvwgt,
                  &h.coop->mc);
-    GKW_CUDA(cudaMemsetAsync(&h.coop->max_cvw, 0, sizeof(i32), h.stream));
-    if (g.n > 0) {
-      const u32 gm = std::max<u32>(1, std::min<u32>(ceil_div(g.n, 256), (u32)h.sm_count * 4));
-      launch(k_max_cvw, gm, 256, 0, h.stream, &h.coop->nc, out.cvwgt, &h.coop->max_cvw);
-      GKW_CHECK_LAUNCH();
-    }
   };
   if (use_fused(h, g)) {
     // one launch: no graph needed (a launch is as cheap as a graph of one)

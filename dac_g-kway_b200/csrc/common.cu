@@ -260,9 +260,37 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const i32* in, i32*
 
 __global__ void k_set_i32(i32* p, i32 v) { *p = v; }
 
+// A scan that fits one tile: one CTA, no tickets, status words or look-back
+// (the single-pass scan's bookkeeping is several dependent round trips to L2,
+// most of a small scan's time).
+__global__ void __launch_bounds__(kScanThreads) k_scan_small(const i32* in, i32* out, i32 n, i32* total) {
+  __shared__ i32 s_warp[33];
+  const i32 b0 = threadIdx.x * kScanItems;
+  i32 v[kScanItems];
+  i32 sum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = (b0 + i < n) ? in[b0 + i] : 0;
+    sum += v[i];
+  }
+  i32 agg;
+  i32 run = block_exclusive_scan(sum, s_warp, agg);
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (b0 + i < n) out[b0 + i] = run;
+    run += v[i];
+  }
+  if (threadIdx.x == 0 && total) *total = agg;
+}
+
 void exclusive_scan_i32(Handle& h, const i32* in, i32* out, i64 n, i32* total) {
   if (n <= 0) {
     if (total) launch(k_set_i32, 1, 1, 0, h.stream, total, 0);
+    GKW_CHECK_LAUNCH();
+    return;
+  }
+  if (n <= kScanTile) {
+    launch(k_scan_small, 1, kScanThreads, 0, h.stream, in, out, (i32)n, total);
     GKW_CHECK_LAUNCH();
     return;
   }
