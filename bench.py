@@ -708,6 +708,8 @@ def bench_configs(args):
     cases = [("grid27 100x100x96", lambda: gen.grid27(100, 100, 96), 64),
              ("road 12M points", lambda: gen.road(12000000, 1), 256),
              ("circuit 4M vertices", lambda: gen.circuit(4000000, 1), 256)]
+    if args.only:
+        cases = [c for c in cases if c[0].startswith(args.only)]
     out = []
     for name, make, k in cases:
         path = os.path.join(CACHE_DIR, name.replace(" ", "_") + ".npz")
@@ -775,6 +777,8 @@ def main():
                     help="plain workload: skip gkw_autotune (default launch shapes; profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain workload: leave the batched and served objects out of the line")
+    ap.add_argument("--only", default="",
+                    help="configs workload: run only the configurations whose name starts with this")
     ap.add_argument("--device-only", action="store_true",
                     help="plain workload: only the device-resident steps (no e2e, CPU baseline, batched or "
                          "served legs); for profiling runs")
