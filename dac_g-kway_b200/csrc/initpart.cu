@@ -108,10 +108,6 @@ struct TrialState {
 };
 
 __host__ __device__ __forceinline__ i32 gggp_nb1(i32 s) { return (s + 31) >> 5; }
-// Up to this many first-level blocks the growth step scans them directly and
-// keeps no second level: a few loads per lane, and no atomic maxima of all
-// lanes on the one or two second-level words (dense rows serialised on them).
-constexpr i32 kGggpB1Scan = 256;
 __host__ __device__ __forceinline__ i32 gggp_nb2(i32 s) { return (s + 1023) >> 10; }
 // i32 words of one trial's state in shared memory (C, R, K, B1, B2; even, so
 // every trial's u64 arrays stay 8-byte aligned)
@@ -223,14 +219,10 @@ __device__ i64 grow_blocks(const LocalTopo& T, const TrialState& S, i32 s, i32 p
   }
   __syncwarp();
   i64 wR = 0;
-  const bool two = nb1 > kGggpB1Scan;   // second-level maxima kept
   for (i32 step = 0; step < s; ++step) {
     if (step > 0) {
       u64 best = 0;
-      if (two)
-        for (i32 c = lane; c < nb2; c += 32) best = best > B2[c] ? best : B2[c];
-      else
-        for (i32 b = lane; b < nb1; b += 32) best = best > B1[b] ? best : B1[b];
+      for (i32 c = lane; c < nb2; c += 32) best = best > B2[c] ? best : B2[c];
       best = warp_max_u64(best);
       if (best == 0) break;
       pick = key_idx(best);
@@ -271,7 +263,7 @@ __device__ i64 grow_blocks(const LocalTopo& T, const TrialState& S, i32 s, i32 p
           const unsigned long long key = grow_key(c[q] > 0, 2 * c[q] - du[q], u[q]);
           atomicMax(reinterpret_cast<unsigned long long*>(&K[u[q]]), key);
           atomicMax(reinterpret_cast<unsigned long long*>(&B1[u[q] >> 5]), key);
-          if (two) atomicMax(reinterpret_cast<unsigned long long*>(&B2[u[q] >> 10]), key);
+          atomicMax(reinterpret_cast<unsigned long long*>(&B2[u[q] >> 10]), key);
         }
       }
     }
@@ -282,12 +274,10 @@ __device__ i64 grow_blocks(const LocalTopo& T, const TrialState& S, i32 s, i32 p
       const u64 m = warp_max_u64(i < s ? K[i] : 0ull);
       if (lane == 0) B1[b] = m;
       __syncwarp();
-      if (two) {
-        const i32 c = pick >> 10, bb = (c << 5) + lane;
-        const u64 m2 = warp_max_u64(bb < nb1 ? B1[bb] : 0ull);
-        if (lane == 0) B2[c] = m2;
-        __syncwarp();
-      }
+      const i32 c = pick >> 10, bb = (c << 5) + lane;
+      const u64 m2 = warp_max_u64(bb < nb1 ? B1[bb] : 0ull);
+      if (lane == 0) B2[c] = m2;
+      __syncwarp();
     }
     if (wR >= TL) break;
   }
@@ -537,10 +527,6 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   const i32 stw = gggp_state_words(s);
   const size_t need = sizeof(i32) * ((size_t)4 * s + 2 * (size_t)ES + (size_t)stw * trials);
   const bool in_smem = !big && need <= kGggpSmem;   // block-uniform
-  // dense sub-problems whose rows do not fit: the members' row starts,
-  // counts and weights and the trials' state still do, the rows stay global
-  const size_t need_mid = sizeof(i32) * ((size_t)4 * s + (size_t)stw * trials);
-  const bool mid = !big && !in_smem && need_mid <= kGggpSmem;   // block-uniform
   LocalTopo T;
   i32 *rb, *rn, *deg, *vw, *nb, *nw, *state;
   if (in_smem) {
@@ -560,23 +546,6 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     }
     __syncthreads();
     block_exscan_smem(rb, s, s_warp);
-  } else if (mid) {
-    // rows in the global arrays at the members' own CSR positions
-    i32* p = reinterpret_cast<i32*>(smem_raw);
-    rb = p; p += s;
-    rn = p; p += s;
-    deg = p; p += s;
-    vw = p; p += s;
-    state = p;
-    nb = g_nb;
-    nw = g_nw;
-    for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
-      rn[i] = g_rn[base_off + i];
-      rb[i] = xadj[M[i]];
-      deg[i] = g_deg[base_off + i];
-      vw[i] = g_vw[base_off + i];
-    }
-    __syncthreads();
   } else {
     // rows in the global arrays at the members' own CSR positions
     rb = g_rb + base_off;
@@ -651,7 +620,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
   const i32 t = wid;
   if (t < trials) {
     TrialState S;
-    if (in_smem || mid) {
+    if (in_smem) {
       i32* q = state + (size_t)t * stw;   // [C | R | K | B1 | B2]
       S.C = q;
       S.R = q + s;
@@ -695,8 +664,7 @@ __global__ void __launch_bounds__(kInitTrials * 32) k_gggp_depth(
     s_best = b;
   }
   __syncthreads();
-  const i32* Rb = (in_smem || mid) ? state + (size_t)s_best * stw + s
-                                    : g_state + (size_t)s_best * 2 * n + n + base_off;
+  const i32* Rb = in_smem ? state + (size_t)s_best * stw + s : g_state + (size_t)s_best * 2 * n + n + base_off;
   for (i32 i = threadIdx.x; i < s; i += blockDim.x) {
     const i32 v = M[i];
     if (Rb[i]) { lo_out[v] = p0; hi_out[v] = pm; }
@@ -823,14 +791,10 @@ __global__ void __launch_bounds__(kBigThreads, 1) k_gggp_big_trial(
     const i32 p0_local = part_base ? p0 - part_base[p0] : p0;
     i32 pick = (i32)(mix32(seed * 0x9e3779b97f4a7c15ull + (u64)p0_local * 1315423911ull + (u64)t) % (u32)s);
     i64 wR = 0;
-    const bool two = nb1 > kGggpB1Scan;   // second-level maxima kept
     for (i32 step = 0; step < s; ++step) {
       if (step > 0) {
         u64 best = 0;
-        if (two)
-          for (i32 c = lane; c < nb2; c += 32) best = best > B2[c] ? best : B2[c];
-        else
-          for (i32 b = lane; b < nb1; b += 32) best = best > B1[b] ? best : B1[b];
+        for (i32 c = lane; c < nb2; c += 32) best = best > B2[c] ? best : B2[c];
         best = warp_max_u64(best);
         if (best == 0) break;
         pick = key_idx(best);
@@ -863,7 +827,7 @@ __global__ void __launch_bounds__(kBigThreads, 1) k_gggp_big_trial(
           if (u[x] >= 0 && !ru[x]) {
             const unsigned long long key = grow_key(cu[x] > 0, 2 * cu[x] - du[x], u[x]);
             atomicMax(reinterpret_cast<unsigned long long*>(&B1[u[x] >> 5]), key);
-            if (two) atomicMax(reinterpret_cast<unsigned long long*>(&B2[u[x] >> 10]), key);
+            atomicMax(reinterpret_cast<unsigned long long*>(&B2[u[x] >> 10]), key);
           }
         }
       }
@@ -873,12 +837,10 @@ __global__ void __launch_bounds__(kBigThreads, 1) k_gggp_big_trial(
         const u64 m = warp_max_u64(i < s ? member_key(C, R, deg, i) : 0ull);
         if (lane == 0) B1[b] = m;
         __syncwarp();
-        if (two) {
-          const i32 c = pick >> 10, bb = (c << 5) + lane;
-          const u64 m2 = warp_max_u64(bb < nb1 ? B1[bb] : 0ull);
-          if (lane == 0) B2[c] = m2;
-          __syncwarp();
-        }
+        const i32 c = pick >> 10, bb = (c << 5) + lane;
+        const u64 m2 = warp_max_u64(bb < nb1 ? B1[bb] : 0ull);
+        if (lane == 0) B2[c] = m2;
+        __syncwarp();
       }
       if (wR >= P.TL) break;
     }
