@@ -74,7 +74,9 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, i32* err, i32* s_fl
 // passed that word's last use (barrier k - 1), and none can reach its next use
 // (barrier k + 2) before this CTA's release at barrier k + 1.  After the flip
 // a word does not change until it is cleared, so every CTA reads the same
-// total.  The host zeroes words 0 and 1 before the launch.  A one-CTA or
+// total.  Words 0 and 1 must be zero before the first of these barriers (the
+// level kernel's block 0 clears all three before an ordinary grid barrier
+// that every CTA passes first).  A one-CTA or
 // one-cluster grid sums nothing: *total = -1 and the caller loads its counter.
 __device__ __forceinline__ u64 atom_add_release_gpu_u64(u64* p, u64 v) {
   u64 old;
