@@ -188,6 +188,18 @@ def test_server_argument_errors_without_device(pkg):
         pkg.Server(0, narrow_max_n=-5)
 
 
+def test_predicted_footprint(pkg):
+    """The server's admission measure (no device needed): at least the input
+    CSR and part vector, and never smaller for a larger graph or more parts."""
+    f = pkg.predict_footprint
+    for n, m, k in ((1000, 6000, 8), (1 << 20, 6291384, 64), (12_000_000, 26_000_000, 256)):
+        assert f(n, m, k) >= 4 * (n + 1) + 8 * m + 8 * n
+        assert f(2 * n, m, k) > f(n, m, k)
+        assert f(n, 2 * m, k) > f(n, m, k)
+        assert f(n, m, 4 * k) >= f(n, m, k)
+    assert f(0, 0, 1) > 0   # empty graphs still hold the fixed per-job state
+
+
 def test_concat_graphs_layout(pkg, gen):
     gs = [gen.delaunay(300, 1), gen.from_edges(0, np.zeros(0, np.int64), np.zeros(0, np.int64)),
           gen.grid27(3, 3, 3)]
